@@ -1,0 +1,334 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 bundle adjuster on the distortion-BA workload (200 cameras).
+
+Workload ("sequence200"): 200 cameras along a forward-moving path with shared refined
+intrinsics (f=800, k1=-0.1, k2=0.01, p1=p2=1e-3, CommonInternals RADIAL_TANGENTIAL), 50,000
+points in tracks of 3-12 consecutive views (~375k observations), N(0,1 px) noise, 2% outliers,
+Huber threshold 1 px; seeded synthetic data (the reference ships no data set).
+
+One step = one complete minimize() from the same perturbed start until the Huber cost reaches
+the reference optimizer's own final cost on this scene times (1 + 1e-6) (its 100-iteration run,
+recorded in tests/golden/bench_reference.json).  Metric: LM iterations per second; ms_per_step is
+the time to the reference cost.  FP32 normal-equation blocks, FP64 residuals / cost / gradient /
+reduced-system Cholesky (dtype "f32+f64").
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU optimizer (compiled from its sources) on the same
+scene, on a bounded sample of LM iterations per step, single-threaded as the reference is.
+With N > 1 every rank solves its own replica (a single BA does not shard; "replicas only").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "sequence200"
+METRIC = "LM iterations/s to the reference cost (distortion BA, 200 cams / 50k pts / ~375k obs)"
+UNIT = "LM iterations/s"
+REL_TOL = 1e-6
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def load_reference_target():
+    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_reference.json")))[WORKLOAD]
+    return ref
+
+
+def make_scene():
+    from v3dsfmtoolkit_b200 import scenes
+    return scenes.sequence_scene()
+
+
+def scene_digest(sc):
+    import hashlib
+    h = hashlib.sha256()
+    for a in (sc.K, sc.R, sc.T, sc.X, sc.meas, sc.view, sc.point):
+        h.update(np.ascontiguousarray(a).tobytes())
+    if sc.dist is not None:
+        h.update(np.ascontiguousarray(sc.dist).tobytes())
+    return h.hexdigest()[:16]
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def stage_bytes(sc, nblocks_pairs):
+    """Algorithmic DRAM bytes of one launch of each memory-bound stage (FP32 blocks, dA=6, dC=7)."""
+    K, M, N = sc.n_obs, sc.n_points, sc.n_cams
+    dA, dC = sc.dims
+    f32, f64 = 4, 8
+    per_obs_lin = (2 * f64 + 2 * 4) + f64 + (2 * dA + 3 * dA + 2 * dC) * f32 + dA * f64  # read meas/idx; write w,A,W,C,ga
+    per_pt_lin = 3 * f64 + 4 + (6 + 3 * dC) * f32 + 3 * f64                              # read X, ptr; write V,Y,gb
+    lin = K * per_obs_lin + M * per_pt_lin + N * (9 + 3 + 9 + 4) * f64
+    elim = K * (3 * dA * f32 * 2) + M * ((6 + 3 * dC) * f32 * 2 + 3 * f64 * 2 + 4)      # read W,V,Y,gb; write T,Vinv,YV,q
+    return {"linearize": lin, "point_eliminate": elim}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from v3dsfmtoolkit_b200 import capi
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    ref = load_reference_target()
+    sc = make_scene()
+    if scene_digest(sc) != ref["digest"]:
+        raise RuntimeError("generated scene differs from the one the reference cost was recorded on")
+    target = ref["cost"] * (1.0 + REL_TOL)
+    h = capi.Handle.from_scene(sc)
+    opts = capi.default_options(max_iterations=2000, stop_cost=target, precision=capi.PRECISION_MIXED)
+    flush = torch.empty(int(256 * 2 ** 20), dtype=torch.uint8, device="cuda")
+
+    def one_step():
+        flush.zero_()
+        torch.cuda.synchronize()
+        h.reset_params()
+        return h.minimize(opts)
+
+    for _ in range(args.warmup):
+        one_step()
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = capi.launch_count()
+    dev_ms, iters, reached = [], [], []
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = one_step()
+        dev_ms.append(r.device_ms)
+        iters.append(r.iterations)
+        reached.append(bool(r.reached_stop_cost))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    launches = capi.launch_count() - launches0
+    clk = clocks.stop()
+    final_cost = h.cost()
+    if dist:
+        dist.barrier()
+
+    total_ms = float(sum(dev_ms))
+    total_it = int(sum(iters))
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms_max = float(t.item())
+        n = torch.tensor([total_it], dtype=torch.float64, device="cuda")
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        total_it_all = int(n.item())
+    else:
+        total_ms_max, total_it_all = total_ms, total_it
+
+    # roofline of the dominant stage of one LM iteration
+    st_ms = h.profile_stages(capi.PRECISION_MIXED, reps=20)
+    peak, peak_kind = measured_peaks()
+    bytes_ = stage_bytes(sc, None)
+    mem_stages = {k: v for k, v in st_ms.items() if k in bytes_}
+    top = max(st_ms, key=lambda k: st_ms[k])
+    top_mem = max(mem_stages, key=lambda k: mem_stages[k])
+    achieved = bytes_[top_mem] / (st_ms[top_mem] * 1e-3) / 1e9
+    roofline = {"kernel": f"k_{top_mem}", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "algorithmic_bytes": int(bytes_[top_mem]), "launch_ms": round(st_ms[top_mem], 5),
+                "peak_source": peak_kind, "dominant_stage_of_iteration": top,
+                "stage_ms": {k: round(v, 5) for k, v in st_ms.items()}}
+
+    # end to end through the C-ABI from host buffers (create = H2D + layout, minimize, get_params = D2H)
+    e2e = None
+    if not args.no_e2e:
+        e2e_steps = max(1, min(3, args.steps))
+        hb = sum(np.asarray(a).nbytes for a in (sc.K, sc.R, sc.T, sc.dist, sc.X, sc.meas)) + \
+            sc.view.astype(np.int32).nbytes + sc.point.astype(np.int32).nbytes
+        db = sum(np.asarray(a).nbytes for a in (sc.K, sc.R, sc.T, sc.dist, sc.X))
+        it_e, t_e = 0, 0.0
+        for _ in range(e2e_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            h2 = capi.Handle.from_scene(sc)
+            r = h2.minimize(opts)
+            h2.get_params()
+            h2.close()
+            t_e += time.perf_counter() - t0
+            it_e += r.iterations
+        e2e = {"value": round(it_e / t_e, 3), "unit": UNIT, "h2d_bytes_per_step": int(hb),
+               "d2h_bytes_per_step": int(db), "time_to_reference_cost_s": round(t_e / e2e_steps, 5)}
+        if dist:
+            t = torch.tensor([t_e], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e["value"] = round(it_e * world / float(t.item()), 3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(sc, iters_per_sample=10)
+        cpu["reference_iterations_to_cost"] = ref["iterations"]
+        cpu["time_to_reference_cost_s_est"] = round(ref["iterations"] / cpu["value"], 2)
+
+    line = {
+        "metric": METRIC, "value": round(total_it_all / (total_ms_max * 1e-3), 3), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "n_cameras": sc.n_cams, "n_points": sc.n_points,
+                   "n_observations": sc.n_obs, "model": "CommonInternalsMetricBundleOptimizer RADIAL_TANGENTIAL",
+                   "huber_threshold_px": sc.inlier_threshold, "stop": f"cost <= reference cost * (1 + {REL_TOL})",
+                   "reference_cost": ref["cost"], "l2": "flushed (256 MiB write) before every step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "precision": "FP32 normal-equation blocks, FP64 residual/gradient/cost/Cholesky"},
+        "time_to_reference_cost_s": round(total_ms_max / args.steps * 1e-3, 5),
+        "lm_iterations_per_step": round(total_it / args.steps, 2),
+        "reached_reference_cost": all(reached), "final_cost": final_cost,
+        "wall_s": round(wall, 4), "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
+        "cpu_baseline": cpu, "e2e": e2e,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    h.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline_sample(sc, iters_per_sample):
+    """The reference optimizer (compiled from its sources) on a bounded sample: one minimize()
+    call of `iters_per_sample` LM iterations, including its one-time ordering setup."""
+    from oracle.bindings import Reference, reference_available
+    if not reference_available():
+        from oracle.bindings import Restatement
+        eng, kind = Restatement(), "port"
+    else:
+        eng, kind = Reference(), "reference"
+    t0 = time.perf_counter()
+    _, info = eng.minimize(sc, max_iterations=iters_per_sample)
+    dt = time.perf_counter() - t0
+    return {"value": round(info["iterations"] / dt, 4), "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{WORKLOAD}: one minimize() of {info['iterations']} LM iterations incl. setup, "
+                      f"{dt:.1f} s on 1 host core", "sample_s": round(dt, 3)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle.bindings import Reference, Restatement, reference_available
+    sc = make_scene()
+    kind = "reference" if reference_available() else "port"
+    eng = Reference() if kind == "reference" else Restatement()
+    m = max(2, min(10, 100 // max(args.steps, 1)))
+    for _ in range(args.warmup):
+        eng.minimize(sc, max_iterations=1)
+    t0 = time.perf_counter()
+    its = 0
+    for _ in range(args.steps):
+        _, info = eng.minimize(sc, max_iterations=m)
+        its += info["iterations"]
+    dt = time.perf_counter() - t0
+    v = its / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "n_cameras": sc.n_cams, "n_points": sc.n_points,
+                   "n_observations": sc.n_obs, "sample": f"{m} LM iterations of minimize() per step"},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": kind,
+                         "sample": f"{args.steps} x minimize() of {m} LM iterations on {WORKLOAD}"},
+        "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

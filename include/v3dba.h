@@ -1,0 +1,231 @@
+/* v3dba.h -- C-ABI of the B200 sparse Levenberg-Marquardt metric bundle adjuster.
+ *
+ * This is the only boundary between host callers and the CUDA implementation.  It replaces
+ * the reference's SparseLevenbergOptimizer / MetricBundleOptimizer family:
+ *
+ *   v3dba_create           <- MetricBundleOptimizerBase ctor + the three model ctors
+ *                             (V3D/include/Geometry/v3d_metricbundle.h:20-46, 111-119, 168-183,
+ *                              260-273); SparseLevenbergOptimizer ctor (V3D/include/Math/
+ *                              v3d_optimization.h:274-291)
+ *   v3dba_set_nonvarying   <- SparseLevenbergOptimizer::setNonvaryingCounts (v3d_optimization.h:295-300)
+ *   v3dba_minimize         <- SparseLevenbergOptimizer::minimize (V3D/src/Math/v3d_optimization.cpp:719-1250)
+ *                             with the public knobs tau / maxIterations / gradientThreshold /
+ *                             updateThreshold / lambda (v3d_optimization.h:25-68, 382) and the global
+ *                             optimizerVerbosenessLevel (v3d_optimization.h:23)
+ *   v3dba_set_params /
+ *   v3dba_get_params       <- the optimizer's in-place mutation of the caller's cameras, points,
+ *                             K and distortion references (v3d_metricbundle.h:94-95, 232-233, 316)
+ *   v3dba_minimize_batched <- the sequential loop of independent triplet / submodel adjustments
+ *                             (SfM/generate_triples/src/generate_triples.cpp:403-415,
+ *                              SfM/generate_submodels_L1/src/generate_submodels_L1.cpp:330-337)
+ *
+ * Conventions: plain pointers and sizes, row-major doubles, 0-based indices, no exceptions.
+ * Every entry point returns an int error code (V3DBA_OK == 0).  The reference's convergence
+ * outcome is reported separately in v3dba_result.status with its own codes (TIMEOUT=0,
+ * SMALL_UPDATE=1, CONVERGED=2, v3d_optimization.h:16-21).
+ *
+ * Parameter arrays:
+ *   K    : V3DBA_MODEL_STD / VARYING -> n_cameras*9 per-camera intrinsics (row-major 3x3)
+ *          V3DBA_MODEL_COMMON        -> 9 (the shared K of CommonInternalsMetricBundleOptimizer)
+ *   R    : n_cameras*9 world-to-camera rotations,  T : n_cameras*3 translations
+ *   dist : COMMON -> 4 {k1,k2,p1,p2};  VARYING -> n_cameras*4;  STD -> unused (may be NULL)
+ *   X    : n_points*3
+ *   measurements : n_measurements*2 pixels;  view / point : n_measurements camera / point ids
+ */
+#ifndef V3DBA_H
+#define V3DBA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+enum {
+  V3DBA_OK = 0,
+  V3DBA_ERR_INVALID_ARGUMENT = 1,   /* null pointer, bad size, bad model / mode           */
+  V3DBA_ERR_INVALID_INPUT = 2,      /* index out of range, NaN / Inf in the inputs          */
+  V3DBA_ERR_CUDA = 3,               /* a CUDA call failed                                   */
+  V3DBA_ERR_OUT_OF_MEMORY = 4,      /* device allocation failed                            */
+  V3DBA_ERR_NO_DEVICE = 5,          /* no CUDA device                                       */
+  V3DBA_ERR_UNSUPPORTED = 6,        /* a configuration this build does not handle           */
+  V3DBA_ERR_TIMEOUT = 7             /* a bounded device-side wait gave up                   */
+};
+
+/* models (the three optimizer classes) */
+enum {
+  V3DBA_MODEL_STD = 0,              /* StdMetricBundleOptimizer                             */
+  V3DBA_MODEL_COMMON = 1,           /* CommonInternalsMetricBundleOptimizer                 */
+  V3DBA_MODEL_VARYING = 2           /* VaryingInternalsMetricBundleOptimizer                */
+};
+
+/* FULL_BUNDLE_* modes (V3D/include/Geometry/v3d_metricbundle.h:140-148) */
+enum {
+  V3DBA_FULL_BUNDLE_NO_ROTATIONS = -1,
+  V3DBA_FULL_BUNDLE_METRIC = 0,
+  V3DBA_FULL_BUNDLE_FOCAL_LENGTH = 1,
+  V3DBA_FULL_BUNDLE_FOCAL_LENGTH_PP = 2,
+  V3DBA_FULL_BUNDLE_RADIAL = 3,
+  V3DBA_FULL_BUNDLE_RADIAL_TANGENTIAL = 4
+};
+
+/* LM outcome (LEVENBERG_OPTIMIZER_*, V3D/include/Math/v3d_optimization.h:16-21) */
+enum {
+  V3DBA_STATUS_TIMEOUT = 0,
+  V3DBA_STATUS_SMALL_UPDATE = 1,
+  V3DBA_STATUS_CONVERGED = 2
+};
+
+/* arithmetic of the normal-equation blocks (residuals, gradient, cost and the reduced-system
+ * factorisation are always FP64) */
+enum {
+  V3DBA_PRECISION_MIXED = 0,        /* FP32 Jacobian blocks / Schur complement (default)    */
+  V3DBA_PRECISION_FP64 = 1          /* FP64 everywhere                                      */
+};
+
+/* reduced camera system solver */
+enum {
+  V3DBA_SOLVER_AUTO = 0,            /* dense Cholesky up to a size limit, else PCG          */
+  V3DBA_SOLVER_CHOLESKY = 1,        /* tile-sparse dense FP64 Cholesky                      */
+  V3DBA_SOLVER_PCG = 2              /* block-Jacobi preconditioned conjugate gradients     */
+};
+
+typedef struct v3dba_problem {
+  int model;                        /* V3DBA_MODEL_*                                        */
+  int mode;                         /* V3DBA_FULL_BUNDLE_*, ignored for MODEL_STD           */
+  int n_cameras, n_points, n_measurements;
+  double inlier_threshold;          /* Huber threshold in pixels                            */
+  const double* K;
+  const double* R;
+  const double* T;
+  const double* dist;
+  const double* X;
+  const double* measurements;
+  const int32_t* view;
+  const int32_t* point;
+} v3dba_problem;
+
+typedef struct v3dba_options {
+  double tau;                       /* initial damping factor (reference default 1e-3)      */
+  int max_iterations;               /* the reference leaves it uninitialised; callers set it */
+  double gradient_threshold;        /* 1e-10                                                */
+  double update_threshold;          /* 1e-10                                                */
+  int verbosity;                    /* optimizerVerbosenessLevel semantics (0, 1, 2)         */
+  int precision;                    /* V3DBA_PRECISION_*                                    */
+  int solver;                       /* V3DBA_SOLVER_*                                       */
+  double pcg_tolerance;             /* relative residual per LM step (PCG solver)           */
+  int pcg_max_iterations;
+  double stop_cost;                 /* > 0: also stop once an accepted cost <= stop_cost    */
+  int mixed_escalation;             /* MIXED only: 1 (default) switches the blocks to FP64 for
+                                       the rest of the call at the first rejected step or gain
+                                       ratio below 0.1; 0 keeps FP32 blocks throughout         */
+} v3dba_options;
+
+typedef struct v3dba_result {
+  int status;                       /* V3DBA_STATUS_*                                       */
+  int iterations;                   /* currentIteration on exit                             */
+  int n_relinearizations;
+  int n_rejected;
+  double initial_cost;              /* sum |w e|^2 at the first linearisation               */
+  double cost;                      /* sum |w e|^2 at the last linearisation                */
+  double lambda;                    /* damping on exit                                      */
+  double device_ms;                 /* device time of the call (CUDA events)                */
+  int pcg_iterations;               /* total PCG iterations (PCG solver)                    */
+  int reached_stop_cost;            /* 1 when stop_cost ended the call                      */
+  int fp64_from_iteration;          /* MIXED: iteration at which FP64 blocks took over, or -1 */
+} v3dba_result;
+
+typedef struct v3dba_handle_s* v3dba_handle;
+
+/* Fills opts with the reference defaults (tau 1e-3, maxIterations 50, thresholds 1e-10). */
+void v3dba_default_options(v3dba_options* opts);
+
+/* Copies the problem to the GPU, builds the point-major layout, the Schur block structure and
+ * the symbolic factorisation of the reduced system.  |p| for the update stopping test and the
+ * COMMON aspect ratio are cached here, as the reference's constructors do. */
+int v3dba_create(const v3dba_problem* problem, v3dba_handle* out);
+int v3dba_destroy(v3dba_handle h);
+
+/* Fixes the first nA cameras, nB points and nC global intrinsic parameters. */
+int v3dba_set_nonvarying(v3dba_handle h, int nA, int nB, int nC);
+
+/* lambda / _nu state carried across minimize calls, as on the reference object. */
+int v3dba_set_lambda(v3dba_handle h, double lambda);
+
+int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_result* result);
+
+/* Host <-> device parameter transfer (same layout as v3dba_problem; dist may be NULL for STD). */
+int v3dba_set_params(v3dba_handle h, const double* K, const double* R, const double* T,
+                     const double* dist, const double* X);
+int v3dba_get_params(v3dba_handle h, double* K, double* R, double* T, double* dist, double* X);
+
+/* Restores the parameters passed to v3dba_create (device-to-device; no host traffic) and the
+ * optimizer state of a new object (lambda 1e-3, _nu 2). */
+int v3dba_reset_params(v3dba_handle h);
+
+/* sum_k |w_k e_k|^2 with Huber weights recomputed at the current device parameters. */
+int v3dba_cost(v3dba_handle h, double* cost);
+
+/* One linearisation at the current parameters, copied to the host for inspection:
+ * e (n_meas*2), w (n_meas), the weighted Jacobian blocks in the caller's measurement order
+ * A (n_meas*2*dA), B (n_meas*2*3), C (n_meas*2*dC) and the gradient J^T(-w e) split as
+ * ga (n_cams*dA), gb (n_points*3), gc (dC).  Any output may be NULL. */
+int v3dba_linearize(v3dba_handle h, int precision, double* e, double* w, double* A, double* B,
+                    double* C, double* ga, double* gb, double* gc);
+
+/* The damped reduced camera system at the current parameters for damping lambda, in FP64:
+ * S (n x n, row-major, n = n_cams*dA + dC, full symmetric) and rhs (n). */
+int v3dba_reduced_system(v3dba_handle h, int precision, double lambda, double* S, double* rhs);
+
+/* Dimensions of a model / mode (dA camera block, dC global block). */
+int v3dba_dims(int model, int mode, int* dA, int* dC);
+
+/* Standalone tile-sparse FP64 Cholesky solve on the GPU of a dense SPD system (row-major n x n,
+ * host memory).  Returns V3DBA_OK and *fail = 1 when a pivot is not positive. */
+int v3dba_dense_cholesky_solve(int n, const double* S, const double* rhs, double* x, int* fail);
+
+/* Batched independent problems (triplets / submodels), all of the same model and mode, solved
+ * in one persistent launch.  Parameters of every problem are updated in place; results[i]
+ * receives problem i's outcome. */
+int v3dba_minimize_batched(const v3dba_problem* problems, int count, const v3dba_options* opts,
+                           double* const* K, double* const* R, double* const* T,
+                           double* const* dist, double* const* X, v3dba_result* results);
+
+/* Stages of one LM iteration (benchmark support; no counterpart in the reference). */
+enum {
+  V3DBA_STAGE_LINEARIZE = 0,        /* residuals, Huber weights, Jacobian blocks, point sums  */
+  V3DBA_STAGE_CAMERA_CHUNKS = 1,    /* partial U_i, gradient, X_i per observation chunk       */
+  V3DBA_STAGE_CAMERA_FINISH = 2,    /* U_i, gradient, X_i per camera                          */
+  V3DBA_STAGE_RELIN_FINALIZE = 3,   /* global sums, gradient max, initial lambda              */
+  V3DBA_STAGE_POINT_ELIMINATE = 4,  /* (V_j + lambda I)^-1 and W_k V_j^-1                     */
+  V3DBA_STAGE_SCHUR_CHUNKS = 5,     /* partial camera-pair blocks per chunk of pairs          */
+  V3DBA_STAGE_SCHUR_FINISH = 6,     /* camera-pair blocks of the reduced system               */
+  V3DBA_STAGE_RHS_CHUNKS = 7,       /* partial reduced right-hand side / border               */
+  V3DBA_STAGE_RHS_FINISH = 8,       /* reduced right-hand side, camera/global border          */
+  V3DBA_STAGE_GLOBAL_BLOCK = 9,     /* global block                                           */
+  V3DBA_STAGE_POINT_BACKSUB = 10,   /* point updates                                          */
+  V3DBA_STAGE_CAMERA_UPDATE = 11,   /* camera and global updates                              */
+  V3DBA_STAGE_TRIAL_COST = 12,      /* cost of the trial step with frozen weights             */
+  V3DBA_STAGE_TRIAL_FINALIZE = 13,  /* step statistics                                        */
+  V3DBA_STAGE_CHOLESKY = 14,        /* tile FP64 Cholesky factor + solve                      */
+  V3DBA_STAGE_ZERO = 15,            /* clearing the pattern tiles of the reduced system       */
+  V3DBA_NUM_STAGES = 16
+};
+
+/* Average device time (ms) of every stage over `reps` launches each, timed with CUDA events on
+ * the handle's stream at the current parameters and damping 1e-3 * max diagonal.  ms receives
+ * V3DBA_NUM_STAGES values.  Leaves the parameters unchanged.  (Benchmark support; no
+ * counterpart in the reference.) */
+int v3dba_profile_stages(v3dba_handle h, int precision, int reps, double* ms);
+
+/* Kernel launches issued by this library in the calling process so far. */
+uint64_t v3dba_launch_count(void);
+
+const char* v3dba_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* V3DBA_H */

@@ -1,0 +1,268 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings for the CPU oracle.
+
+* :class:`Reference` -- the reference's own optimizer compiled from its sources
+  (``oracle/_ref/libv3dref.so``, built by ``oracle/Makefile`` where the reference is mounted;
+  the prebuilt file travels with the repository snapshot).
+* :class:`Restatement` -- the plain-C FP64 restatement (``oracle/_build/libv3dba_oracle.so``).
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import this
+module, and only as the checker / the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libv3dref.so")
+ORC_LIB = os.path.join(HERE, "_build", "libv3dba_oracle.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _scene_arrays(scene):
+    K, R, T, dist, X = (np.array(a, dtype=np.float64, copy=True) for a in scene.params())
+    return K, R, T, dist, X
+
+
+def build(quiet=True):
+    """Builds whatever oracle/Makefile can build here (the reference part needs its sources)."""
+    import subprocess
+    cmd = ["make", "-C", HERE]
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL if quiet else None)
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+class Reference:
+    """The reference optimizer classes driven through oracle/ref_capi.cpp."""
+
+    def __init__(self, path=REF_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference oracle library missing: {path} (run make -C oracle)")
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.v3dref_minimize.restype = C.c_int
+        L.v3dref_minimize.argtypes = [C.c_int] * 5 + [C.c_double] + [_dp] * 5 + [_dp, _ip, _ip] + \
+            [C.c_int] * 3 + [C.c_double, C.c_int, C.c_int] + [_ip, _ip, _dp] + [_dp, _dp, _ip, C.c_int, _ip, _ip]
+        L.v3dref_linearize.restype = C.c_int
+        L.v3dref_linearize.argtypes = [C.c_int] * 5 + [C.c_double] + [_dp] * 5 + [_dp, _ip, _ip] + [_dp] * 5
+        L.v3dref_cost.restype = C.c_double
+        L.v3dref_cost.argtypes = [C.c_int] * 5 + [C.c_double] + [_dp] * 5 + [_dp, _ip, _ip]
+
+    def _head(self, sc):
+        return (sc.model, sc.mode, sc.n_cams, sc.n_points, sc.n_obs, float(sc.inlier_threshold))
+
+    def minimize(self, scene, tau=1e-3, max_iterations=50, nonvarying=(0, 0, 0), verbosity=0,
+                 trace_cap=256):
+        """Runs minimize() on a copy of ``scene``'s parameters; returns (params, info)."""
+        K, R, T, dist, X = _scene_arrays(scene)
+        meas, view, point = _f64(scene.meas), _i32(scene.view), _i32(scene.point)
+        st, it, lam = C.c_int(), C.c_int(), C.c_double()
+        tc, tl, ti = np.zeros(trace_cap), np.zeros(trace_cap), np.zeros(trace_cap, dtype=np.int32)
+        tlen, nrej = C.c_int(), C.c_int()
+        rc = self.lib.v3dref_minimize(*self._head(scene), _d(K), _d(R), _d(T), _d(dist), _d(X),
+                                      _d(meas), _i(view), _i(point), *nonvarying, tau, max_iterations,
+                                      verbosity, C.byref(st), C.byref(it), C.byref(lam),
+                                      _d(tc), _d(tl), _i(ti), trace_cap, C.byref(tlen), C.byref(nrej))
+        if rc != 0:
+            raise ValueError("reference rejected the problem")
+        n = min(tlen.value, trace_cap)
+        info = dict(status=st.value, iterations=it.value, lambda_=lam.value,
+                    trace_cost=tc[:n].copy(), trace_lambda=tl[:n].copy(), trace_iter=ti[:n].copy(),
+                    n_relinearizations=tlen.value, n_rejected=nrej.value)
+        return (K, R, T, dist, X), info
+
+    def linearize(self, scene, params=None):
+        dA, dC = scene.dims
+        K, R, T, dist, X = params if params is not None else _scene_arrays(scene)
+        n = scene.n_obs
+        e, w = np.zeros((n, 2)), np.zeros(n)
+        A, B, Cm = np.zeros((n, 2, dA)), np.zeros((n, 2, 3)), np.zeros((n, 2, max(dC, 1)))
+        rc = self.lib.v3dref_linearize(*self._head(scene), _d(_f64(K)), _d(_f64(R)), _d(_f64(T)),
+                                       _d(_f64(dist)), _d(_f64(X)), _d(_f64(scene.meas)),
+                                       _i(_i32(scene.view)), _i(_i32(scene.point)),
+                                       _d(e), _d(w), _d(A), _d(B), _d(Cm) if dC else None)
+        if rc != 0:
+            raise ValueError("reference rejected the problem")
+        return e, w, A, B, Cm[..., :dC]
+
+    def cost(self, scene, params=None):
+        K, R, T, dist, X = params if params is not None else _scene_arrays(scene)
+        return self.lib.v3dref_cost(*self._head(scene), _d(_f64(K)), _d(_f64(R)), _d(_f64(T)),
+                                    _d(_f64(dist)), _d(_f64(X)), _d(_f64(scene.meas)),
+                                    _i(_i32(scene.view)), _i(_i32(scene.point)))
+
+
+class _OrcProblem(C.Structure):
+    _fields_ = [("model", C.c_int), ("mode", C.c_int), ("n_cams", C.c_int), ("n_points", C.c_int),
+                ("n_obs", C.c_int), ("inlier_threshold", C.c_double), ("nnA", C.c_int),
+                ("nnB", C.c_int), ("nnC", C.c_int), ("meas", _dp), ("view", _ip), ("point", _ip)]
+
+
+class _OrcParams(C.Structure):
+    _fields_ = [("K", _dp), ("R", _dp), ("T", _dp), ("dist", _dp), ("X", _dp)]
+
+
+class _OrcOptions(C.Structure):
+    _fields_ = [("tau", C.c_double), ("max_iterations", C.c_int), ("gradient_threshold", C.c_double),
+                ("update_threshold", C.c_double), ("param_length", C.c_double),
+                ("cached_aspect_ratio", C.c_double), ("lambda_", C.c_double), ("nu", C.c_double)]
+
+
+class _OrcResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("n_relinearizations", C.c_int),
+                ("n_rejected", C.c_int), ("final_err", C.c_double)]
+
+
+class Restatement:
+    """The C restatement in oracle/v3dba_oracle.c."""
+
+    def __init__(self, path=ORC_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle restatement library missing: {path} (run make -C oracle restate)")
+        self.lib = C.CDLL(path)
+        L = self.lib
+        P, X_ = C.POINTER(_OrcProblem), C.POINTER(_OrcParams)
+        L.orc_param_length.restype = C.c_double
+        L.orc_param_length.argtypes = [P, X_]
+        L.orc_linearize.argtypes = [P, X_, C.c_double] + [_dp] * 5
+        L.orc_cost.restype = C.c_double
+        L.orc_cost.argtypes = [P, X_, C.c_double, _dp]
+        L.orc_normal_blocks.restype = C.c_double
+        L.orc_normal_blocks.argtypes = [P, X_, C.c_double] + [_dp] * 10
+        L.orc_reduced_system.argtypes = [P, C.c_int, C.c_int, C.c_double] + [_dp] * 12
+        L.orc_cholesky_solve.argtypes = [C.c_int, _dp, _dp]
+        L.orc_point_update.argtypes = [P, C.c_int, C.c_int] + [_dp] * 7
+        L.orc_minimize.argtypes = [P, X_, C.POINTER(_OrcOptions), C.POINTER(_OrcResult), _ip, _dp, _dp, C.c_int]
+        L.orc_pcg.restype = C.c_int
+        L.orc_pcg.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, C.c_int, _dp]
+        L.orc_rodrigues.argtypes = [_dp, _dp]
+
+    @staticmethod
+    def _problem(scene, nonvarying=(0, 0, 0)):
+        keep = (_f64(scene.meas), _i32(scene.view), _i32(scene.point))
+        p = _OrcProblem(scene.model, scene.mode, scene.n_cams, scene.n_points, scene.n_obs,
+                        float(scene.inlier_threshold), *nonvarying, _d(keep[0]), _i(keep[1]), _i(keep[2]))
+        return p, keep
+
+    @staticmethod
+    def _params(arrs):
+        K, R, T, dist, X = arrs
+        return _OrcParams(_d(K), _d(R), _d(T), _d(dist), _d(X))
+
+    @staticmethod
+    def cached_ar(scene):
+        K = scene.K if scene.K.ndim == 2 else scene.K[0]
+        return float(K[1, 1] / K[0, 0])
+
+    def param_length(self, scene):
+        p, keep = self._problem(scene)
+        arrs = _scene_arrays(scene)
+        return self.lib.orc_param_length(C.byref(p), C.byref(self._params(arrs)))
+
+    def linearize(self, scene, params=None):
+        dA, dC = scene.dims
+        p, keep = self._problem(scene)
+        arrs = params if params is not None else _scene_arrays(scene)
+        arrs = tuple(_f64(a) for a in arrs)
+        n = scene.n_obs
+        e, w = np.zeros((n, 2)), np.zeros(n)
+        A, B, Cm = np.zeros((n, 2, dA)), np.zeros((n, 2, 3)), np.zeros((n, 2, max(dC, 1)))
+        self.lib.orc_linearize(C.byref(p), C.byref(self._params(arrs)), self.cached_ar(scene),
+                               _d(e), _d(w), _d(A), _d(B), _d(Cm))
+        return e, w, A, B, Cm[..., :dC]
+
+    def cost(self, scene, params=None, weights=None):
+        p, keep = self._problem(scene)
+        arrs = tuple(_f64(a) for a in (params if params is not None else _scene_arrays(scene)))
+        return self.lib.orc_cost(C.byref(p), C.byref(self._params(arrs)), self.cached_ar(scene),
+                                 _d(_f64(weights)) if weights is not None else None)
+
+    def normal_blocks(self, scene, params=None, nonvarying=(0, 0, 0)):
+        dA, dC = scene.dims
+        N, M, n = scene.n_cams, scene.n_points, scene.n_obs
+        p, keep = self._problem(scene, nonvarying)
+        arrs = tuple(_f64(a) for a in (params if params is not None else _scene_arrays(scene)))
+        dc = max(dC, 1)
+        out = dict(w=np.zeros(n), U=np.zeros((N, dA, dA)), V=np.zeros((M, 3, 3)), W=np.zeros((n, dA, 3)),
+                   X=np.zeros((N, dA, dc)), Y=np.zeros((M, 3, dc)), Z=np.zeros((dc, dc)),
+                   ga=np.zeros((N, dA)), gb=np.zeros((M, 3)), gc=np.zeros(dc))
+        err = self.lib.orc_normal_blocks(C.byref(p), C.byref(self._params(arrs)), self.cached_ar(scene),
+                                         *[_d(out[k]) for k in ("w", "U", "V", "W", "X", "Y", "Z", "ga", "gb", "gc")])
+        out["X"], out["Y"], out["Z"], out["gc"] = out["X"][..., :dC], out["Y"][..., :dC], out["Z"][:dC, :dC], out["gc"][:dC]
+        out["err"] = err
+        return out
+
+    def reduced_system(self, scene, blocks, lam, nonvarying=(0, 0, 0)):
+        dA, dC = scene.dims
+        N, M = scene.n_cams, scene.n_points
+        p, keep = self._problem(scene, nonvarying)
+        n = N * dA + dC
+        S, rhs, Vinv = np.zeros((n, n)), np.zeros(n), np.zeros((M, 3, 3))
+        dc = max(dC, 1)
+        Xb = np.zeros((N, dA, dc)); Xb[..., :dC] = blocks["X"]
+        Yb = np.zeros((M, 3, dc)); Yb[..., :dC] = blocks["Y"]
+        Zb = np.zeros((dc, dc)); Zb[:dC, :dC] = blocks["Z"]
+        gcb = np.zeros(dc); gcb[:dC] = blocks["gc"]
+        # the C side indexes X/Y/Z with leading dimension dC; repack without padding
+        Xp = _f64(blocks["X"]) if dC else np.zeros(1)
+        Yp = _f64(blocks["Y"]) if dC else np.zeros(1)
+        Zp = _f64(blocks["Z"]) if dC else np.zeros(1)
+        gcp = _f64(blocks["gc"]) if dC else np.zeros(1)
+        fail = self.lib.orc_reduced_system(C.byref(p), dA, dC, lam, _d(_f64(blocks["U"])), _d(_f64(blocks["V"])),
+                                           _d(_f64(blocks["W"])), _d(Xp), _d(Yp), _d(Zp),
+                                           _d(_f64(blocks["ga"])), _d(_f64(blocks["gb"])), _d(gcp),
+                                           _d(S), _d(rhs), _d(Vinv))
+        return S, rhs, Vinv, fail
+
+    def cholesky_solve(self, S, rhs):
+        S = np.array(S, dtype=np.float64, copy=True)
+        x = np.array(rhs, dtype=np.float64, copy=True)
+        fail = self.lib.orc_cholesky_solve(S.shape[0], _d(S), _d(x))
+        return x, fail
+
+    def minimize(self, scene, tau=1e-3, max_iterations=50, nonvarying=(0, 0, 0), lambda0=1e-3,
+                 trace_cap=256, gradient_threshold=1e-10, update_threshold=1e-10):
+        p, keep = self._problem(scene, nonvarying)
+        arrs = _scene_arrays(scene)
+        opt = _OrcOptions(tau, max_iterations, gradient_threshold, update_threshold,
+                          self.param_length(scene), self.cached_ar(scene), lambda0, 2.0)
+        res = _OrcResult()
+        ti, tl, te = np.zeros(trace_cap, dtype=np.int32), np.zeros(trace_cap), np.zeros(trace_cap)
+        rc = self.lib.orc_minimize(C.byref(p), C.byref(self._params(arrs)), C.byref(opt), C.byref(res),
+                                   _i(ti), _d(tl), _d(te), trace_cap)
+        if rc != 0:
+            raise ValueError("oracle rejected the problem")
+        n = min(res.n_relinearizations, trace_cap)
+        info = dict(status=res.status, iterations=res.iterations, lambda_=opt.lambda_,
+                    n_relinearizations=res.n_relinearizations, n_rejected=res.n_rejected,
+                    trace_cost=te[:n].copy(), trace_lambda=tl[:n].copy(), trace_iter=ti[:n].copy())
+        return arrs, info
+
+    def pcg(self, S, b, bs, rel_tol=1e-6, max_iter=1000, Minv=None):
+        x = np.zeros_like(b)
+        it = self.lib.orc_pcg(S.shape[0], bs, _d(_f64(S)), _d(_f64(b)),
+                              _d(_f64(Minv)) if Minv is not None else None, rel_tol, max_iter, _d(x))
+        return x, it

@@ -1,0 +1,295 @@
+// TEST INFRASTRUCTURE ONLY -- never linked into, or called by, the product library.
+//
+// A C-ABI around the reference's own sparse LM bundle adjuster, compiled from the
+// untouched reference sources (see oracle/Makefile).  It lets tests and the bench's
+// CPU baseline drive the reference optimizer classes on flat structure-of-arrays
+// inputs:
+//   * V3D::StdMetricBundleOptimizer             (V3D/include/Geometry/v3d_metricbundle.h:107-136)
+//   * V3D::CommonInternalsMetricBundleOptimizer (V3D/include/Geometry/v3d_metricbundle.h:150-238)
+//   * V3D::VaryingInternalsMetricBundleOptimizer(V3D/include/Geometry/v3d_metricbundle.h:242-320)
+// all running V3D::SparseLevenbergOptimizer::minimize (V3D/src/Math/v3d_optimization.cpp:719-1250).
+//
+// Parameter layout (row-major, doubles), shared with the product C-ABI:
+//   K    : model 0/2 -> nCams*9 per-camera intrinsics; model 1 -> 9 (the shared K)
+//   R    : nCams*9,  T : nCams*3,  X : nPoints*3
+//   dist : model 1 -> 4 {k1,k2,p1,p2}; model 2 -> nCams*4; model 0 -> unused
+//   meas : nObs*2,  view/point : nObs (0-based)
+
+#include "Geometry/v3d_metricbundle.h"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+using namespace V3D;
+
+namespace
+{
+   enum { MODEL_STD = 0, MODEL_COMMON = 1, MODEL_VARYING = 2 };
+
+   struct Trace
+   {
+      double* cost; double* lambda; int* iter; int cap; int len;
+      int nRejected;
+   };
+
+   // Records the weighted cost each time the optimizer relinearizes: fillWeights is
+   // called once per relinearization (v3d_optimization.cpp:785), before the lambda
+   // for that iteration is initialised.
+   template <typename Opt>
+   struct Traced : public Opt
+   {
+      template <typename... Args>
+      Traced(Trace* tr, Args&&... args) : Opt(std::forward<Args>(args)...), _tr(tr) { }
+
+      virtual void fillWeights(VectorArray<double> const& residual, Vector<double>& w)
+      {
+         Opt::fillWeights(residual, w);
+         if (_tr && _tr->len < _tr->cap)
+         {
+            double err = 0.0;
+            for (unsigned k = 0; k < w.size(); ++k)
+               err += w[k] * w[k] * (residual[k][0] * residual[k][0] + residual[k][1] * residual[k][1]);
+            _tr->cost[_tr->len] = err;
+            _tr->lambda[_tr->len] = this->lambda;
+            _tr->iter[_tr->len] = this->currentIteration;
+         }
+         if (_tr) ++_tr->len;
+      }
+
+      virtual void restoreAllParameters()
+      {
+         Opt::restoreAllParameters();
+         if (_tr) ++_tr->nRejected;
+      }
+
+      Trace* _tr;
+   };
+
+   struct Scene
+   {
+      std::vector<CameraMatrix> cams;
+      std::vector<Vector3d> Xs;
+      std::vector<Vector2d> meas;
+      std::vector<int> view, point;
+      Matrix3x3d Kshared;
+      StdDistortionFunction dist;
+      std::vector<StdDistortionFunction> dists;
+   };
+
+   void loadMat3(double const* p, Matrix3x3d& M)
+   {
+      for (int r = 0; r < 3; ++r)
+         for (int c = 0; c < 3; ++c) M[r][c] = p[3 * r + c];
+   }
+
+   void storeMat3(Matrix3x3d const& M, double* p)
+   {
+      for (int r = 0; r < 3; ++r)
+         for (int c = 0; c < 3; ++c) p[3 * r + c] = M[r][c];
+   }
+
+   void loadDist(double const* p, StdDistortionFunction& d)
+   {
+      d.k1 = p[0]; d.k2 = p[1]; d.p1 = p[2]; d.p2 = p[3];
+   }
+
+   void storeDist(StdDistortionFunction const& d, double* p)
+   {
+      p[0] = d.k1; p[1] = d.k2; p[2] = d.p1; p[3] = d.p2;
+   }
+
+   void buildScene(Scene& s, int model, int nCams, int nPoints, int nObs,
+                   double const* K, double const* R, double const* T, double const* dist,
+                   double const* X, double const* meas, int const* view, int const* point)
+   {
+      s.cams.resize(nCams);
+      if (model == MODEL_COMMON) loadMat3(K, s.Kshared);
+      for (int i = 0; i < nCams; ++i)
+      {
+         Matrix3x3d Ki, Ri;
+         Vector3d Ti;
+         if (model == MODEL_COMMON) Ki = s.Kshared; else loadMat3(K + 9 * i, Ki);
+         loadMat3(R + 9 * i, Ri);
+         Ti[0] = T[3 * i]; Ti[1] = T[3 * i + 1]; Ti[2] = T[3 * i + 2];
+         s.cams[i] = CameraMatrix(Ki, Ri, Ti);
+      }
+      s.Xs.resize(nPoints);
+      for (int j = 0; j < nPoints; ++j)
+         s.Xs[j] = Vector3d(X[3 * j], X[3 * j + 1], X[3 * j + 2]);
+      s.meas.resize(nObs);
+      for (int k = 0; k < nObs; ++k)
+      {
+         s.meas[k][0] = meas[2 * k];
+         s.meas[k][1] = meas[2 * k + 1];
+      }
+      s.view.assign(view, view + nObs);
+      s.point.assign(point, point + nObs);
+      if (model == MODEL_COMMON) loadDist(dist, s.dist);
+      if (model == MODEL_VARYING)
+      {
+         s.dists.resize(nCams);
+         for (int i = 0; i < nCams; ++i) loadDist(dist + 4 * i, s.dists[i]);
+      }
+   }
+
+   void exportScene(Scene const& s, int model, double* K, double* R, double* T, double* dist, double* X)
+   {
+      int const nCams = s.cams.size();
+      for (int i = 0; i < nCams; ++i)
+      {
+         if (model != MODEL_COMMON) storeMat3(s.cams[i].getIntrinsic(), K + 9 * i);
+         storeMat3(s.cams[i].getRotation(), R + 9 * i);
+         Vector3d const& Ti = s.cams[i].getTranslation();
+         T[3 * i] = Ti[0]; T[3 * i + 1] = Ti[1]; T[3 * i + 2] = Ti[2];
+      }
+      if (model == MODEL_COMMON) { storeMat3(s.Kshared, K); storeDist(s.dist, dist); }
+      if (model == MODEL_VARYING)
+         for (int i = 0; i < nCams; ++i) storeDist(s.dists[i], dist + 4 * i);
+      for (size_t j = 0; j < s.Xs.size(); ++j)
+      {
+         X[3 * j] = s.Xs[j][0]; X[3 * j + 1] = s.Xs[j][1]; X[3 * j + 2] = s.Xs[j][2];
+      }
+   }
+
+   bool validModel(int model, int mode)
+   {
+      if (model < MODEL_STD || model > MODEL_VARYING) return false;
+      if (model != MODEL_STD && (mode < FULL_BUNDLE_NO_ROTATIONS || mode > FULL_BUNDLE_RADIAL_TANGENTIAL))
+         return false;
+      return true;
+   }
+
+   template <typename Opt>
+   void runMinimize(Opt& opt, int nnA, int nnB, int nnC, double tau, int maxIterations,
+                    int* status, int* iterations, double* lambda)
+   {
+      opt.setNonvaryingCounts(nnA, nnB, nnC);
+      opt.tau = tau;
+      opt.maxIterations = maxIterations;
+      opt.minimize();
+      *status = opt.status;
+      *iterations = opt.currentIteration;
+      *lambda = opt.lambda;
+   }
+} // end namespace <>
+
+extern "C"
+{
+
+int v3dref_param_dims(int model, int mode, int* dA, int* dC)
+{
+   if (!validModel(model, mode)) return -1;
+   *dA = 6; *dC = 0;
+   if (model == MODEL_COMMON) *dC = CommonInternalsMetricBundleOptimizer::globalParamDimensionFromMode(mode);
+   if (model == MODEL_VARYING) *dA = 6 + VaryingInternalsMetricBundleOptimizer::extParamDimensionFromMode(mode);
+   return 0;
+}
+
+// Runs the reference minimize(). Parameters are updated in place.  The optional trace
+// (any pointer may be NULL when traceCap == 0) receives one (iteration, lambda, cost)
+// entry per relinearization.
+int v3dref_minimize(int model, int mode, int nCams, int nPoints, int nObs, double inlierThreshold,
+                    double* K, double* R, double* T, double* dist, double* X,
+                    double const* meas, int const* view, int const* point,
+                    int nnA, int nnB, int nnC, double tau, int maxIterations, int verbosity,
+                    int* status, int* iterations, double* lambda,
+                    double* traceCost, double* traceLambda, int* traceIter, int traceCap,
+                    int* traceLen, int* nRejected)
+{
+   if (!validModel(model, mode)) return -1;
+   Scene s;
+   buildScene(s, model, nCams, nPoints, nObs, K, R, T, dist, X, meas, view, point);
+   Trace tr = { traceCost, traceLambda, traceIter, traceCap, 0, 0 };
+   V3D::optimizerVerbosenessLevel = verbosity;
+
+   if (model == MODEL_STD)
+   {
+      Traced<StdMetricBundleOptimizer> opt(&tr, inlierThreshold, s.cams, s.Xs, s.meas, s.view, s.point);
+      runMinimize(opt, nnA, nnB, nnC, tau, maxIterations, status, iterations, lambda);
+   }
+   else if (model == MODEL_COMMON)
+   {
+      Traced<CommonInternalsMetricBundleOptimizer> opt(&tr, mode, inlierThreshold, s.Kshared, s.dist,
+                                                       s.cams, s.Xs, s.meas, s.view, s.point);
+      runMinimize(opt, nnA, nnB, nnC, tau, maxIterations, status, iterations, lambda);
+   }
+   else
+   {
+      Traced<VaryingInternalsMetricBundleOptimizer> opt(&tr, mode, inlierThreshold, s.dists,
+                                                        s.cams, s.Xs, s.meas, s.view, s.point);
+      runMinimize(opt, nnA, nnB, nnC, tau, maxIterations, status, iterations, lambda);
+   }
+   V3D::optimizerVerbosenessLevel = 0;
+   exportScene(s, model, K, R, T, dist, X);
+   if (traceLen) *traceLen = tr.len;
+   if (nRejected) *nRejected = tr.nRejected;
+   return 0;
+}
+
+// Per-observation residual e_k = proj - m_k, Huber weight w_k and the raw (unweighted)
+// Jacobian blocks A_k (2 x dA), B_k (2 x 3), C_k (2 x dC), all row-major, evaluated by the
+// reference's own evalResidual / fillWeights / fillJacobians.  Any output may be NULL.
+int v3dref_linearize(int model, int mode, int nCams, int nPoints, int nObs, double inlierThreshold,
+                     double const* K, double const* R, double const* T, double const* dist,
+                     double const* X, double const* meas, int const* view, int const* point,
+                     double* e, double* w, double* A, double* B, double* C)
+{
+   int dA, dC;
+   if (v3dref_param_dims(model, mode, &dA, &dC) != 0) return -1;
+   Scene s;
+   buildScene(s, model, nCams, nPoints, nObs, K, R, T, dist, X, meas, view, point);
+
+   SparseLevenbergOptimizer* opt = 0;
+   if (model == MODEL_STD)
+      opt = new StdMetricBundleOptimizer(inlierThreshold, s.cams, s.Xs, s.meas, s.view, s.point);
+   else if (model == MODEL_COMMON)
+      opt = new CommonInternalsMetricBundleOptimizer(mode, inlierThreshold, s.Kshared, s.dist,
+                                                     s.cams, s.Xs, s.meas, s.view, s.point);
+   else
+      opt = new VaryingInternalsMetricBundleOptimizer(mode, inlierThreshold, s.dists,
+                                                      s.cams, s.Xs, s.meas, s.view, s.point);
+
+   VectorArray<double> res(nObs, 2);
+   Vector<double> weights(nObs);
+   opt->evalResidual(res);
+   opt->fillWeights(res, weights);
+
+   Matrix<double> Ak(2, dA), Bk(2, 3), Ck(2, dC > 0 ? dC : 1);
+   for (int k = 0; k < nObs; ++k)
+   {
+      if (e) { e[2 * k] = res[k][0]; e[2 * k + 1] = res[k][1]; }
+      if (w) w[k] = weights[k];
+      if (A || B || C)
+      {
+         makeZeroMatrix(Ak); makeZeroMatrix(Bk); makeZeroMatrix(Ck);
+         opt->fillJacobians(Ak, Bk, Ck, view[k], point[k], k);
+         for (int r = 0; r < 2; ++r)
+         {
+            if (A) for (int c = 0; c < dA; ++c) A[(2 * k + r) * dA + c] = Ak[r][c];
+            if (B) for (int c = 0; c < 3; ++c) B[(2 * k + r) * 3 + c] = Bk[r][c];
+            if (C) for (int c = 0; c < dC; ++c) C[(2 * k + r) * dC + c] = Ck[r][c];
+         }
+      }
+   }
+   delete opt;
+   return 0;
+}
+
+// Final cost as the harness defines it: sum_k |w_k e_k|^2 with the Huber weights
+// recomputed at the given parameters (v3d_metricbundle.h:49-57, v3d_optimization.cpp:784-789).
+double v3dref_cost(int model, int mode, int nCams, int nPoints, int nObs, double inlierThreshold,
+                   double const* K, double const* R, double const* T, double const* dist,
+                   double const* X, double const* meas, int const* view, int const* point)
+{
+   std::vector<double> e(2 * (size_t)nObs), w(nObs);
+   if (v3dref_linearize(model, mode, nCams, nPoints, nObs, inlierThreshold, K, R, T, dist, X,
+                        meas, view, point, e.data(), w.data(), 0, 0, 0) != 0)
+      return -1.0;
+   double err = 0.0;
+   for (int k = 0; k < nObs; ++k)
+      err += w[k] * w[k] * (e[2 * k] * e[2 * k] + e[2 * k + 1] * e[2 * k + 1]);
+   return err;
+}
+
+} // extern "C"

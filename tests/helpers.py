@@ -1,0 +1,37 @@
+"""Shared helpers of the test suite (fixture loading, scene construction, comparisons)."""
+import glob
+import os
+
+import numpy as np
+
+from v3dsfmtoolkit_b200 import scenes
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden_names():
+    return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_golden(name):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    sc = scenes.Scene(int(g["model"]), int(g["mode"]), float(g["inlier_threshold"]), g["K0"].copy(),
+                      g["R0"].copy(), g["T0"].copy(), g["X0"].copy(), g["meas"].copy(), g["view"].copy(),
+                      g["point"].copy(), g["dist0"].copy() if g["dist0"].size else None, name=name)
+    return sc, g
+
+
+def rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def param_rel(pa, pb):
+    """max relative difference over K, R, T, X (and distortion when present)."""
+    out = 0.0
+    for a, b in zip(pa, pb):
+        a, b = np.asarray(a), np.asarray(b)
+        if a.size == 0 or b.size == 0:
+            continue
+        out = max(out, rel(a, b))
+    return out

@@ -1,0 +1,159 @@
+"""Parity of the CUDA path (through the C-ABI) with the oracle: per-observation linearisation,
+the damped reduced system, the tile Cholesky, and full minimize() runs against the reference's
+own outputs (golden fixtures) and the restatement."""
+import numpy as np
+import pytest
+
+from oracle.bindings import Restatement
+from v3dsfmtoolkit_b200 import capi, scenes
+from tests.helpers import golden_names, load_golden, param_rel, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return Restatement()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_linearization_matches_reference(name):
+    sc, g = load_golden(name)
+    h = capi.Handle.from_scene(sc)
+    lin = h.linearize(capi.PRECISION_FP64)
+    n = g["e"].shape[0]
+    assert rel(lin["e"][:n], g["e"]) < 1e-12
+    np.testing.assert_allclose(lin["w"][:n], g["w"], rtol=1e-13, atol=0)
+    assert rel(lin["A"][:n], g["A"]) < 1e-12
+    assert rel(lin["B"][:n], g["B"]) < 1e-12
+    if sc.dims[1]:
+        assert rel(lin["C"][:n], g["C"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["std_circle", "common_rt", "varying_rt", "std_fixed"])
+def test_gradient_matches_oracle(orc, name):
+    sc, g = load_golden(name)
+    nv = tuple(int(v) for v in g["nonvarying"])
+    h = capi.Handle.from_scene(sc)
+    h.set_nonvarying(*nv)
+    lin = h.linearize(capi.PRECISION_FP64)
+    bl = orc.normal_blocks(sc, nonvarying=nv)
+    assert rel(lin["ga"], bl["ga"]) < 1e-11
+    assert rel(lin["gb"], bl["gb"]) < 1e-11
+    if sc.dims[1]:
+        assert rel(lin["gc"], bl["gc"]) < 1e-11
+
+
+@pytest.mark.parametrize("name", ["std_circle", "std_fixed", "common_rt", "common_focal", "varying_rt", "varying_pp"])
+@pytest.mark.parametrize("precision,tol", [(capi.PRECISION_FP64, 1e-10), (capi.PRECISION_MIXED, 2e-5)])
+def test_reduced_system_matches_oracle(orc, name, precision, tol):
+    sc, g = load_golden(name)
+    nv = tuple(int(v) for v in g["nonvarying"])
+    h = capi.Handle.from_scene(sc)
+    h.set_nonvarying(*nv)
+    bl = orc.normal_blocks(sc, nonvarying=nv)
+    lam = 1e-3 * max(np.diagonal(bl["U"], axis1=1, axis2=2).max(), 1.0)
+    S_ref, rhs_ref, _, fail = orc.reduced_system(sc, bl, lam, nonvarying=nv)
+    S, rhs = h.reduced_system(lam, precision)
+    assert rel(S, S_ref) < tol
+    assert rel(rhs, rhs_ref) < tol
+
+
+@pytest.mark.parametrize("n", [5, 64, 120, 200, 257])
+def test_tile_cholesky_solves_spd(n):
+    rng = np.random.default_rng(n)
+    A = rng.normal(size=(n, n))
+    S = A @ A.T + n * np.eye(n)
+    b = rng.normal(size=n)
+    x, fail = capi.dense_cholesky_solve(S, b)
+    assert not fail
+    assert rel(x, np.linalg.solve(S, b)) < 1e-10
+
+
+def test_tile_cholesky_reports_indefinite():
+    rng = np.random.default_rng(5)
+    A = rng.normal(size=(100, 100))
+    S = A @ A.T + np.eye(100)
+    S[70, 70] = -5.0
+    _, fail = capi.dense_cholesky_solve(S, np.ones(100))
+    assert fail
+
+
+def test_tile_cholesky_banded_pattern():
+    n = 400
+    rng = np.random.default_rng(9)
+    S = np.zeros((n, n))
+    for i in range(n):
+        for j in range(max(0, i - 20), i + 1):
+            S[i, j] = S[j, i] = rng.normal()
+    S += 50 * np.eye(n)
+    b = rng.normal(size=n)
+    x, fail = capi.dense_cholesky_solve(S, b)
+    assert not fail
+    assert rel(x, np.linalg.solve(S, b)) < 1e-10
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_minimize_fp64_matches_reference(name):
+    """FP64 mode follows the reference's LM path: same status, iterations and rejections."""
+    sc, g = load_golden(name)
+    nv = tuple(int(v) for v in g["nonvarying"])
+    h = capi.Handle.from_scene(sc)
+    h.set_nonvarying(*nv)
+    r = h.minimize(max_iterations=int(g["max_iterations"]), precision=capi.PRECISION_FP64)
+    assert r.status == int(g["status"])
+    assert r.iterations == int(g["iterations"])
+    assert r.n_rejected == int(g["n_rejected"])
+    K, R, T, dist, X = h.get_params()
+    assert abs(h.cost() - float(g["cost"])) <= 1e-8 * float(g["cost"])
+    assert param_rel((K, R, T, X), (g["K"], g["R"], g["T"], g["X"])) < 1e-5
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_minimize_mixed_reaches_reference_cost(name):
+    """Mixed precision (FP32 normal-equation blocks) takes a slightly different LM path; it must
+    reach the reference's final cost within 1e-6 relative (the time-to-reference-cost criterion)."""
+    sc, g = load_golden(name)
+    nv = tuple(int(v) for v in g["nonvarying"])
+    h = capi.Handle.from_scene(sc)
+    h.set_nonvarying(*nv)
+    target = float(g["cost"]) * (1 + 1e-6)
+    r = h.minimize(max_iterations=4 * int(g["max_iterations"]), precision=capi.PRECISION_MIXED, stop_cost=target)
+    assert h.cost() <= target or (r.status != capi.STATUS_TIMEOUT and abs(h.cost() - float(g["cost"])) <= 1e-6 * float(g["cost"]))
+
+
+@pytest.mark.parametrize("name", ["std_circle"])
+def test_minimize_mixed_converged_case_matches_reference(name):
+    """On a case the reference drives to SMALL_UPDATE, mixed precision ends with the same status,
+    the same cost (1e-6) and the same parameters (1e-5)."""
+    sc, g = load_golden(name)
+    h = capi.Handle.from_scene(sc)
+    r = h.minimize(max_iterations=int(g["max_iterations"]) * 2, precision=capi.PRECISION_MIXED)
+    assert r.status == int(g["status"])
+    assert abs(h.cost() - float(g["cost"])) <= 1e-6 * float(g["cost"])
+    K, R, T, dist, X = h.get_params()
+    assert param_rel((R, T, X), (g["R"], g["T"], g["X"])) < 1e-5
+
+
+def test_minimize_circle_fp64_parameters_match_reference_tightly():
+    sc, g = load_golden("std_circle")
+    h = capi.Handle.from_scene(sc)
+    r = h.minimize(max_iterations=int(g["max_iterations"]), precision=capi.PRECISION_FP64)
+    K, R, T, dist, X = h.get_params()
+    assert r.status == capi.STATUS_SMALL_UPDATE
+    assert param_rel((R, T, X), (g["R"], g["T"], g["X"])) < 1e-9
+
+
+def test_reset_and_repeat_are_deterministic():
+    sc = scenes.circle_scene(n_cams=8, n_points=300, seed=4)
+    h = capi.Handle.from_scene(sc)
+    r1 = h.minimize(max_iterations=15)
+    p1 = h.get_params()
+    h2 = capi.Handle.from_scene(sc)
+    r2 = h2.minimize(max_iterations=15)
+    p2 = h2.get_params()
+    h.reset_params()
+    np.testing.assert_array_equal(h.get_params()[4], sc.X)
+    assert r1.iterations == r2.iterations and r1.cost == r2.cost
+    for a, b in zip(p1, p2):
+        assert np.array_equal(a, b)

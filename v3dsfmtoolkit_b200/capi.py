@@ -1,0 +1,233 @@
+"""ctypes binding of the C-ABI in ``include/v3dba.h`` (``_lib/libv3dba.so``).
+
+There is no CPU fallback: when the CUDA library is missing, or no GPU is present, the calls
+raise.  Build the library with ``python -m v3dsfmtoolkit_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "_lib", "libv3dba.so")
+
+OK = 0
+ERR_INVALID_ARGUMENT, ERR_INVALID_INPUT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NO_DEVICE, ERR_UNSUPPORTED, ERR_TIMEOUT = range(1, 8)
+STATUS_TIMEOUT, STATUS_SMALL_UPDATE, STATUS_CONVERGED = 0, 1, 2
+PRECISION_MIXED, PRECISION_FP64 = 0, 1
+SOLVER_AUTO, SOLVER_CHOLESKY, SOLVER_PCG = 0, 1, 2
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+# every symbol include/v3dba.h declares
+EXPORTS = (
+    "v3dba_default_options", "v3dba_create", "v3dba_destroy", "v3dba_set_nonvarying",
+    "v3dba_set_lambda", "v3dba_minimize", "v3dba_set_params", "v3dba_get_params",
+    "v3dba_reset_params", "v3dba_cost", "v3dba_linearize", "v3dba_reduced_system", "v3dba_dims",
+    "v3dba_dense_cholesky_solve", "v3dba_minimize_batched", "v3dba_launch_count",
+    "v3dba_error_string", "v3dba_profile_stages",
+)
+STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
+          "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
+          "trial_cost", "trial_finalize", "cholesky", "zero")
+
+
+class Problem(C.Structure):
+    _fields_ = [("model", C.c_int), ("mode", C.c_int), ("n_cameras", C.c_int), ("n_points", C.c_int),
+                ("n_measurements", C.c_int), ("inlier_threshold", C.c_double), ("K", _dp), ("R", _dp),
+                ("T", _dp), ("dist", _dp), ("X", _dp), ("measurements", _dp), ("view", _ip), ("point", _ip)]
+
+
+class Options(C.Structure):
+    _fields_ = [("tau", C.c_double), ("max_iterations", C.c_int), ("gradient_threshold", C.c_double),
+                ("update_threshold", C.c_double), ("verbosity", C.c_int), ("precision", C.c_int),
+                ("solver", C.c_int), ("pcg_tolerance", C.c_double), ("pcg_max_iterations", C.c_int),
+                ("stop_cost", C.c_double), ("mixed_escalation", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("n_relinearizations", C.c_int),
+                ("n_rejected", C.c_int), ("initial_cost", C.c_double), ("cost", C.c_double),
+                ("lambda_", C.c_double), ("device_ms", C.c_double), ("pcg_iterations", C.c_int),
+                ("reached_stop_cost", C.c_int), ("fp64_from_iteration", C.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class V3dbaError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        msg = _lib().v3dba_error_string(code).decode() if _LIB is not None else str(code)
+        super().__init__(f"{what}: {msg} (code {code})" if what else f"{msg} (code {code})")
+
+
+_LIB = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"CUDA library not built: {LIB_PATH} (python -m v3dsfmtoolkit_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        L.v3dba_default_options.argtypes = [C.POINTER(Options)]
+        L.v3dba_default_options.restype = None
+        L.v3dba_create.argtypes = [C.POINTER(Problem), C.POINTER(C.c_void_p)]
+        L.v3dba_destroy.argtypes = [C.c_void_p]
+        L.v3dba_set_nonvarying.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.v3dba_set_lambda.argtypes = [C.c_void_p, C.c_double]
+        L.v3dba_minimize.argtypes = [C.c_void_p, C.POINTER(Options), C.POINTER(Result)]
+        L.v3dba_set_params.argtypes = [C.c_void_p] + [_dp] * 5
+        L.v3dba_get_params.argtypes = [C.c_void_p] + [_dp] * 5
+        L.v3dba_reset_params.argtypes = [C.c_void_p]
+        L.v3dba_cost.argtypes = [C.c_void_p, _dp]
+        L.v3dba_linearize.argtypes = [C.c_void_p, C.c_int] + [_dp] * 8
+        L.v3dba_reduced_system.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
+        L.v3dba_dims.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.v3dba_dense_cholesky_solve.argtypes = [C.c_int, _dp, _dp, _dp, C.POINTER(C.c_int)]
+        L.v3dba_minimize_batched.argtypes = [C.POINTER(Problem), C.c_int, C.POINTER(Options)] + \
+            [C.POINTER(_dp)] * 5 + [C.POINTER(Result)]
+        L.v3dba_profile_stages.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+        L.v3dba_launch_count.restype = C.c_uint64
+        L.v3dba_launch_count.argtypes = []
+        L.v3dba_error_string.restype = C.c_char_p
+        L.v3dba_error_string.argtypes = [C.c_int]
+        _LIB = L
+    return _LIB
+
+
+def library():
+    """The loaded CDLL (raises if the library is missing)."""
+    return _lib()
+
+
+def check(rc, what=""):
+    if rc != OK:
+        raise V3dbaError(rc, what)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    _lib().v3dba_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def dims(model, mode):
+    a, c = C.c_int(), C.c_int()
+    check(_lib().v3dba_dims(model, mode, C.byref(a), C.byref(c)), "v3dba_dims")
+    return a.value, c.value
+
+
+def launch_count() -> int:
+    return int(_lib().v3dba_launch_count())
+
+
+class Handle:
+    """One problem resident on the GPU (wraps v3dba_create / v3dba_destroy)."""
+
+    def __init__(self, model, mode, inlier_threshold, K, R, T, dist, X, measurements, view, point):
+        L = _lib()
+        self._keep = [_f64(K), _f64(R), _f64(T), _f64(dist if dist is not None else np.zeros(4)), _f64(X),
+                      _f64(measurements), np.ascontiguousarray(view, dtype=np.int32),
+                      np.ascontiguousarray(point, dtype=np.int32)]
+        K_, R_, T_, d_, X_, m_, v_, p_ = self._keep
+        self.model, self.mode = int(model), int(mode)
+        self.n_cams, self.n_points, self.n_obs = R_.size // 9, X_.size // 3, v_.size
+        self.shapes = (K_.shape, R_.shape, T_.shape, d_.shape, X_.shape)
+        prob = Problem(self.model, self.mode, self.n_cams, self.n_points, self.n_obs, float(inlier_threshold),
+                       _d(K_), _d(R_), _d(T_), _d(d_), _d(X_), _d(m_), v_.ctypes.data_as(_ip), p_.ctypes.data_as(_ip))
+        h = C.c_void_p()
+        check(L.v3dba_create(C.byref(prob), C.byref(h)), "v3dba_create")
+        self.h = h
+        self.dA, self.dC = dims(self.model, self.mode)
+
+    @classmethod
+    def from_scene(cls, sc):
+        return cls(sc.model, sc.mode, sc.inlier_threshold, sc.K, sc.R, sc.T, sc.dist, sc.X, sc.meas, sc.view, sc.point)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            _lib().v3dba_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_nonvarying(self, a, b, c):
+        check(_lib().v3dba_set_nonvarying(self.h, a, b, c), "v3dba_set_nonvarying")
+
+    def set_lambda(self, lam):
+        check(_lib().v3dba_set_lambda(self.h, lam), "v3dba_set_lambda")
+
+    def minimize(self, options: Options | None = None, **kw) -> Result:
+        o = options if options is not None else default_options(**kw)
+        if options is not None:
+            for k, v in kw.items():
+                setattr(o, k, v)
+        r = Result()
+        check(_lib().v3dba_minimize(self.h, C.byref(o), C.byref(r)), "v3dba_minimize")
+        return r
+
+    def get_params(self):
+        out = [np.zeros(s) for s in self.shapes]
+        check(_lib().v3dba_get_params(self.h, *[_d(a) for a in out]), "v3dba_get_params")
+        return tuple(out)
+
+    def set_params(self, K, R, T, dist, X):
+        arrs = [_f64(K), _f64(R), _f64(T), _f64(dist if dist is not None else np.zeros(4)), _f64(X)]
+        check(_lib().v3dba_set_params(self.h, *[_d(a) for a in arrs]), "v3dba_set_params")
+
+    def reset_params(self):
+        check(_lib().v3dba_reset_params(self.h), "v3dba_reset_params")
+
+    def cost(self) -> float:
+        c = C.c_double()
+        check(_lib().v3dba_cost(self.h, C.byref(c)), "v3dba_cost")
+        return c.value
+
+    def linearize(self, precision=PRECISION_FP64):
+        n, dA, dC = self.n_obs, self.dA, self.dC
+        e, w = np.zeros((n, 2)), np.zeros(n)
+        A, B, Cm = np.zeros((n, 2, dA)), np.zeros((n, 2, 3)), np.zeros((n, 2, max(dC, 1)))
+        ga, gb, gc = np.zeros((self.n_cams, dA)), np.zeros((self.n_points, 3)), np.zeros(max(dC, 1))
+        check(_lib().v3dba_linearize(self.h, precision, _d(e), _d(w), _d(A), _d(B), _d(Cm), _d(ga), _d(gb), _d(gc)),
+              "v3dba_linearize")
+        return dict(e=e, w=w, A=A, B=B, C=Cm[..., :dC], ga=ga, gb=gb, gc=gc[:dC])
+
+    def profile_stages(self, precision=PRECISION_MIXED, reps=20):
+        ms = np.zeros(len(STAGES))
+        check(_lib().v3dba_profile_stages(self.h, precision, reps, _d(ms)), "v3dba_profile_stages")
+        return dict(zip(STAGES, ms.tolist()))
+
+    def reduced_system(self, lam, precision=PRECISION_FP64):
+        n = self.n_cams * self.dA + self.dC
+        S, rhs = np.zeros((n, n)), np.zeros(n)
+        check(_lib().v3dba_reduced_system(self.h, precision, float(lam), _d(S), _d(rhs)), "v3dba_reduced_system")
+        return S, rhs
+
+
+def dense_cholesky_solve(S, rhs):
+    S = _f64(S)
+    rhs = _f64(rhs)
+    x = np.zeros_like(rhs)
+    fail = C.c_int()
+    check(_lib().v3dba_dense_cholesky_solve(S.shape[0], _d(S), _d(rhs), _d(x), C.byref(fail)),
+          "v3dba_dense_cholesky_solve")
+    return x, bool(fail.value)

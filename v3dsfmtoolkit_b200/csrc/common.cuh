@@ -1,0 +1,83 @@
+// Shared device/host helpers of the B200 bundle adjuster.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "v3dba.h"
+
+namespace v3dba {
+
+// Counts every kernel launch issued by this library (reported by v3dba_launch_count()).
+void note_launches(uint64_t n);
+
+#define V3DBA_CUDA_TRY(expr)                                                        \
+  do {                                                                              \
+    cudaError_t _e = (expr);                                                        \
+    if (_e != cudaSuccess) {                                                        \
+      fprintf(stderr, "v3dba: %s failed: %s (%s:%d)\n", #expr, cudaGetErrorString(_e), \
+              __FILE__, __LINE__);                                                  \
+      return _e == cudaErrorMemoryAllocation ? V3DBA_ERR_OUT_OF_MEMORY : V3DBA_ERR_CUDA; \
+    }                                                                               \
+  } while (0)
+
+#define V3DBA_LAUNCH_CHECK()                                                        \
+  do {                                                                              \
+    ::v3dba::note_launches(1);                                                      \
+    cudaError_t _e = cudaPeekAtLastError();                                         \
+    if (_e != cudaSuccess) {                                                        \
+      fprintf(stderr, "v3dba: launch failed: %s (%s:%d)\n", cudaGetErrorString(_e), \
+              __FILE__, __LINE__);                                                  \
+      return V3DBA_ERR_CUDA;                                                        \
+    }                                                                               \
+  } while (0)
+
+constexpr int kWarp = 32;
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T u = __shfl_xor_sync(0xffffffffu, v, o);
+    v = u > v ? u : v;
+  }
+  return v;
+}
+
+// Deterministic block-wide reduction of NV values (first NS summed, the rest max-reduced),
+// result valid in thread 0.  smem needs blockDim.x/32 * NV doubles.
+template <int NV, int NS>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], double* smem) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int t = 0; t < NV; ++t) v[t] = (t < NS) ? warp_sum(v[t]) : warp_max(v[t]);
+  if (lane == 0) {
+#pragma unroll
+    for (int t = 0; t < NV; ++t) smem[wid * NV + t] = v[t];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < nw; ++w) {
+#pragma unroll
+      for (int t = 0; t < NV; ++t) {
+        double u = smem[w * NV + t];
+        v[t] = (t < NS) ? v[t] + u : (u > v[t] ? u : v[t]);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Real-valued storage type of the normal-equation blocks.
+template <typename Real>
+__device__ __forceinline__ Real to_real(double x) { return static_cast<Real>(x); }
+
+}  // namespace v3dba

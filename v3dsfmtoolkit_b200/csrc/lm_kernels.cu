@@ -1,0 +1,1059 @@
+// LM kernels of the B200 bundle adjuster: linearisation, point elimination (Schur complement),
+// back-substitution, parameter update and cost.  See lm.cuh for the data layout.
+//
+// The arithmetic restates V3D/src/Math/v3d_optimization.cpp:784-1187 (weighting, J^T e, the
+// U/V/W/X/Y/Z blocks, damping, update, cost with the old weights) on a point-eliminated system.
+// Residuals, weights, gradient and cost are FP64.  The normal-equation blocks are stored in
+// `Real` (float in mixed mode, double in FP64 mode); their sums are taken in FP64, except the
+// camera-pair Schur sums of the mixed mode, which accumulate in FP32.  All reductions run in a
+// fixed order (no floating-point atomics), so results are bit-reproducible run to run.
+#include <algorithm>
+#include <cstdio>
+
+#include "common.cuh"
+#include "lm.cuh"
+#include "model.cuh"
+
+namespace v3dba {
+
+// ---- layout ---------------------------------------------------------------------------------
+
+__host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
+__host__ __device__ constexpr int nsym(int n) { return n * (n + 1) / 2; }
+
+template <int DA, int DC>
+struct Lay {
+  static constexpr int DCc = DC > 0 ? DC : 1;
+  static constexpr int SA = round4(2 * DA);      // A_k, Real
+  static constexpr int SW = round4(3 * DA);      // W_k / T_k, Real
+  static constexpr int SC = round4(2 * DCc);     // C_k, Real
+  static constexpr int SG = (DA + 1) & ~1;       // A_k^T r_k, double
+  static constexpr int SV = 8;                   // V_j / Vinv_j upper triangle, Real
+  static constexpr int SY = round4(3 * DCc);     // Y_j / Vinv_j Y_j, Real
+  static constexpr int SU = round4(DA * DA);     // U_i, Real
+  static constexpr int SX = round4(DA * DCc);    // X_i, Real
+  static constexpr int NZ = nsym(DC);
+};
+
+// symmetric 3x3 index of the packed upper triangle (00,01,02,11,12,22)
+__device__ __forceinline__ int s3(int r, int c) {
+  const int a = r < c ? r : c, b = r < c ? c : r;
+  return a == 0 ? b : (a == 1 ? 2 + b : 5);
+}
+
+template <int N>
+__device__ __forceinline__ void vload(const float* __restrict__ p, float (&v)[N]) {
+  static_assert(N % 4 == 0, "float vectors are loaded 4 at a time");
+  const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int t = 0; t < N / 4; ++t) {
+    const float4 u = __ldg(q + t);
+    v[4 * t] = u.x; v[4 * t + 1] = u.y; v[4 * t + 2] = u.z; v[4 * t + 3] = u.w;
+  }
+}
+template <int N>
+__device__ __forceinline__ void vload(const double* __restrict__ p, double (&v)[N]) {
+  static_assert(N % 2 == 0, "double vectors are loaded 2 at a time");
+  const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int t = 0; t < N / 2; ++t) {
+    const double2 u = __ldg(q + t);
+    v[2 * t] = u.x; v[2 * t + 1] = u.y;
+  }
+}
+template <int N>
+__device__ __forceinline__ void vstore(float* p, const float (&v)[N]) {
+  float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+  for (int t = 0; t < N / 4; ++t) q[t] = make_float4(v[4 * t], v[4 * t + 1], v[4 * t + 2], v[4 * t + 3]);
+}
+template <int N>
+__device__ __forceinline__ void vstore(double* p, const double (&v)[N]) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int t = 0; t < N / 2; ++t) q[t] = make_double2(v[2 * t], v[2 * t + 1]);
+}
+
+// Deterministically folds `nblk` rows of NV partials (first NS summed, the rest maxed) with
+// one block; result in out[0..NV) of thread 0.
+template <int NV, int NS>
+__device__ void fold_partials(const double* __restrict__ part, int nblk, double (&out)[NV], double* smem) {
+#pragma unroll
+  for (int t = 0; t < NV; ++t) out[t] = (t < NS) ? 0.0 : -1e30;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+#pragma unroll
+    for (int t = 0; t < NV; ++t) {
+      const double u = part[(size_t)b * NV + t];
+      out[t] = (t < NS) ? out[t] + u : fmax(out[t], u);
+    }
+  }
+  block_reduce<NV, NS>(out, smem);
+}
+
+// Warp-wide sum of V values (V a multiple of 32) by recursive halving: each of the five
+// butterfly stages exchanges half of the remaining values, V - V/32 shuffles in total instead
+// of 5V.  Afterwards lane L holds the totals of values [L*V/32, (L+1)*V/32) in v[0 .. V/32).
+template <int H, typename T, int V>
+__device__ __forceinline__ void rt_stage(T (&v)[V], int lane, int m) {
+#pragma unroll
+  for (int t = 0; t < H; ++t) {
+    const bool up = (lane & m) != 0;
+    const T send = up ? v[t] : v[t + H];
+    const T keep = up ? v[t + H] : v[t];
+    v[t] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+  }
+}
+template <int V, typename T>
+__device__ __forceinline__ void warp_reduce_transpose(T (&v)[V]) {
+  static_assert(V % 32 == 0, "pad the value count to a multiple of 32");
+  const int lane = threadIdx.x & 31;
+  rt_stage<V / 2>(v, lane, 16);
+  rt_stage<V / 4>(v, lane, 8);
+  rt_stage<V / 8>(v, lane, 4);
+  rt_stage<V / 16>(v, lane, 2);
+  rt_stage<V / 32>(v, lane, 1);
+}
+
+__host__ __device__ constexpr int round32(int x) { return (x + 31) & ~31; }
+
+// value layout of the per-camera sums: U (packed upper triangle), ga, X
+template <int DA, int DC>
+struct CamV {
+  static constexpr int NU = nsym(DA);
+  static constexpr int NX = DC > 0 ? DA * DC : 0;
+  static constexpr int NV = NU + DA + NX;
+  static constexpr int VP = round32(NV);
+};
+// value layout of the per-camera reduced rhs / border sums: W q, T Y
+template <int DA, int DC>
+struct RhsV {
+  static constexpr int NX = DC > 0 ? DA * DC : 0;
+  static constexpr int NV = DA + NX;
+  static constexpr int VP = round32(NV);
+};
+template <int DA>
+struct SchurV {
+  static constexpr int NV = DA * DA;
+  static constexpr int VP = round32(NV);
+};
+
+// row / column of the packed upper-triangle index u of a DA x DA matrix
+template <int DA>
+__device__ __forceinline__ void unpack_sym(int u, int& r, int& c) {
+  r = 0;
+  int start = 0;
+  while (u >= start + (DA - r)) { start += DA - r; ++r; }
+  c = r + (u - start);
+}
+
+// ---- relinearisation --------------------------------------------------------------------
+
+constexpr int kPtThreads = 128;
+constexpr int kCamWarps = 4;
+
+template <int DC>
+struct RelinNV {
+  static constexpr int NZ = nsym(DC);
+  static constexpr int NS = 1 + NZ + DC;   // cost, Z (packed), gc
+  static constexpr int NV = NS + 2;        // + max |gb|, max diag V
+};
+
+// One thread per point: linearise every observation of its track (FP64), store the weighted
+// blocks, and accumulate V_j, gb_j, Y_j; Z, gc and the cost go to per-block partials.
+template <int MODEL, int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __restrict__ part) {
+  using L = Lay<DA, DC>;
+  constexpr int DCc = L::DCc;
+  constexpr int NS = RelinNV<DC>::NS, NV = RelinNV<DC>::NV, NZ = L::NZ;
+  __shared__ double red[(kPtThreads / 32) * NV];
+  const Dims& D = s.d;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[NV];
+#pragma unroll
+  for (int t = 0; t < NV; ++t) v[t] = (t < NS) ? 0.0 : -1e30;
+
+  if (j < D.M) {
+    const bool fixB = j < D.nnB;
+    const double X[3] = {s.cur.X[3 * j], s.cur.X[3 * j + 1], s.cur.X[3 * j + 2]};
+    double V[6] = {0, 0, 0, 0, 0, 0}, gb[3] = {0, 0, 0}, Y[3][DCc];
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < DCc; ++c) Y[b][c] = 0.0;
+    Real* oA = reinterpret_cast<Real*>(s.o_A);
+    Real* oW = reinterpret_cast<Real*>(s.o_W);
+    Real* oC = reinterpret_cast<Real*>(s.o_C);
+    const int k0 = s.p_ptr[j], k1 = s.p_ptr[j + 1];
+    for (int k = k0; k < k1; ++k) {
+      const int i = s.o_cam[k];
+      const bool fixA = i < D.nnA;
+      Cam cam;
+      load_cam<MODEL>(cam, s.cur.R, s.cur.T, s.cur.K, s.cur.dist, i);
+      double e[2], A[2][DA], B[2][3], C[2][DCc];
+      linearize_obs<MODEL, DA, DC>(cam, X, s.o_meas[2 * k], s.o_meas[2 * k + 1], D.mode, D.cached_ar, e, A, B, C);
+      const double w = huber_weight(D.thr, e);
+      s.o_w[k] = w;
+      v[0] += w * w * (e[0] * e[0] + e[1] * e[1]);
+      const double r0 = -w * e[0], r1 = -w * e[1];
+      const double wa = fixA ? 0.0 : w, wb = fixB ? 0.0 : w;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+#pragma unroll
+        for (int q = 0; q < DA; ++q) A[r][q] *= wa;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) B[r][q] *= wb;
+#pragma unroll
+        for (int q = 0; q < DCc; ++q) C[r][q] = (DC > 0 && q >= D.nnC) ? C[r][q] * w : 0.0;
+      }
+      // per-observation blocks
+      {
+        Real a[L::SA];
+#pragma unroll
+        for (int t = 0; t < L::SA; ++t) a[t] = Real(0);
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+          for (int q = 0; q < DA; ++q) a[r * DA + q] = Real(A[r][q]);
+        vstore(oA + (size_t)k * L::SA, a);
+        Real wv[L::SW];
+#pragma unroll
+        for (int t = 0; t < L::SW; ++t) wv[t] = Real(0);
+#pragma unroll
+        for (int q = 0; q < DA; ++q)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) wv[q * 3 + b] = Real(A[0][q] * B[0][b] + A[1][q] * B[1][b]);
+        vstore(oW + (size_t)k * L::SW, wv);
+        if (DC > 0) {
+          Real cv[L::SC];
+#pragma unroll
+          for (int t = 0; t < L::SC; ++t) cv[t] = Real(0);
+#pragma unroll
+          for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int q = 0; q < DCc; ++q) cv[r * DCc + q] = Real(C[r][q]);
+          vstore(oC + (size_t)k * L::SC, cv);
+        }
+        double g[L::SG];
+#pragma unroll
+        for (int t = 0; t < L::SG; ++t) g[t] = 0.0;
+#pragma unroll
+        for (int q = 0; q < DA; ++q) g[q] = A[0][q] * r0 + A[1][q] * r1;
+        vstore(s.o_ga + (size_t)k * L::SG, g);
+      }
+      // point sums
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = r; c < 3; ++c) V[s3(r, c)] += B[0][r] * B[0][c] + B[1][r] * B[1][c];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        gb[b] += B[0][b] * r0 + B[1][b] * r1;
+#pragma unroll
+        for (int c = 0; c < DCc; ++c) Y[b][c] += B[0][b] * C[0][c] + B[1][b] * C[1][c];
+      }
+      if (DC > 0) {
+        int z = 0;
+#pragma unroll
+        for (int r = 0; r < DCc; ++r)
+#pragma unroll
+          for (int c = r; c < DCc; ++c) v[1 + z++] += C[0][r] * C[0][c] + C[1][r] * C[1][c];
+#pragma unroll
+        for (int c = 0; c < DCc; ++c) v[1 + NZ + c] += C[0][c] * r0 + C[1][c] * r1;
+      }
+    }
+    Real* pV = reinterpret_cast<Real*>(s.p_V) + (size_t)j * L::SV;
+    Real vv[L::SV];
+#pragma unroll
+    for (int t = 0; t < L::SV; ++t) vv[t] = t < 6 ? Real(V[t]) : Real(0);
+    vstore(reinterpret_cast<Real*>(s.p_V) + (size_t)j * L::SV, vv);
+    (void)pV;
+    double g4[4] = {gb[0], gb[1], gb[2], 0.0};
+    vstore(s.p_gb + (size_t)j * 4, g4);
+    if (DC > 0) {
+      Real yv[L::SY];
+#pragma unroll
+      for (int t = 0; t < L::SY; ++t) yv[t] = Real(0);
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < DCc; ++c) yv[b * DCc + c] = Real(Y[b][c]);
+      vstore(reinterpret_cast<Real*>(s.p_Y) + (size_t)j * L::SY, yv);
+    }
+    if (!fixB && k1 > k0) {
+      v[NS] = fmax(fabs(gb[0]), fmax(fabs(gb[1]), fabs(gb[2])));
+      v[NS + 1] = fmax(V[0], fmax(V[3], V[5]));
+    } else if (!fixB) {
+      v[NS] = 0.0;
+      v[NS + 1] = 0.0;
+    }
+  }
+  block_reduce<NV, NS>(v, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int t = 0; t < NV; ++t) part[(size_t)blockIdx.x * NV + t] = v[t];
+  }
+}
+
+// One warp per chunk of a camera's observation list: partial U = sum A^T A, ga = sum A^T r,
+// X = sum A^T C (FP64 sums); the partials of a camera are folded in chunk order afterwards.
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kCamWarps * 32) k_camera_chunks(DevState s, double* __restrict__ part) {
+  using L = Lay<DA, DC>;
+  using CV = CamV<DA, DC>;
+  constexpr int DCc = L::DCc;
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * kCamWarps + (threadIdx.x >> 5);
+  if (ch >= s.nch_cam) return;
+  double acc[CV::VP];
+#pragma unroll
+  for (int t = 0; t < CV::VP; ++t) acc[t] = 0.0;
+  const Real* oA = reinterpret_cast<const Real*>(s.o_A);
+  const Real* oC = reinterpret_cast<const Real*>(s.o_C);
+  for (int idx = s.cc_beg[ch] + lane; idx < s.cc_end[ch]; idx += 32) {
+    const int k = s.c_obs[idx];
+    Real a[L::SA];
+    vload(oA + (size_t)k * L::SA, a);
+    double g[L::SG];
+    vload(s.o_ga + (size_t)k * L::SG, g);
+    int u = 0;
+#pragma unroll
+    for (int r = 0; r < DA; ++r) {
+      acc[CV::NU + r] += g[r];
+#pragma unroll
+      for (int c = r; c < DA; ++c)
+        acc[u++] += double(a[r]) * double(a[c]) + double(a[DA + r]) * double(a[DA + c]);
+    }
+    if (DC > 0) {
+      Real cv[L::SC];
+      vload(oC + (size_t)k * L::SC, cv);
+#pragma unroll
+      for (int r = 0; r < DA; ++r)
+#pragma unroll
+        for (int c = 0; c < DCc; ++c)
+          acc[CV::NU + DA + r * DCc + c] += double(a[r]) * double(cv[c]) + double(a[DA + r]) * double(cv[DCc + c]);
+    }
+  }
+  warp_reduce_transpose(acc);
+#pragma unroll
+  for (int t = 0; t < CV::VP / 32; ++t) part[(size_t)ch * CV::VP + lane * (CV::VP / 32) + t] = acc[t];
+}
+
+// One warp per camera: folds its chunk partials in order and stores U_i, ga_i, X_i; gradient
+// max and max diagonal of the varying cameras go to per-block partials.
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kCamWarps * 32) k_camera_finish(DevState s, const double* __restrict__ cpart,
+                                                                   double* __restrict__ part) {
+  using L = Lay<DA, DC>;
+  using CV = CamV<DA, DC>;
+  constexpr int DCc = L::DCc;
+  constexpr int PER = CV::VP / 32;
+  __shared__ double red[kCamWarps * 2];
+  const Dims& D = s.d;
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kCamWarps + (threadIdx.x >> 5);
+  double v[2] = {-1e30, -1e30};
+  if (i < D.N) {
+    double sum[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) sum[t] = 0.0;
+    for (int ch = s.cam_cc_ptr[i]; ch < s.cam_cc_ptr[i + 1]; ++ch)
+#pragma unroll
+      for (int t = 0; t < PER; ++t) sum[t] += cpart[(size_t)ch * CV::VP + lane + 32 * t];
+    Real* cU = reinterpret_cast<Real*>(s.c_U) + (size_t)i * L::SU;
+    Real* cX = reinterpret_cast<Real*>(s.c_X) + (size_t)i * L::SX;
+    double gm = 0.0, dm = -1e30;
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+      const int vi = lane + 32 * t;
+      if (vi < CV::NU) {
+        int r, c;
+        unpack_sym<DA>(vi, r, c);
+        cU[r * DA + c] = Real(sum[t]);
+        cU[c * DA + r] = Real(sum[t]);
+        if (r == c) dm = fmax(dm, sum[t]);
+      } else if (vi < CV::NU + DA) {
+        s.c_ga[(size_t)i * L::SG + (vi - CV::NU)] = sum[t];
+        gm = fmax(gm, fabs(sum[t]));
+      } else if (vi < CV::NV) {
+        const int x = vi - CV::NU - DA;
+        cX[(x / DCc) * DCc + x % DCc] = Real(sum[t]);
+      }
+    }
+    gm = warp_max(gm);
+    dm = warp_max(dm);
+    if (i >= D.nnA) {
+      v[0] = gm;
+      v[1] = dm;
+    }
+  }
+  block_reduce<2, 0>(v, red);
+  if (threadIdx.x == 0) {
+    part[(size_t)blockIdx.x * 2] = v[0];
+    part[(size_t)blockIdx.x * 2 + 1] = v[1];
+  }
+}
+
+// Sums the relinearisation partials: cost, Z, gc, gradient max, max diagonal, initial lambda.
+template <int DC>
+__global__ void __launch_bounds__(256) k_relin_finalize(DevState s, const double* __restrict__ part_pt, int nbp,
+                                                        const double* __restrict__ part_cam, int nbc,
+                                                        int init_lambda, double tau) {
+  constexpr int NS = RelinNV<DC>::NS, NV = RelinNV<DC>::NV, NZ = nsym(DC);
+  constexpr int DCc = DC > 0 ? DC : 1;
+  __shared__ double red[8 * (NV > 2 ? NV : 2)];
+  double a[NV];
+  fold_partials<NV, NS>(part_pt, nbp, a, red);
+  double b[2];
+  fold_partials<2, 0>(part_cam, nbc, b, red);
+  if (threadIdx.x == 0) {
+    const Dims& D = s.d;
+    double gmax = fmax(fmax(a[NS], b[0]), 0.0);
+    double dmax = fmax(a[NS + 1], b[1]);
+    if (DC > 0) {
+      int z = 0;
+      for (int r = 0; r < DCc; ++r)
+        for (int c = r; c < DCc; ++c, ++z) {
+          s.g_Z[r * DCc + c] = a[1 + z];
+          s.g_Z[c * DCc + r] = a[1 + z];
+          if (r == c && r >= D.nnC) dmax = fmax(dmax, a[1 + z]);
+        }
+      for (int c = 0; c < DCc; ++c) {
+        s.g_gc[c] = a[1 + NZ + c];
+        if (c >= D.nnC) gmax = fmax(gmax, fabs(a[1 + NZ + c]));
+      }
+    }
+    s.d_relin[0] = a[0];
+    s.d_relin[1] = gmax;
+    s.d_relin[2] = dmax;
+    if (init_lambda) *s.d_lambda = tau * dmax;
+  }
+}
+
+// ---- reduced system ---------------------------------------------------------------------
+
+template <int DC>
+struct ElimNV {
+  static constexpr int NZ = nsym(DC);
+  static constexpr int NV = (DC > 0) ? NZ + DC : 1;
+};
+
+__device__ __forceinline__ bool inv3(const double a[6], double o[6]) {
+  // inverse of the symmetric matrix [[a0,a1,a2],[a1,a3,a4],[a2,a4,a5]] by cofactors
+  const double c00 = a[3] * a[5] - a[4] * a[4];
+  const double c01 = a[2] * a[4] - a[1] * a[5];
+  const double c02 = a[1] * a[4] - a[2] * a[3];
+  const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+  if (!(det != 0.0) || !isfinite(det)) return false;
+  const double id = 1.0 / det;
+  o[0] = c00 * id;
+  o[1] = c01 * id;
+  o[2] = c02 * id;
+  o[3] = (a[0] * a[5] - a[2] * a[2]) * id;
+  o[4] = (a[1] * a[2] - a[0] * a[4]) * id;
+  o[5] = (a[0] * a[3] - a[1] * a[1]) * id;
+  return true;
+}
+
+// One thread per point: Vinv_j = (V_j + lambda I)^-1, q_j = Vinv gb, Vinv Y_j and
+// T_k = W_k Vinv_j for its observations; Y^T Vinv Y and Y^T q go to per-block partials.
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, double* __restrict__ part) {
+  using L = Lay<DA, DC>;
+  constexpr int DCc = L::DCc;
+  constexpr int NV = ElimNV<DC>::NV;
+  __shared__ double red[(kPtThreads / 32) * NV];
+  const Dims& D = s.d;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[NV];
+#pragma unroll
+  for (int t = 0; t < NV; ++t) v[t] = 0.0;
+  if (j < D.M) {
+    const double lam = *s.d_lambda;
+    Real vv[L::SV];
+    vload(reinterpret_cast<const Real*>(s.p_V) + (size_t)j * L::SV, vv);
+    double a[6] = {double(vv[0]) + lam, double(vv[1]), double(vv[2]), double(vv[3]) + lam, double(vv[4]),
+                   double(vv[5]) + lam};
+    double vi[6] = {0, 0, 0, 0, 0, 0};
+    const bool fixB = j < D.nnB;
+    if (!fixB && !inv3(a, vi)) {
+      *s.d_fail = 1;
+      vi[0] = vi[1] = vi[2] = vi[3] = vi[4] = vi[5] = 0.0;
+    }
+    Real vo[L::SV];
+#pragma unroll
+    for (int t = 0; t < L::SV; ++t) vo[t] = t < 6 ? Real(vi[t]) : Real(0);
+    vstore(reinterpret_cast<Real*>(s.p_Vinv) + (size_t)j * L::SV, vo);
+    double gb[4];
+    vload(s.p_gb + (size_t)j * 4, gb);
+    double q[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) q[r] = vi[s3(r, 0)] * gb[0] + vi[s3(r, 1)] * gb[1] + vi[s3(r, 2)] * gb[2];
+    vstore(s.p_q + (size_t)j * 4, q);
+    if (DC > 0) {
+      Real yv[L::SY];
+      vload(reinterpret_cast<const Real*>(s.p_Y) + (size_t)j * L::SY, yv);
+      double YV[3][DCc];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < DCc; ++c)
+          YV[r][c] = vi[s3(r, 0)] * double(yv[c]) + vi[s3(r, 1)] * double(yv[DCc + c]) + vi[s3(r, 2)] * double(yv[2 * DCc + c]);
+      Real yo[L::SY];
+#pragma unroll
+      for (int t = 0; t < L::SY; ++t) yo[t] = Real(0);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < DCc; ++c) yo[r * DCc + c] = Real(YV[r][c]);
+      vstore(reinterpret_cast<Real*>(s.p_YV) + (size_t)j * L::SY, yo);
+      int z = 0;
+#pragma unroll
+      for (int r = 0; r < DCc; ++r)
+#pragma unroll
+        for (int c = r; c < DCc; ++c, ++z)
+          v[z] = double(yv[r]) * YV[0][c] + double(yv[DCc + r]) * YV[1][c] + double(yv[2 * DCc + r]) * YV[2][c];
+#pragma unroll
+      for (int c = 0; c < DCc; ++c)
+        v[nsym(DC) + c] = double(yv[c]) * q[0] + double(yv[DCc + c]) * q[1] + double(yv[2 * DCc + c]) * q[2];
+    }
+    const Real* oW = reinterpret_cast<const Real*>(s.o_W);
+    Real* oT = reinterpret_cast<Real*>(s.o_T);
+    for (int k = s.p_ptr[j]; k < s.p_ptr[j + 1]; ++k) {
+      Real w[L::SW];
+      vload(oW + (size_t)k * L::SW, w);
+      Real t[L::SW];
+#pragma unroll
+      for (int x = 0; x < L::SW; ++x) t[x] = Real(0);
+#pragma unroll
+      for (int r = 0; r < DA; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          t[r * 3 + c] = Real(double(w[r * 3]) * vi[s3(0, c)] + double(w[r * 3 + 1]) * vi[s3(1, c)] +
+                              double(w[r * 3 + 2]) * vi[s3(2, c)]);
+      vstore(oT + (size_t)k * L::SW, t);
+    }
+  }
+  block_reduce<NV, NV>(v, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int t = 0; t < NV; ++t) part[(size_t)blockIdx.x * NV + t] = v[t];
+  }
+}
+
+// One warp per chunk of a camera-pair block's observation pairs: partial sum T_k W_m^T.
+template <int DA, typename Real>
+__global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __restrict__ part) {
+  using L = Lay<DA, 0>;
+  using SV = SchurV<DA>;
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (ch >= s.nch_blk) return;
+  Real acc[SV::VP];
+#pragma unroll
+  for (int t = 0; t < SV::VP; ++t) acc[t] = Real(0);
+  const Real* oT = reinterpret_cast<const Real*>(s.o_T);
+  const Real* oW = reinterpret_cast<const Real*>(s.o_W);
+  for (int p = s.bc_beg[ch] + lane; p < s.bc_end[ch]; p += 32) {
+    const int k = s.pr_k[p], m = s.pr_m[p];
+    Real t[L::SW], w[L::SW];
+    vload(oT + (size_t)k * L::SW, t);
+    vload(oW + (size_t)m * L::SW, w);
+#pragma unroll
+    for (int a = 0; a < DA; ++a)
+#pragma unroll
+      for (int c = 0; c < DA; ++c)
+        acc[a * DA + c] += t[a * 3] * w[c * 3] + t[a * 3 + 1] * w[c * 3 + 1] + t[a * 3 + 2] * w[c * 3 + 2];
+  }
+  warp_reduce_transpose(acc);
+#pragma unroll
+  for (int t = 0; t < SV::VP / 32; ++t) part[(size_t)ch * SV::VP + lane * (SV::VP / 32) + t] = double(acc[t]);
+}
+
+// One warp per camera-pair block (i <= l): S_il = delta_il (U_i + lambda I) - sum of its chunk
+// partials, written into the lower triangle of the dense column-major S.
+template <int DA, typename Real>
+__global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* __restrict__ part) {
+  using L = Lay<DA, 0>;
+  using SV = SchurV<DA>;
+  constexpr int PER = SV::VP / 32;
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (b >= s.nb) return;
+  const int i = s.b_i[b], l = s.b_l[b];
+  double sum[PER];
+#pragma unroll
+  for (int t = 0; t < PER; ++t) sum[t] = 0.0;
+  for (int ch = s.blk_bc_ptr[b]; ch < s.blk_bc_ptr[b + 1]; ++ch)
+#pragma unroll
+    for (int t = 0; t < PER; ++t) sum[t] += part[(size_t)ch * SV::VP + lane + 32 * t];
+  const double lam = *s.d_lambda;
+  const Real* cU = reinterpret_cast<const Real*>(s.c_U) + (size_t)i * L::SU;
+  const size_t ld = s.ld;
+#pragma unroll
+  for (int t = 0; t < PER; ++t) {
+    const int e = lane + 32 * t;
+    if (e >= SV::NV) continue;
+    const int a = e / DA, c = e % DA;
+    double val = -sum[t];
+    if (i == l) val += double(cU[a * DA + c]) + (a == c ? lam : 0.0);
+    // element (row l*DA + c, col i*DA + a) of the lower triangle holds S_il[a][c]
+    s.S[(size_t)(i * DA + a) * ld + (l * DA + c)] = val;
+  }
+}
+
+// One warp per chunk of a camera's observations: partial sum_k W_k q_j(k) and sum_k T_k Y_j(k).
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, double* __restrict__ part) {
+  using L = Lay<DA, DC>;
+  using RV = RhsV<DA, DC>;
+  constexpr int DCc = L::DCc;
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * kCamWarps + (threadIdx.x >> 5);
+  if (ch >= s.nch_cam) return;
+  double acc[RV::VP];
+#pragma unroll
+  for (int t = 0; t < RV::VP; ++t) acc[t] = 0.0;
+  const Real* oW = reinterpret_cast<const Real*>(s.o_W);
+  const Real* oT = reinterpret_cast<const Real*>(s.o_T);
+  for (int idx = s.cc_beg[ch] + lane; idx < s.cc_end[ch]; idx += 32) {
+    const int k = s.c_obs[idx];
+    const int j = s.o_pt[k];
+    Real w[L::SW];
+    vload(oW + (size_t)k * L::SW, w);
+    double q[4];
+    vload(s.p_q + (size_t)j * 4, q);
+#pragma unroll
+    for (int a = 0; a < DA; ++a) acc[a] += double(w[a * 3]) * q[0] + double(w[a * 3 + 1]) * q[1] + double(w[a * 3 + 2]) * q[2];
+    if (DC > 0) {
+      Real t[L::SW], y[L::SY];
+      vload(oT + (size_t)k * L::SW, t);
+      vload(reinterpret_cast<const Real*>(s.p_Y) + (size_t)j * L::SY, y);
+#pragma unroll
+      for (int a = 0; a < DA; ++a)
+#pragma unroll
+        for (int c = 0; c < DCc; ++c)
+          acc[DA + a * DCc + c] += double(t[a * 3]) * double(y[c]) + double(t[a * 3 + 1]) * double(y[DCc + c]) +
+                                   double(t[a * 3 + 2]) * double(y[2 * DCc + c]);
+    }
+  }
+  warp_reduce_transpose(acc);
+#pragma unroll
+  for (int t = 0; t < RV::VP / 32; ++t) part[(size_t)ch * RV::VP + lane * (RV::VP / 32) + t] = acc[t];
+}
+
+// One warp per camera: rhs_i = ga_i - sum W q and the camera/global border X_i - sum T Y into S;
+// identity block, zero rhs and zero border for fixed cameras.
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const double* __restrict__ cpart) {
+  using L = Lay<DA, DC>;
+  using RV = RhsV<DA, DC>;
+  constexpr int DCc = L::DCc;
+  constexpr int PER = RV::VP / 32;
+  const Dims& D = s.d;
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kCamWarps + (threadIdx.x >> 5);
+  if (i >= D.N) return;
+  const size_t ld = s.ld;
+  const int c0 = D.N * DA;
+  if (i < D.nnA) {
+    for (int t = lane; t < DA * DA; t += 32) {
+      const int a = t / DA, c = t % DA;
+      s.S[(size_t)(i * DA + a) * ld + (i * DA + c)] = (a == c) ? 1.0 : 0.0;
+    }
+    for (int a = lane; a < DA; a += 32) s.rhs[(size_t)(i * DA + a) * ld] = 0.0;
+    for (int t = lane; t < RV::NX; t += 32) s.S[(size_t)(i * DA + t / DCc) * ld + c0 + t % DCc] = 0.0;
+    return;
+  }
+  double sum[PER];
+#pragma unroll
+  for (int t = 0; t < PER; ++t) sum[t] = 0.0;
+  for (int ch = s.cam_cc_ptr[i]; ch < s.cam_cc_ptr[i + 1]; ++ch)
+#pragma unroll
+    for (int t = 0; t < PER; ++t) sum[t] += cpart[(size_t)ch * RV::VP + lane + 32 * t];
+  const Real* cX = reinterpret_cast<const Real*>(s.c_X) + (size_t)i * L::SX;
+#pragma unroll
+  for (int t = 0; t < PER; ++t) {
+    const int e = lane + 32 * t;
+    if (e < DA) {
+      s.rhs[(size_t)(i * DA + e) * ld] = s.c_ga[(size_t)i * L::SG + e] - sum[t];
+    } else if (e < RV::NV) {
+      const int x = e - DA, a = x / DCc, c = x % DCc;
+      const double val = (c >= D.nnC) ? double(cX[a * DCc + c]) - sum[t] : 0.0;
+      s.S[(size_t)(i * DA + a) * ld + (c0 + c)] = val;  // row c0+c, col i*DA+a
+    }
+  }
+}
+
+// Global block: S_cc = Z + lambda I - sum_j Y_j^T Vinv_j Y_j, rhs_c = gc - sum_j Y_j^T q_j.
+template <int DA, int DC>
+__global__ void __launch_bounds__(256) k_global_block(DevState s, const double* __restrict__ part, int nbp) {
+  constexpr int NV = ElimNV<DC>::NV;
+  constexpr int DCc = DC > 0 ? DC : 1;
+  __shared__ double red[8 * NV];
+  double a[NV];
+  fold_partials<NV, NV>(part, nbp, a, red);
+  if (threadIdx.x == 0 && DC > 0) {
+    const Dims& D = s.d;
+    const double lam = *s.d_lambda;
+    const int c0 = D.N * DA;
+    const size_t ld = s.ld;
+    int z = 0;
+    for (int r = 0; r < DCc; ++r)
+      for (int c = r; c < DCc; ++c, ++z) {
+        double val;
+        if (r < D.nnC || c < D.nnC) val = (r == c) ? 1.0 : 0.0;
+        else val = s.g_Z[r * DCc + c] - a[z] + (r == c ? lam : 0.0);
+        s.S[(size_t)(c0 + r) * ld + (c0 + c)] = val;   // row c0+c >= col c0+r
+      }
+    for (int c = 0; c < DCc; ++c) s.rhs[(size_t)(c0 + c) * ld] = (c < D.nnC) ? 0.0 : s.g_gc[c] - a[nsym(DC) + c];
+  }
+}
+
+// ---- trial step ----------------------------------------------------------------------------
+
+// One thread per point: db_j = q_j - sum_k T_k^T da_i(k) - (Vinv Y_j) dc; X' = X + db.
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double* __restrict__ part) {
+  using L = Lay<DA, DC>;
+  constexpr int DCc = L::DCc;
+  __shared__ double red[(kPtThreads / 32) * 2];
+  const Dims& D = s.d;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (j < D.M) {
+    const double* x = s.x;
+    double db[3] = {0, 0, 0};
+    if (j >= D.nnB) {
+      double q[4];
+      vload(s.p_q + (size_t)j * 4, q);
+      double acc[3] = {0, 0, 0};
+      const Real* oT = reinterpret_cast<const Real*>(s.o_T);
+      for (int k = s.p_ptr[j]; k < s.p_ptr[j + 1]; ++k) {
+        const int i = s.o_cam[k];
+        Real t[L::SW];
+        vload(oT + (size_t)k * L::SW, t);
+#pragma unroll
+        for (int a = 0; a < DA; ++a) {
+          const double da = x[i * DA + a];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[c] += double(t[a * 3 + c]) * da;
+        }
+      }
+      if (DC > 0) {
+        Real yv[L::SY];
+        vload(reinterpret_cast<const Real*>(s.p_YV) + (size_t)j * L::SY, yv);
+        const int c0 = D.N * DA;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < DCc; ++c) acc[r] += double(yv[r * DCc + c]) * x[c0 + c];
+      }
+      double gb[4];
+      vload(s.p_gb + (size_t)j * 4, gb);
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        db[r] = q[r] - acc[r];
+        v[0] += db[r] * db[r];
+        v[1] += db[r] * gb[r];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) s.trial.X[3 * j + r] = s.cur.X[3 * j + r] + db[r];
+  }
+  block_reduce<2, 2>(v, red);
+  if (threadIdx.x == 0) {
+    part[(size_t)blockIdx.x * 2] = v[0];
+    part[(size_t)blockIdx.x * 2 + 1] = v[1];
+  }
+}
+
+// One thread per camera (plus the globals on thread 0 of block 0): trial parameters.
+template <int MODEL, int DA, int DC>
+__global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __restrict__ part) {
+  __shared__ double red[4 * 2];
+  const Dims& D = s.d;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double* x = s.x;
+  double v[2] = {0.0, 0.0};
+  if (i < D.N) {
+    double R[9], T[3];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) R[t] = s.cur.R[9 * i + t];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) T[t] = s.cur.T[3 * i + t];
+    double K[9];
+    double dist[4] = {0, 0, 0, 0};
+    if (MODEL != kModelCommon) {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) K[t] = s.cur.K[9 * i + t];
+    }
+    if (MODEL == kModelVarying) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) dist[t] = s.cur.dist[4 * i + t];
+    }
+    if (i >= D.nnA) {
+      double d[DA];
+#pragma unroll
+      for (int a = 0; a < DA; ++a) {
+        d[a] = x[i * DA + a];
+        v[0] += d[a] * d[a];
+        v[1] += d[a] * s.c_ga[(size_t)i * Lay<DA, DC>::SG + a];
+      }
+      T[0] += d[0]; T[1] += d[1]; T[2] += d[2];
+      rotate_update(d + 3, R);
+      if (MODEL == kModelVarying && DA > 6) {
+        double di[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 6; a < DA; ++a) di[a - 6] = d[a];
+        intrinsic_update(D.mode, di, K, dist, -1.0);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 9; ++t) s.trial.R[9 * i + t] = R[t];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) s.trial.T[3 * i + t] = T[t];
+    if (MODEL != kModelCommon) {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) s.trial.K[9 * i + t] = K[t];
+    }
+    if (MODEL == kModelVarying) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) s.trial.dist[4 * i + t] = dist[t];
+    }
+  }
+  if (MODEL == kModelCommon && blockIdx.x == 0 && threadIdx.x == 0) {
+    double K[9], dist[4];
+    for (int t = 0; t < 9; ++t) K[t] = s.cur.K[t];
+    for (int t = 0; t < 4; ++t) dist[t] = s.cur.dist[t];
+    if (DC > D.nnC) {
+      double di[7] = {0, 0, 0, 0, 0, 0, 0};
+      const int c0 = D.N * DA;
+      for (int c = 0; c < DC; ++c) {
+        di[c] = (c >= D.nnC) ? x[c0 + c] : 0.0;
+        v[0] += di[c] * di[c];
+        v[1] += di[c] * s.g_gc[c];
+      }
+      intrinsic_update(D.mode, di, K, dist, D.cached_ar);
+    }
+    for (int t = 0; t < 9; ++t) s.trial.K[t] = K[t];
+    for (int t = 0; t < 4; ++t) s.trial.dist[t] = dist[t];
+  }
+  block_reduce<2, 2>(v, red);
+  if (threadIdx.x == 0) {
+    part[(size_t)blockIdx.x * 2] = v[0];
+    part[(size_t)blockIdx.x * 2 + 1] = v[1];
+  }
+}
+
+// One thread per observation: sum |w e|^2 at parameters P, with the stored (frozen) weights or
+// with weights recomputed at P.
+template <int MODEL>
+__global__ void __launch_bounds__(256) k_obs_cost(DevState s, ParamSet P, int recompute_w, double* __restrict__ part) {
+  __shared__ double red[8];
+  const Dims& D = s.d;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (k < D.K) {
+    const int i = s.o_cam[k], j = s.o_pt[k];
+    Cam cam;
+    load_cam<MODEL>(cam, P.R, P.T, P.K, P.dist, i);
+    const double X[3] = {P.X[3 * j], P.X[3 * j + 1], P.X[3 * j + 2]};
+    double XX[3], e[2];
+    residual<MODEL>(cam, X, s.o_meas[2 * k], s.o_meas[2 * k + 1], XX, e);
+    const double w = recompute_w ? huber_weight(D.thr, e) : s.o_w[k];
+    v[0] = w * w * (e[0] * e[0] + e[1] * e[1]);
+  }
+  block_reduce<1, 1>(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+__global__ void __launch_bounds__(256) k_trial_finalize(DevState s, const double* __restrict__ pb, int nbp,
+                                                        const double* __restrict__ pc, int nbc,
+                                                        const double* __restrict__ po, int nbo) {
+  __shared__ double red[8 * 2];
+  double a[2], b[2], c[1];
+  fold_partials<2, 2>(pb, nbp, a, red);
+  fold_partials<2, 2>(pc, nbc, b, red);
+  fold_partials<1, 1>(po, nbo, c, red);
+  if (threadIdx.x == 0) {
+    s.d_trial[0] = c[0];
+    s.d_trial[1] = a[0] + b[0];
+    s.d_trial[2] = a[1] + b[1];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_sum_to(const double* __restrict__ po, int nbo, double* out) {
+  __shared__ double red[8];
+  double c[1];
+  fold_partials<1, 1>(po, nbo, c, red);
+  if (threadIdx.x == 0) *out = c[0];
+}
+
+// ---- host launchers ----------------------------------------------------------------------
+
+inline int cdiv(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// partial-buffer regions (in doubles)
+struct PartLayout {
+  size_t relin_pt, relin_cam, elim, backsub, camupd, obs;
+};
+
+template <int DA, int DC>
+inline PartLayout part_layout(const DevState& s) {
+  PartLayout p;
+  const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);
+  const int bc = cdiv(std::max(s.d.N, 1), kCamWarps);
+  const int bu = cdiv(std::max(s.d.N, 1), 128);
+  p.relin_pt = 0;
+  p.relin_cam = p.relin_pt + (size_t)bp * RelinNV<DC>::NV;
+  p.elim = p.relin_cam + (size_t)bc * 2;
+  p.backsub = p.elim + (size_t)bp * ElimNV<DC>::NV;
+  p.camupd = p.backsub + (size_t)bp * 2;
+  p.obs = p.camupd + (size_t)bu * 2;
+  return p;
+}
+
+template <int MODEL, int DA, int DC, typename Real>
+struct Ops {
+  // Launches one stage of the LM iteration (see LmStage in lm.cuh).
+  static int stage(DevState& s, int id, int init_lambda, double tau, cudaStream_t st) {
+    const PartLayout pl = part_layout<DA, DC>(s);
+    const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);
+    const int bc = cdiv(std::max(s.d.N, 1), kCamWarps);
+    const int bu = cdiv(std::max(s.d.N, 1), 128);
+    const int bo = cdiv(std::max(s.d.K, 1), 256);
+    switch (id) {
+      case kStageLinearize:
+        k_linearize<MODEL, DA, DC, Real><<<bp, kPtThreads, 0, st>>>(s, s.part + pl.relin_pt);
+        break;
+      case kStageCameraChunks:
+        if (s.nch_cam == 0) return V3DBA_OK;
+        k_camera_chunks<DA, DC, Real><<<cdiv(s.nch_cam, kCamWarps), kCamWarps * 32, 0, st>>>(s, s.part_cc);
+        break;
+      case kStageCameraFinish:
+        k_camera_finish<DA, DC, Real><<<bc, kCamWarps * 32, 0, st>>>(s, s.part_cc, s.part + pl.relin_cam);
+        break;
+      case kStageRelinFinalize:
+        k_relin_finalize<DC><<<1, 256, 0, st>>>(s, s.part + pl.relin_pt, bp, s.part + pl.relin_cam, bc,
+                                                 init_lambda, tau);
+        break;
+      case kStagePointEliminate:
+        k_point_eliminate<DA, DC, Real><<<bp, kPtThreads, 0, st>>>(s, s.part + pl.elim);
+        break;
+      case kStageSchurChunks:
+        if (s.nch_blk == 0) return V3DBA_OK;
+        k_schur_chunks<DA, Real><<<cdiv(s.nch_blk, 4), 128, 0, st>>>(s, s.part_bc);
+        break;
+      case kStageSchurFinish:
+        if (s.nb == 0) return V3DBA_OK;
+        k_schur_finish<DA, Real><<<cdiv(s.nb, 4), 128, 0, st>>>(s, s.part_bc);
+        break;
+      case kStageRhsChunks:
+        if (s.nch_cam == 0) return V3DBA_OK;
+        k_rhs_chunks<DA, DC, Real><<<cdiv(s.nch_cam, kCamWarps), kCamWarps * 32, 0, st>>>(s, s.part_cc);
+        break;
+      case kStageRhsFinish:
+        k_rhs_finish<DA, DC, Real><<<bc, kCamWarps * 32, 0, st>>>(s, s.part_cc);
+        break;
+      case kStageGlobalBlock:
+        if (DC == 0) return V3DBA_OK;
+        k_global_block<DA, DC><<<1, 256, 0, st>>>(s, s.part + pl.elim, bp);
+        break;
+      case kStagePointBacksub:
+        k_point_backsub<DA, DC, Real><<<bp, kPtThreads, 0, st>>>(s, s.part + pl.backsub);
+        break;
+      case kStageCameraUpdate:
+        k_camera_update<MODEL, DA, DC><<<bu, 128, 0, st>>>(s, s.part + pl.camupd);
+        break;
+      case kStageTrialCost:
+        k_obs_cost<MODEL><<<bo, 256, 0, st>>>(s, s.trial, 0, s.part + pl.obs);
+        break;
+      case kStageTrialFinalize:
+        k_trial_finalize<<<1, 256, 0, st>>>(s, s.part + pl.backsub, bp, s.part + pl.camupd, bu, s.part + pl.obs, bo);
+        break;
+      default:
+        return V3DBA_ERR_INVALID_ARGUMENT;
+    }
+    V3DBA_LAUNCH_CHECK();
+    return V3DBA_OK;
+  }
+  static int run(DevState& s, int first, int last, int init_lambda, double tau, cudaStream_t st) {
+    for (int id = first; id <= last; ++id) {
+      const int rc = stage(s, id, init_lambda, tau, st);
+      if (rc) return rc;
+    }
+    return V3DBA_OK;
+  }
+  static int relinearize(DevState& s, bool init_lambda, double tau, cudaStream_t st) {
+    return run(s, kStageLinearize, kStageRelinFinalize, init_lambda ? 1 : 0, tau, st);
+  }
+  static int build_reduced(DevState& s, cudaStream_t st) {
+    return run(s, kStagePointEliminate, kStageGlobalBlock, 0, 0.0, st);
+  }
+  static int finish_trial(DevState& s, cudaStream_t st) {
+    return run(s, kStagePointBacksub, kStageTrialFinalize, 0, 0.0, st);
+  }
+  static int cost(DevState& s, const ParamSet& P, double* d_out, cudaStream_t st) {
+    const PartLayout pl = part_layout<DA, DC>(s);
+    const int bo = cdiv(std::max(s.d.K, 1), 256);
+    k_obs_cost<MODEL><<<bo, 256, 0, st>>>(s, P, 1, s.part + pl.obs);
+    V3DBA_LAUNCH_CHECK();
+    k_sum_to<<<1, 256, 0, st>>>(s.part + pl.obs, bo, d_out);
+    V3DBA_LAUNCH_CHECK();
+    return V3DBA_OK;
+  }
+  static const LmOps* table() {
+    static const LmOps t = {&relinearize, &build_reduced, &finish_trial, &cost, &stage};
+    return &t;
+  }
+};
+
+size_t camera_chunk_values(int DA, int DC) {
+  const int nu = DA * (DA + 1) / 2 + DA + DA * DC;
+  const int nr = DA + DA * DC;
+  return (size_t)round32(std::max(nu, nr));
+}
+size_t block_chunk_values(int DA) { return (size_t)round32(DA * DA); }
+
+// size (in doubles) of the partial buffer for the given dims
+size_t partial_doubles(const DevState& s) {
+  const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);
+  const int bc = cdiv(std::max(s.d.N, 1), kCamWarps);
+  const int bu = cdiv(std::max(s.d.N, 1), 128);
+  const int bo = cdiv(std::max(s.d.K, 1), 256);
+  const size_t maxNV = RelinNV<7>::NV;
+  return (size_t)bp * maxNV + (size_t)bc * 2 + (size_t)bp * ElimNV<7>::NV + (size_t)bp * 2 + (size_t)bu * 2 + bo + 64;
+}
+
+template <typename Real>
+const LmOps* ops_for(int model, int DA, int DC) {
+  if (model == kModelStd) return DA == 6 && DC == 0 ? Ops<kModelStd, 6, 0, Real>::table() : nullptr;
+  if (model == kModelCommon) {
+    if (DA != 6) return nullptr;
+    switch (DC) {
+      case 0: return Ops<kModelCommon, 6, 0, Real>::table();
+      case 1: return Ops<kModelCommon, 6, 1, Real>::table();
+      case 3: return Ops<kModelCommon, 6, 3, Real>::table();
+      case 5: return Ops<kModelCommon, 6, 5, Real>::table();
+      case 7: return Ops<kModelCommon, 6, 7, Real>::table();
+    }
+    return nullptr;
+  }
+  if (model == kModelVarying) {
+    if (DC != 0) return nullptr;
+    switch (DA) {
+      case 6: return Ops<kModelVarying, 6, 0, Real>::table();
+      case 7: return Ops<kModelVarying, 7, 0, Real>::table();
+      case 9: return Ops<kModelVarying, 9, 0, Real>::table();
+      case 11: return Ops<kModelVarying, 11, 0, Real>::table();
+      case 13: return Ops<kModelVarying, 13, 0, Real>::table();
+    }
+  }
+  return nullptr;
+}
+
+const LmOps* lm_ops(int model, int DA, int DC, bool fp64) {
+  return fp64 ? ops_for<double>(model, DA, DC) : ops_for<float>(model, DA, DC);
+}
+
+}  // namespace v3dba

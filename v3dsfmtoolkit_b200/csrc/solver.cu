@@ -1,0 +1,678 @@
+// Host side of the C-ABI: problem validation, device layout, structure analysis and the LM
+// driver.  The driver restates SparseLevenbergOptimizer::minimize
+// (V3D/src/Math/v3d_optimization.cpp:719-1250) and the lambda schedule of
+// LevenbergOptimizerCommon (V3D/include/Math/v3d_optimization.h:38-59); every numeric step runs
+// on the GPU, the host only reads back three or four FP64 scalars per LM iteration to take the
+// accept / reject decision with the reference's exact tests.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "lm.cuh"
+#include "model.cuh"
+
+namespace v3dba {
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+size_t partial_doubles(const DevState& s);
+
+}  // namespace v3dba
+
+using namespace v3dba;
+
+struct v3dba_handle_s {
+  DevState s;
+  TileChol chol;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double param_length = 0.0;
+  double lambda = 1e-3;   // LevenbergOptimizerCommon ctor default (v3d_optimization.h:29)
+  double nu = 2.0;        // _nu (v3d_optimization.h:31)
+  double* h_scalars = nullptr;   // pinned readback area
+  std::vector<void*> allocs;
+  size_t nK = 0, nD = 0;
+};
+
+namespace {
+
+int dims_of(int model, int mode, int* dA, int* dC) {
+  if (model < V3DBA_MODEL_STD || model > V3DBA_MODEL_VARYING) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (model != V3DBA_MODEL_STD &&
+      (mode < V3DBA_FULL_BUNDLE_NO_ROTATIONS || mode > V3DBA_FULL_BUNDLE_RADIAL_TANGENTIAL))
+    return V3DBA_ERR_INVALID_ARGUMENT;
+  const int ni = (model == V3DBA_MODEL_STD) ? 0 : intrinsic_dim(mode);
+  *dA = 6 + (model == V3DBA_MODEL_VARYING ? ni : 0);
+  *dC = (model == V3DBA_MODEL_COMMON ? ni : 0);
+  return V3DBA_OK;
+}
+
+bool all_finite(const double* p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+template <typename T>
+int dalloc(v3dba_handle h, T** p, size_t count) {
+  void* q = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? V3DBA_ERR_OUT_OF_MEMORY : V3DBA_ERR_CUDA;
+  }
+  h->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return V3DBA_OK;
+}
+
+int alloc_params(v3dba_handle h, ParamSet& P, int N, int M) {
+  int rc;
+  if ((rc = dalloc(h, &P.K, h->nK))) return rc;
+  if ((rc = dalloc(h, &P.R, (size_t)N * 9))) return rc;
+  if ((rc = dalloc(h, &P.T, (size_t)N * 3))) return rc;
+  if ((rc = dalloc(h, &P.dist, std::max<size_t>(h->nD, 4)))) return rc;
+  if ((rc = dalloc(h, &P.X, (size_t)M * 3))) return rc;
+  return V3DBA_OK;
+}
+
+int copy_params(const ParamSet& dst, const ParamSet& src, const v3dba_handle h, cudaStream_t st) {
+  const Dims& D = h->s.d;
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.K, src.K, sizeof(double) * h->nK, cudaMemcpyDeviceToDevice, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.R, src.R, sizeof(double) * 9 * D.N, cudaMemcpyDeviceToDevice, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.T, src.T, sizeof(double) * 3 * D.N, cudaMemcpyDeviceToDevice, st));
+  if (h->nD) V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.dist, src.dist, sizeof(double) * h->nD, cudaMemcpyDeviceToDevice, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.X, src.X, sizeof(double) * 3 * D.M, cudaMemcpyDeviceToDevice, st));
+  return V3DBA_OK;
+}
+
+int upload_params(v3dba_handle h, const ParamSet& P, const double* K, const double* R, const double* T,
+                  const double* dist, const double* X) {
+  const Dims& D = h->s.d;
+  cudaStream_t st = h->stream;
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(P.K, K, sizeof(double) * h->nK, cudaMemcpyHostToDevice, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(P.R, R, sizeof(double) * 9 * D.N, cudaMemcpyHostToDevice, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(P.T, T, sizeof(double) * 3 * D.N, cudaMemcpyHostToDevice, st));
+  if (h->nD) V3DBA_CUDA_TRY(cudaMemcpyAsync(P.dist, dist, sizeof(double) * h->nD, cudaMemcpyHostToDevice, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(P.X, X, sizeof(double) * 3 * D.M, cudaMemcpyHostToDevice, st));
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+  return V3DBA_OK;
+}
+
+template <typename T>
+int upload(v3dba_handle h, T** d, const std::vector<T>& v) {
+  int rc = dalloc(h, d, v.size());
+  if (rc) return rc;
+  if (!v.empty()) V3DBA_CUDA_TRY(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return V3DBA_OK;
+}
+
+void free_handle(v3dba_handle h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void* p : h->allocs) cudaFree(p);
+  tile_chol_free(h->chol);
+  if (h->h_scalars) cudaFreeHost(h->h_scalars);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+// Host-side structure analysis: point-major permutation, camera lists, camera-pair blocks with
+// their observation pairs (sorted by block, then by point), and the tile pattern of S.
+struct Structure {
+  std::vector<int> o_cam, o_pt, o_orig, p_ptr, c_ptr, c_obs;
+  std::vector<double> o_meas;
+  std::vector<int> b_i, b_l, b_ptr, pr_k, pr_m;
+  std::vector<int> cc_beg, cc_end, cam_cc_ptr, bc_beg, bc_end, blk_bc_ptr;
+};
+
+constexpr int kCamChunk = 64;     // observations per camera work chunk
+constexpr int kPairChunk = 128;   // observation pairs per camera-pair work chunk
+
+void build_chunks(Structure& S, int N) {
+  S.cam_cc_ptr.assign(1, 0);
+  for (int i = 0; i < N; ++i) {
+    for (int b = S.c_ptr[i]; b < S.c_ptr[i + 1]; b += kCamChunk) {
+      S.cc_beg.push_back(b);
+      S.cc_end.push_back(std::min(b + kCamChunk, S.c_ptr[i + 1]));
+    }
+    S.cam_cc_ptr.push_back((int)S.cc_beg.size());
+  }
+  const int nb = (int)S.b_i.size();
+  S.blk_bc_ptr.assign(1, 0);
+  for (int b = 0; b < nb; ++b) {
+    for (int p = S.b_ptr[b]; p < S.b_ptr[b + 1]; p += kPairChunk) {
+      S.bc_beg.push_back(p);
+      S.bc_end.push_back(std::min(p + kPairChunk, S.b_ptr[b + 1]));
+    }
+    S.blk_bc_ptr.push_back((int)S.bc_beg.size());
+  }
+}
+
+void build_structure(const v3dba_problem* p, Structure& S) {
+  const int N = p->n_cameras, M = p->n_points, K = p->n_measurements;
+  // point-major permutation (stable: keeps the caller's order inside a track)
+  S.p_ptr.assign(M + 1, 0);
+  for (int k = 0; k < K; ++k) S.p_ptr[p->point[k] + 1]++;
+  for (int j = 0; j < M; ++j) S.p_ptr[j + 1] += S.p_ptr[j];
+  std::vector<int> fill(S.p_ptr.begin(), S.p_ptr.end() - 1);
+  S.o_orig.resize(K);
+  for (int k = 0; k < K; ++k) S.o_orig[fill[p->point[k]]++] = k;
+  S.o_cam.resize(K);
+  S.o_pt.resize(K);
+  S.o_meas.resize(2 * (size_t)K);
+  for (int k = 0; k < K; ++k) {
+    const int o = S.o_orig[k];
+    S.o_cam[k] = p->view[o];
+    S.o_pt[k] = p->point[o];
+    S.o_meas[2 * k] = p->measurements[2 * o];
+    S.o_meas[2 * k + 1] = p->measurements[2 * o + 1];
+  }
+  // camera lists over permuted observations
+  S.c_ptr.assign(N + 1, 0);
+  for (int k = 0; k < K; ++k) S.c_ptr[S.o_cam[k] + 1]++;
+  for (int i = 0; i < N; ++i) S.c_ptr[i + 1] += S.c_ptr[i];
+  S.c_obs.resize(K);
+  fill.assign(S.c_ptr.begin(), S.c_ptr.end() - 1);
+  for (int k = 0; k < K; ++k) S.c_obs[fill[S.o_cam[k]]++] = k;
+  // camera-pair blocks: for camera i, every observation k of i and every observation m of the
+  // same point seen by a camera l >= i gives the pair (k, m) of block (i, l)
+  std::vector<int> local(N, -1), touched;
+  std::vector<int> cnt;
+  std::vector<int> tk, tm, tl;
+  S.b_ptr.assign(1, 0);
+  for (int i = 0; i < N; ++i) {
+    tk.clear(); tm.clear(); tl.clear(); touched.clear();
+    for (int idx = S.c_ptr[i]; idx < S.c_ptr[i + 1]; ++idx) {
+      const int k = S.c_obs[idx];
+      const int j = S.o_pt[k];
+      for (int m = S.p_ptr[j]; m < S.p_ptr[j + 1]; ++m) {
+        const int l = S.o_cam[m];
+        if (l < i) continue;
+        if (local[l] < 0) { local[l] = 0; touched.push_back(l); }
+        tk.push_back(k); tm.push_back(m); tl.push_back(l);
+      }
+    }
+    std::sort(touched.begin(), touched.end());
+    for (size_t t = 0; t < touched.size(); ++t) local[touched[t]] = (int)t;
+    cnt.assign(touched.size() + 1, 0);
+    for (int l : tl) cnt[local[l] + 1]++;
+    for (size_t t = 0; t < touched.size(); ++t) cnt[t + 1] += cnt[t];
+    const size_t base = S.pr_k.size();
+    S.pr_k.resize(base + tk.size());
+    S.pr_m.resize(base + tk.size());
+    std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+    for (size_t t = 0; t < tk.size(); ++t) {
+      const int b = local[tl[t]];
+      S.pr_k[base + pos[b]] = tk[t];
+      S.pr_m[base + pos[b]] = tm[t];
+      pos[b]++;
+    }
+    for (size_t t = 0; t < touched.size(); ++t) {
+      S.b_i.push_back(i);
+      S.b_l.push_back(touched[t]);
+      S.b_ptr.push_back((int)(base + cnt[t + 1]));
+      local[touched[t]] = -1;
+    }
+  }
+  build_chunks(S, N);
+}
+
+}  // namespace
+
+extern "C" {
+
+void v3dba_default_options(v3dba_options* o) {
+  if (!o) return;
+  o->tau = 1e-3;
+  o->max_iterations = 50;
+  o->gradient_threshold = 1e-10;
+  o->update_threshold = 1e-10;
+  o->verbosity = 0;
+  o->precision = V3DBA_PRECISION_MIXED;
+  o->solver = V3DBA_SOLVER_AUTO;
+  o->pcg_tolerance = 1e-6;
+  o->pcg_max_iterations = 500;
+  o->stop_cost = 0.0;
+  o->mixed_escalation = 1;
+}
+
+int v3dba_dims(int model, int mode, int* dA, int* dC) {
+  if (!dA || !dC) return V3DBA_ERR_INVALID_ARGUMENT;
+  return dims_of(model, mode, dA, dC);
+}
+
+const char* v3dba_error_string(int code) {
+  switch (code) {
+    case V3DBA_OK: return "ok";
+    case V3DBA_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case V3DBA_ERR_INVALID_INPUT: return "invalid input (index out of range or non-finite value)";
+    case V3DBA_ERR_CUDA: return "CUDA error";
+    case V3DBA_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case V3DBA_ERR_NO_DEVICE: return "no CUDA device";
+    case V3DBA_ERR_UNSUPPORTED: return "unsupported configuration";
+    case V3DBA_ERR_TIMEOUT: return "device-side wait timed out";
+  }
+  return "unknown error";
+}
+
+uint64_t v3dba_launch_count(void) { return g_launches.load(); }
+
+int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
+  if (!p || !out) return V3DBA_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int dA, dC;
+  int rc = dims_of(p->model, p->mode, &dA, &dC);
+  if (rc) return rc;
+  const int N = p->n_cameras, M = p->n_points, K = p->n_measurements;
+  if (N < 0 || M < 0 || K < 0) return V3DBA_ERR_INVALID_ARGUMENT;
+  if ((N > 0 && (!p->R || !p->T || !p->K)) || (M > 0 && !p->X) ||
+      (K > 0 && (!p->measurements || !p->view || !p->point)))
+    return V3DBA_ERR_INVALID_ARGUMENT;
+  if (p->model == V3DBA_MODEL_COMMON && !p->K) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (p->model != V3DBA_MODEL_STD && !p->dist) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (!(p->inlier_threshold > 0.0) || !std::isfinite(p->inlier_threshold)) return V3DBA_ERR_INVALID_INPUT;
+  for (int k = 0; k < K; ++k)
+    if (p->view[k] < 0 || p->view[k] >= N || p->point[k] < 0 || p->point[k] >= M) return V3DBA_ERR_INVALID_INPUT;
+  const size_t nK = (p->model == V3DBA_MODEL_COMMON) ? 9 : (size_t)9 * N;
+  const size_t nD = (p->model == V3DBA_MODEL_COMMON) ? 4 : (p->model == V3DBA_MODEL_VARYING ? (size_t)4 * N : 0);
+  if (!all_finite(p->K, nK) || !all_finite(p->R, (size_t)9 * N) || !all_finite(p->T, (size_t)3 * N) ||
+      !all_finite(p->X, (size_t)3 * M) || !all_finite(p->measurements, (size_t)2 * K) ||
+      (nD && !all_finite(p->dist, nD)))
+    return V3DBA_ERR_INVALID_INPUT;
+  if (p->model == V3DBA_MODEL_COMMON && p->K[0] == 0.0) return V3DBA_ERR_INVALID_INPUT;
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return V3DBA_ERR_NO_DEVICE;
+  }
+
+  v3dba_handle h = new (std::nothrow) v3dba_handle_s();
+  if (!h) return V3DBA_ERR_OUT_OF_MEMORY;
+  h->nK = nK;
+  h->nD = nD;
+  DevState& s = h->s;
+  Dims& D = s.d;
+  D.N = N; D.M = M; D.K = K; D.DA = dA; D.DC = dC;
+  D.model = p->model; D.mode = (p->model == V3DBA_MODEL_STD) ? 0 : p->mode;
+  D.thr = p->inlier_threshold;
+  D.cached_ar = (p->model == V3DBA_MODEL_COMMON) ? p->K[4] / p->K[0] : 1.0;
+
+  // |p| cached at construction over every camera and point (v3d_metricbundle.h:37-45)
+  double pl = 0.0;
+  for (int i = 0; i < N; ++i)
+    pl += p->T[3 * i] * p->T[3 * i] + p->T[3 * i + 1] * p->T[3 * i + 1] + p->T[3 * i + 2] * p->T[3 * i + 2] + 3.0;
+  for (int j = 0; j < M; ++j)
+    pl += p->X[3 * j] * p->X[3 * j] + p->X[3 * j + 1] * p->X[3 * j + 1] + p->X[3 * j + 2] * p->X[3 * j + 2];
+  h->param_length = std::sqrt(pl);
+
+#define TRY(x) do { if ((rc = (x)) != V3DBA_OK) { free_handle(h); return rc; } } while (0)
+#define CTRY(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { cudaGetLastError(); free_handle(h); \
+    return _e == cudaErrorMemoryAllocation ? V3DBA_ERR_OUT_OF_MEMORY : V3DBA_ERR_CUDA; } } while (0)
+
+  CTRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CTRY(cudaEventCreate(&h->ev0));
+  CTRY(cudaEventCreate(&h->ev1));
+  CTRY(cudaMallocHost(&h->h_scalars, 16 * sizeof(double)));
+
+  Structure st;
+  build_structure(p, st);
+  TRY(upload(h, &s.o_cam, st.o_cam));
+  TRY(upload(h, &s.o_pt, st.o_pt));
+  TRY(upload(h, &s.o_orig, st.o_orig));
+  TRY(upload(h, &s.o_meas, st.o_meas));
+  TRY(upload(h, &s.p_ptr, st.p_ptr));
+  TRY(upload(h, &s.c_ptr, st.c_ptr));
+  TRY(upload(h, &s.c_obs, st.c_obs));
+  s.nb = (int)st.b_i.size();
+  s.P = (int64_t)st.pr_k.size();
+  TRY(upload(h, &s.b_i, st.b_i));
+  TRY(upload(h, &s.b_l, st.b_l));
+  TRY(upload(h, &s.b_ptr, st.b_ptr));
+  TRY(upload(h, &s.pr_k, st.pr_k));
+  TRY(upload(h, &s.pr_m, st.pr_m));
+  s.nch_cam = (int)st.cc_beg.size();
+  s.nch_blk = (int)st.bc_beg.size();
+  TRY(upload(h, &s.cc_beg, st.cc_beg));
+  TRY(upload(h, &s.cc_end, st.cc_end));
+  TRY(upload(h, &s.cam_cc_ptr, st.cam_cc_ptr));
+  TRY(upload(h, &s.bc_beg, st.bc_beg));
+  TRY(upload(h, &s.bc_end, st.bc_end));
+  TRY(upload(h, &s.blk_bc_ptr, st.blk_bc_ptr));
+  TRY(dalloc(h, &s.part_cc, (size_t)std::max(s.nch_cam, 1) * camera_chunk_values(dA, dC)));
+  TRY(dalloc(h, &s.part_bc, (size_t)std::max(s.nch_blk, 1) * block_chunk_values(dA)));
+
+  TRY(alloc_params(h, s.cur, N, M));
+  TRY(alloc_params(h, s.trial, N, M));
+  TRY(alloc_params(h, s.init, N, M));
+  const size_t Kz = std::max(K, 1), Mz = std::max(M, 1), Nz = std::max(N, 1);
+  const int SA = (2 * dA + 3) & ~3, SW = (3 * dA + 3) & ~3, SC = (2 * std::max(dC, 1) + 3) & ~3;
+  const int SG = (dA + 1) & ~1, SY = (3 * std::max(dC, 1) + 3) & ~3, SU = (dA * dA + 3) & ~3;
+  const int SX = (dA * std::max(dC, 1) + 3) & ~3;
+  double* tmp;
+  TRY(dalloc(h, &tmp, Kz * SA)); s.o_A = tmp;
+  TRY(dalloc(h, &tmp, Kz * SW)); s.o_W = tmp;
+  TRY(dalloc(h, &tmp, dC ? Kz * SC : 4)); s.o_C = tmp;
+  TRY(dalloc(h, &tmp, Kz * SW)); s.o_T = tmp;
+  TRY(dalloc(h, &s.o_ga, Kz * SG));
+  TRY(dalloc(h, &s.o_w, Kz));
+  TRY(dalloc(h, &tmp, Mz * 8)); s.p_V = tmp;
+  TRY(dalloc(h, &tmp, Mz * SY)); s.p_Y = tmp;
+  TRY(dalloc(h, &tmp, Mz * 8)); s.p_Vinv = tmp;
+  TRY(dalloc(h, &tmp, Mz * SY)); s.p_YV = tmp;
+  TRY(dalloc(h, &s.p_gb, Mz * 4));
+  TRY(dalloc(h, &s.p_q, Mz * 4));
+  TRY(dalloc(h, &tmp, Nz * SU)); s.c_U = tmp;
+  TRY(dalloc(h, &tmp, Nz * SX)); s.c_X = tmp;
+  TRY(dalloc(h, &s.c_ga, Nz * SG));
+  TRY(dalloc(h, &s.g_Z, 64));
+  TRY(dalloc(h, &s.g_gc, 8));
+  TRY(dalloc(h, &s.d_lambda, 1));
+  TRY(dalloc(h, &s.d_relin, 4));
+  TRY(dalloc(h, &s.d_trial, 4));
+  TRY(dalloc(h, &s.d_fail, 1));
+  s.part_cap = partial_doubles(s);
+  TRY(dalloc(h, &s.part, s.part_cap));
+  CTRY(cudaMemset(s.g_Z, 0, 64 * sizeof(double)));
+  CTRY(cudaMemset(s.g_gc, 0, 8 * sizeof(double)));
+
+  // reduced system: n = N*dA + dC, tile pattern from the camera-pair blocks and the border
+  s.n = N * dA + dC;
+  const int nt = std::max(1, (s.n + TileChol::TB - 1) / TileChol::TB);
+  std::vector<uint8_t> nz((size_t)nt * nt, 0);
+  auto mark = [&](int r0, int r1, int c0, int c1) {  // scalar row range x col range, r >= c part
+    for (int tr = r0 / 64; tr <= (r1 - 1) / 64; ++tr)
+      for (int tcl = c0 / 64; tcl <= (c1 - 1) / 64; ++tcl)
+        if (tr >= tcl) nz[(size_t)tr * nt + tcl] = 1;
+  };
+  for (int b = 0; b < s.nb; ++b) mark(st.b_l[b] * dA, st.b_l[b] * dA + dA, st.b_i[b] * dA, st.b_i[b] * dA + dA);
+  for (int i = 0; i < N; ++i) {
+    mark(i * dA, i * dA + dA, i * dA, i * dA + dA);
+    if (dC) mark(N * dA, N * dA + dC, i * dA, i * dA + dA);
+  }
+  if (dC) mark(N * dA, N * dA + dC, N * dA, N * dA + dC);
+  TRY(tile_chol_plan(h->chol, std::max(s.n, 1), nz));
+  s.n_pad = h->chol.n_pad;
+  s.ld = h->chol.ld;
+  TRY(dalloc(h, &s.S, (size_t)s.ld * s.n_pad));
+  s.rhs = s.S + s.n_pad;
+  TRY(dalloc(h, &s.x, (size_t)s.n_pad));
+
+  TRY(upload_params(h, s.cur, p->K, p->R, p->T, p->dist, p->X));
+  TRY(copy_params(s.init, s.cur, h, h->stream));
+  TRY(copy_params(s.trial, s.cur, h, h->stream));
+  CTRY(cudaStreamSynchronize(h->stream));
+#undef TRY
+#undef CTRY
+  *out = h;
+  return V3DBA_OK;
+}
+
+int v3dba_destroy(v3dba_handle h) {
+  if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
+  free_handle(h);
+  return V3DBA_OK;
+}
+
+int v3dba_set_nonvarying(v3dba_handle h, int nA, int nB, int nC) {
+  if (!h || nA < 0 || nB < 0 || nC < 0) return V3DBA_ERR_INVALID_ARGUMENT;
+  h->s.d.nnA = std::min(nA, h->s.d.N);
+  h->s.d.nnB = std::min(nB, h->s.d.M);
+  h->s.d.nnC = std::min(nC, h->s.d.DC);
+  return V3DBA_OK;
+}
+
+int v3dba_set_lambda(v3dba_handle h, double lambda) {
+  if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
+  h->lambda = lambda;
+  return V3DBA_OK;
+}
+
+int v3dba_set_params(v3dba_handle h, const double* K, const double* R, const double* T, const double* dist,
+                     const double* X) {
+  if (!h || !K || !R || !T || !X || (h->nD && !dist)) return V3DBA_ERR_INVALID_ARGUMENT;
+  return upload_params(h, h->s.cur, K, R, T, dist, X);
+}
+
+int v3dba_get_params(v3dba_handle h, double* K, double* R, double* T, double* dist, double* X) {
+  if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
+  const Dims& D = h->s.d;
+  const ParamSet& P = h->s.cur;
+  cudaStream_t st = h->stream;
+  if (K) V3DBA_CUDA_TRY(cudaMemcpyAsync(K, P.K, sizeof(double) * h->nK, cudaMemcpyDeviceToHost, st));
+  if (R) V3DBA_CUDA_TRY(cudaMemcpyAsync(R, P.R, sizeof(double) * 9 * D.N, cudaMemcpyDeviceToHost, st));
+  if (T) V3DBA_CUDA_TRY(cudaMemcpyAsync(T, P.T, sizeof(double) * 3 * D.N, cudaMemcpyDeviceToHost, st));
+  if (dist && h->nD) V3DBA_CUDA_TRY(cudaMemcpyAsync(dist, P.dist, sizeof(double) * h->nD, cudaMemcpyDeviceToHost, st));
+  if (X) V3DBA_CUDA_TRY(cudaMemcpyAsync(X, P.X, sizeof(double) * 3 * D.M, cudaMemcpyDeviceToHost, st));
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+  return V3DBA_OK;
+}
+
+int v3dba_reset_params(v3dba_handle h) {
+  if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
+  int rc = copy_params(h->s.cur, h->s.init, h, h->stream);
+  if (rc) return rc;
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->lambda = 1e-3;
+  h->nu = 2.0;
+  return V3DBA_OK;
+}
+
+int v3dba_cost(v3dba_handle h, double* cost) {
+  if (!h || !cost) return V3DBA_ERR_INVALID_ARGUMENT;
+  DevState& s = h->s;
+  const LmOps* ops = lm_ops(s.d.model, s.d.DA, s.d.DC, true);
+  if (!ops) return V3DBA_ERR_UNSUPPORTED;
+  int rc = ops->cost(s, s.cur, s.d_trial, h->stream);
+  if (rc) return rc;
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars, s.d_trial, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *cost = h->h_scalars[0];
+  return V3DBA_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One damped trial: reduced system at *d_lambda, Cholesky, back-substitution, trial parameters
+// and their cost.  Reads back {new_err, |delta|^2, delta . g, fail}.
+int run_trial(v3dba_handle h, const LmOps* ops, double lambda, double out[4]) {
+  DevState& s = h->s;
+  cudaStream_t st = h->stream;
+  h->h_scalars[8] = lambda;
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(s.d_lambda, h->h_scalars + 8, sizeof(double), cudaMemcpyHostToDevice, st));
+  V3DBA_CUDA_TRY(cudaMemsetAsync(s.d_fail, 0, sizeof(int), st));
+  int rc;
+  if ((rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
+  if ((rc = ops->build_reduced(s, st))) return rc;
+  if ((rc = tile_chol_solve(h->chol, s.S, s.x, s.d_fail, st))) return rc;
+  if ((rc = ops->finish_trial(s, st))) return rc;
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars, s.d_trial, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 3, s.d_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+  out[0] = h->h_scalars[0];
+  out[1] = h->h_scalars[1];
+  out[2] = h->h_scalars[2];
+  int fail;
+  std::memcpy(&fail, h->h_scalars + 3, sizeof(int));
+  out[3] = fail ? 1.0 : 0.0;
+  return V3DBA_OK;
+}
+
+}  // namespace
+
+extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_result* res) {
+  if (!h || !res) return V3DBA_ERR_INVALID_ARGUMENT;
+  v3dba_options o;
+  if (opts) o = *opts; else v3dba_default_options(&o);
+  std::memset(res, 0, sizeof(*res));
+  res->status = V3DBA_STATUS_TIMEOUT;
+  res->fp64_from_iteration = -1;
+  DevState& s = h->s;
+  const Dims& D = s.d;
+  bool fp64 = (o.precision == V3DBA_PRECISION_FP64);
+  const LmOps* ops64 = lm_ops(D.model, D.DA, D.DC, true);
+  const LmOps* ops = lm_ops(D.model, D.DA, D.DC, fp64);
+  if (!ops || !ops64) return V3DBA_ERR_UNSUPPORTED;
+  bool relinearize_again = false;   // blocks to be rebuilt in FP64 at unchanged parameters
+  if (o.solver == V3DBA_SOLVER_PCG) return V3DBA_ERR_UNSUPPORTED;
+
+  const int nvA = D.N - D.nnA, nvB = D.M - D.nnB, nvC = D.DC - D.nnC;
+  if (nvA <= 0 && nvB <= 0 && nvC <= 0) {
+    res->status = V3DBA_STATUS_CONVERGED;
+    res->lambda = h->lambda;
+    return V3DBA_OK;
+  }
+  cudaStream_t st = h->stream;
+  V3DBA_CUDA_TRY(cudaEventRecord(h->ev0, st));
+  bool compute_derivatives = true;
+  double err = 0.0;
+  double lambda = h->lambda;
+  int it;
+  int rc;
+  for (it = 0; it < o.max_iterations; ++it) {
+    if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: currentIteration: %d\n", it);
+    if (relinearize_again && !compute_derivatives) {
+      // same parameters, same FP64 cost and gradient; only the block precision changes
+      if ((rc = ops->relinearize(s, false, o.tau, st))) return rc;
+    }
+    relinearize_again = false;
+    if (compute_derivatives) {
+      if ((rc = ops->relinearize(s, it == 0, o.tau, st))) return rc;
+      V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 4, s.d_relin, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+      err = h->h_scalars[4];
+      const double gmax = h->h_scalars[5], dmax = h->h_scalars[6];
+      if (res->n_relinearizations == 0) res->initial_cost = err;
+      res->n_relinearizations++;
+      res->cost = err;
+      if (o.verbosity >= 1) printf("SparseLevenbergOptimizer: |residual|^2 = %.17g\n", err);
+      if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: lambda = %.17g\n", lambda);
+      if (o.stop_cost > 0.0 && err <= o.stop_cost) {
+        res->reached_stop_cost = 1;
+        break;
+      }
+      if (gmax < o.gradient_threshold) {   // cpp:857-861
+        res->status = V3DBA_STATUS_CONVERGED;
+        break;
+      }
+      if (it == 0) {
+        lambda = o.tau * dmax;             // cpp:981-1052
+        if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: initial lambda = %.17g\n", lambda);
+      }
+    }
+    double t[4];
+    if ((rc = run_trial(h, ops, lambda, t))) return rc;
+    const bool success = t[3] == 0.0;
+    double rho = 0.0;
+    if (success) {
+      const double d2 = t[1];
+      if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: ||delta||^2 = %.17g\n", d2);
+      if (std::sqrt(d2) < o.update_threshold * (h->param_length + o.update_threshold)) {  // cpp:1154-1159
+        res->status = V3DBA_STATUS_SMALL_UPDATE;
+        break;
+      }
+      const double new_err = t[0];
+      rho = (err - new_err) / (lambda * d2 + t[2]);   // cpp:1188-1210
+      if (o.verbosity >= 2)
+        printf("SparseLevenbergOptimizer: |new residual|^2 = %.17g rho = %.17g\n", new_err, rho);
+    } else if (o.verbosity >= 2) {
+      printf("SparseLevenbergOptimizer: LDL decomposition failed. Increasing lambda.\n");
+    }
+    if (!fp64 && o.mixed_escalation && (!success || rho < 0.1)) {
+      // the quadratic model is no longer trusted: stop adding FP32 rounding to it
+      fp64 = true;
+      ops = ops64;
+      res->fp64_from_iteration = it;
+      relinearize_again = true;
+      if (o.verbosity >= 2) printf("v3dba: normal-equation blocks switched to FP64 at iteration %d\n", it);
+    }
+    if (success && rho > 0.0) {
+      std::swap(s.cur, s.trial);           // accept
+      const double r = 2.0 * rho - 1.0;
+      lambda *= std::max(1.0 / 3.0, 1.0 - r * r * r);
+      if (lambda < 1e-10) lambda = 1e-10;
+      h->nu = 2.0;
+      compute_derivatives = true;
+    } else {
+      res->n_rejected++;
+      lambda *= h->nu;
+      h->nu *= 2.0;
+      compute_derivatives = false;
+    }
+  }
+  V3DBA_CUDA_TRY(cudaEventRecord(h->ev1, st));
+  V3DBA_CUDA_TRY(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  res->device_ms = ms;
+  res->iterations = it;
+  res->lambda = lambda;
+  h->lambda = lambda;
+  if (o.verbosity >= 2) printf("Leaving SparseLevenbergOptimizer::minimize().\n");
+  return V3DBA_OK;
+}
+
+extern "C" int v3dba_profile_stages(v3dba_handle h, int precision, int reps, double* ms) {
+  if (!h || !ms || reps <= 0) return V3DBA_ERR_INVALID_ARGUMENT;
+  DevState& s = h->s;
+  const Dims& D = s.d;
+  const LmOps* ops = lm_ops(D.model, D.DA, D.DC, precision == V3DBA_PRECISION_FP64);
+  if (!ops) return V3DBA_ERR_UNSUPPORTED;
+  cudaStream_t st = h->stream;
+  int rc;
+  // a valid state for every stage: linearise, damp with tau * max diagonal, build and solve once
+  if ((rc = ops->relinearize(s, true, 1e-3, st))) return rc;
+  V3DBA_CUDA_TRY(cudaMemsetAsync(s.d_fail, 0, sizeof(int), st));
+  if ((rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
+  if ((rc = ops->build_reduced(s, st))) return rc;
+  if ((rc = tile_chol_solve(h->chol, s.S, s.x, s.d_fail, st))) return rc;
+  if ((rc = ops->finish_trial(s, st))) return rc;
+  float t = 0.f;
+  for (int id = 0; id < kNumLmStages; ++id) {
+    V3DBA_CUDA_TRY(cudaEventRecord(h->ev0, st));
+    for (int r = 0; r < reps; ++r)
+      if ((rc = ops->stage(s, id, 0, 1e-3, st))) return rc;
+    V3DBA_CUDA_TRY(cudaEventRecord(h->ev1, st));
+    V3DBA_CUDA_TRY(cudaEventSynchronize(h->ev1));
+    cudaEventElapsedTime(&t, h->ev0, h->ev1);
+    ms[id] = t / reps;
+  }
+  // Cholesky factor + solve: rebuild the system before every timed factorisation
+  double chol = 0.0, zero = 0.0;
+  for (int r = 0; r < reps; ++r) {
+    V3DBA_CUDA_TRY(cudaEventRecord(h->ev0, st));
+    if ((rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
+    V3DBA_CUDA_TRY(cudaEventRecord(h->ev1, st));
+    V3DBA_CUDA_TRY(cudaEventSynchronize(h->ev1));
+    cudaEventElapsedTime(&t, h->ev0, h->ev1);
+    zero += t;
+    if ((rc = ops->build_reduced(s, st))) return rc;
+    V3DBA_CUDA_TRY(cudaEventRecord(h->ev0, st));
+    if ((rc = tile_chol_solve(h->chol, s.S, s.x, s.d_fail, st))) return rc;
+    V3DBA_CUDA_TRY(cudaEventRecord(h->ev1, st));
+    V3DBA_CUDA_TRY(cudaEventSynchronize(h->ev1));
+    cudaEventElapsedTime(&t, h->ev0, h->ev1);
+    chol += t;
+  }
+  ms[kNumLmStages] = chol / reps;
+  ms[kNumLmStages + 1] = zero / reps;
+  return V3DBA_OK;
+}
+
+namespace v3dba {
+DevState& handle_state(v3dba_handle h) { return h->s; }
+TileChol& handle_chol(v3dba_handle h) { return h->chol; }
+cudaStream_t handle_stream(v3dba_handle h) { return h->stream; }
+}  // namespace v3dba
