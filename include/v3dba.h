@@ -186,6 +186,21 @@ int v3dba_dims(int model, int mode, int* dA, int* dC);
  * host memory).  Returns V3DBA_OK and *fail = 1 when a pivot is not positive. */
 int v3dba_dense_cholesky_solve(int n, const double* S, const double* rhs, double* x, int* fail);
 
+/* Dense SPD solve that allocates nothing (no counterpart in the reference).  For callers that
+ * cannot allocate device memory where they solve: a loop that reserved its GPU memory up front
+ * and cannot afford cudaMalloc's implicit device synchronisation, or a host framework that owns
+ * every device allocation.  S (n x n row-major, lower triangle used), rhs, x (n) and fail (one
+ * int) are device buffers owned by the caller; all working memory is a fixed array compiled into
+ * the library (about 0.8 MB per GPU, held until the process exits), so n must not exceed
+ * V3DBA_NOALLOC_MAX_N (larger n is rejected with V3DBA_ERR_INVALID_ARGUMENT).  Calls share that
+ * array: calls that overlap on the GPU race and must not be issued.  The first call on a device
+ * looks up the array's device address and should come before any stream capture.  The work is
+ * enqueued on `stream` (a cudaStream_t, NULL for the default stream); synchronise before
+ * reading x or fail (1 when a pivot is not positive). */
+#define V3DBA_NOALLOC_MAX_N 256
+int v3dba_dense_cholesky_solve_noalloc(int n, const double* S, const double* rhs, double* x, int* fail,
+                                       void* stream);
+
 /* Batched independent problems (triplets / submodels), all of the same model and mode, solved
  * in one persistent launch.  Parameters of every problem are updated in place; results[i]
  * receives problem i's outcome. */
