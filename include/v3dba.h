@@ -235,6 +235,26 @@ enum {
  * counterpart in the reference.) */
 int v3dba_profile_stages(v3dba_handle h, int precision, int reps, double* ms);
 
+/* Device-resident batch of independent problems (StdMetricBundleOptimizer, at most 4 cameras
+ * each; triplets and small submodels).  One persistent launch runs the full LM loop of every
+ * problem, one thread block per problem at a time, largest problems first. */
+typedef struct v3dba_batch_s* v3dba_batch_t;
+int v3dba_batch_create(const v3dba_problem* problems, int count, v3dba_batch_t* out);
+int v3dba_batch_destroy(v3dba_batch_t b);
+/* results (may be NULL) receives one entry per problem; device_ms (may be NULL) the device time. */
+int v3dba_batch_minimize(v3dba_batch_t b, const v3dba_options* opts, v3dba_result* results, double* device_ms);
+/* Restores the parameters the batch was created with. */
+int v3dba_batch_reset(v3dba_batch_t b);
+/* Schedule: the first `split` problems of the size order run with `large_threads` threads per
+ * block, the rest with `small_threads` (64, 128 or 256). */
+int v3dba_batch_set_schedule(v3dba_batch_t b, int large_threads, int small_threads, int split);
+/* Times candidate schedules on the batch itself (restoring the parameters after each) and keeps
+ * the fastest; reports it when the pointers are not NULL. */
+int v3dba_batch_autotune(v3dba_batch_t b, const v3dba_options* opts, int* large_threads, int* small_threads,
+                         int* split);
+int v3dba_batch_get_params(v3dba_batch_t b, int index, double* R, double* T, double* X);
+int v3dba_batch_get_all_params(v3dba_batch_t b, double* R, double* T, double* X);
+
 /* Kernel launches issued by this library in the calling process so far. */
 uint64_t v3dba_launch_count(void);
 

@@ -1,0 +1,67 @@
+"""The drop-in C++ header (include/v3d_b200/v3d_metricbundle.h) used the way the reference's
+pipeline uses its optimizer: tests/shim/shim_demo.cpp is compiled against the reference's own
+headers, constructs the optimizer classes with the reference's signatures and calls minimize().
+Its results must match the reference's (golden fixtures)."""
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from v3dsfmtoolkit_b200 import capi
+from tests.helpers import golden_names, load_golden, param_rel
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DEMO = os.path.join(ROOT, "tests", "shim", "_build", "shim_demo")
+
+
+def _write_scene(path, sc, max_iterations, precision, nv):
+    with open(path, "wb") as f:
+        f.write(struct.pack("<10i", sc.model, sc.mode, sc.n_cams, sc.n_points, sc.n_obs, max_iterations,
+                            precision, *nv))
+        f.write(struct.pack("<d", sc.inlier_threshold))
+        for a in (sc.K, sc.R, sc.T):
+            f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+        if sc.dist is not None:
+            f.write(np.ascontiguousarray(sc.dist, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(sc.X, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(sc.meas, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(sc.view, dtype=np.int32).tobytes())
+        f.write(np.ascontiguousarray(sc.point, dtype=np.int32).tobytes())
+
+
+def _read_out(path, sc):
+    b = open(path, "rb").read()
+    status, iters = struct.unpack_from("<2i", b, 0)
+    off = 8
+    out = []
+    for shape in (sc.K.shape, sc.R.shape, sc.T.shape, None if sc.dist is None else sc.dist.shape, sc.X.shape):
+        if shape is None:
+            out.append(None)
+            continue
+        n = int(np.prod(shape))
+        out.append(np.frombuffer(b, dtype=np.float64, count=n, offset=off).reshape(shape))
+        off += 8 * n
+    return status, iters, out
+
+
+@pytest.mark.skipif(not os.path.exists(DEMO), reason="shim demo not built (needs the reference headers at build time)")
+@pytest.mark.parametrize("name", golden_names())
+def test_dropin_header_matches_reference(name):
+    sc, g = load_golden(name)
+    nv = tuple(int(v) for v in g["nonvarying"])
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "scene.bin"), os.path.join(d, "out.bin")
+        _write_scene(sp, sc, int(g["max_iterations"]), capi.PRECISION_FP64, nv)
+        r = subprocess.run([DEMO, sp, op], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        status, iters, (K, R, T, dist, X) = _read_out(op, sc)
+    assert status == int(g["status"])
+    assert iters == int(g["iterations"])
+    assert param_rel((K, R, T, X), (g["K"], g["R"], g["T"], g["X"])) < 1e-5
+    if sc.dist is not None:
+        assert param_rel((dist,), (g["dist"],)) < 1e-4 or np.abs(dist - g["dist"]).max() < 1e-9

@@ -28,7 +28,9 @@ EXPORTS = (
     "v3dba_set_lambda", "v3dba_minimize", "v3dba_set_params", "v3dba_get_params",
     "v3dba_reset_params", "v3dba_cost", "v3dba_linearize", "v3dba_reduced_system", "v3dba_dims",
     "v3dba_dense_cholesky_solve", "v3dba_minimize_batched", "v3dba_launch_count",
-    "v3dba_error_string", "v3dba_profile_stages",
+    "v3dba_error_string", "v3dba_profile_stages", "v3dba_batch_create", "v3dba_batch_destroy",
+    "v3dba_batch_minimize", "v3dba_batch_reset", "v3dba_batch_set_schedule", "v3dba_batch_autotune",
+    "v3dba_batch_get_params", "v3dba_batch_get_all_params",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -92,6 +94,14 @@ def _lib():
         L.v3dba_minimize_batched.argtypes = [C.POINTER(Problem), C.c_int, C.POINTER(Options)] + \
             [C.POINTER(_dp)] * 5 + [C.POINTER(Result)]
         L.v3dba_profile_stages.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+        L.v3dba_batch_create.argtypes = [C.POINTER(Problem), C.c_int, C.POINTER(C.c_void_p)]
+        L.v3dba_batch_destroy.argtypes = [C.c_void_p]
+        L.v3dba_batch_minimize.argtypes = [C.c_void_p, C.POINTER(Options), C.POINTER(Result), _dp]
+        L.v3dba_batch_reset.argtypes = [C.c_void_p]
+        L.v3dba_batch_set_schedule.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.v3dba_batch_autotune.argtypes = [C.c_void_p, C.POINTER(Options)] + [C.POINTER(C.c_int)] * 3
+        L.v3dba_batch_get_params.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
+        L.v3dba_batch_get_all_params.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -231,3 +241,61 @@ def dense_cholesky_solve(S, rhs):
     check(_lib().v3dba_dense_cholesky_solve(S.shape[0], _d(S), _d(rhs), _d(x), C.byref(fail)),
           "v3dba_dense_cholesky_solve")
     return x, bool(fail.value)
+
+
+class Batch:
+    """Many small independent problems (StdMetricBundleOptimizer, <= 4 cameras each) solved in one
+    persistent launch (wraps v3dba_batch_*)."""
+
+    def __init__(self, scenes):
+        L = _lib()
+        self.scenes = list(scenes)
+        self._keep = []
+        probs = (Problem * len(self.scenes))()
+        for i, sc in enumerate(self.scenes):
+            arrs = [_f64(sc.K), _f64(sc.R), _f64(sc.T), _f64(sc.X), _f64(sc.meas),
+                    np.ascontiguousarray(sc.view, dtype=np.int32), np.ascontiguousarray(sc.point, dtype=np.int32)]
+            self._keep.append(arrs)
+            K_, R_, T_, X_, m_, v_, p_ = arrs
+            probs[i] = Problem(sc.model, sc.mode, sc.n_cams, sc.n_points, sc.n_obs, float(sc.inlier_threshold),
+                               _d(K_), _d(R_), _d(T_), None, _d(X_), _d(m_), v_.ctypes.data_as(_ip), p_.ctypes.data_as(_ip))
+        h = C.c_void_p()
+        check(L.v3dba_batch_create(probs, len(self.scenes), C.byref(h)), "v3dba_batch_create")
+        self.h = h
+        self.count = len(self.scenes)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            _lib().v3dba_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def minimize(self, options: Options | None = None, want_results=True, **kw):
+        o = options if options is not None else default_options(**kw)
+        res = (Result * self.count)() if want_results else None
+        ms = C.c_double()
+        check(_lib().v3dba_batch_minimize(self.h, C.byref(o), res, C.byref(ms)), "v3dba_batch_minimize")
+        return (list(res) if want_results else None), ms.value
+
+    def reset(self):
+        check(_lib().v3dba_batch_reset(self.h), "v3dba_batch_reset")
+
+    def set_schedule(self, large_threads, small_threads, split):
+        check(_lib().v3dba_batch_set_schedule(self.h, large_threads, small_threads, split), "v3dba_batch_set_schedule")
+
+    def autotune(self, options: Options | None = None, **kw):
+        o = options if options is not None else default_options(**kw)
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(_lib().v3dba_batch_autotune(self.h, C.byref(o), C.byref(a), C.byref(b), C.byref(c)), "v3dba_batch_autotune")
+        return a.value, b.value, c.value
+
+    def get_params(self, i):
+        sc = self.scenes[i]
+        R, T, X = np.zeros((sc.n_cams, 3, 3)), np.zeros((sc.n_cams, 3)), np.zeros((sc.n_points, 3))
+        check(_lib().v3dba_batch_get_params(self.h, i, _d(R), _d(T), _d(X)), "v3dba_batch_get_params")
+        return R, T, X

@@ -200,10 +200,3 @@ extern "C" int v3dba_dense_cholesky_solve(int n, const double* S, const double* 
   tile_chol_free(tc);
   return rc;
 }
-
-extern "C" int v3dba_minimize_batched(const v3dba_problem* problems, int count, const v3dba_options* opts,
-                                      double* const* K, double* const* R, double* const* T,
-                                      double* const* dist, double* const* X, v3dba_result* results) {
-  (void)problems; (void)count; (void)opts; (void)K; (void)R; (void)T; (void)dist; (void)X; (void)results;
-  return V3DBA_ERR_UNSUPPORTED;
-}
