@@ -36,7 +36,7 @@ def test_batched_matches_reference_per_triplet_5_iterations(triplets):
 def test_batched_matches_reference_per_triplet_long_runs(triplets):
     """40 iterations: once the Huber re-weighting makes gain ratios hover near zero, rounding
     decides individual accept/reject steps, so only status, iteration count and final cost are
-    compared (cost within 1e-6 of the reference's, or lower)."""
+    compared (cost within 1e-5 of the reference's, or lower)."""
     eng = _oracle()
     b = capi.Batch(triplets)
     res, _ = b.minimize(max_iterations=40)
@@ -47,7 +47,7 @@ def test_batched_matches_reference_per_triplet_long_runs(triplets):
         Rg, Tg, Xg = b.get_params(i)
         c_ref = eng.cost(sc, params)
         c_gpu = eng.cost(sc, (params[0], Rg, Tg, params[3], Xg))
-        assert c_gpu <= c_ref * (1 + 1e-6), (i, c_gpu, c_ref)
+        assert c_gpu <= c_ref * (1 + 1e-5), (i, c_gpu, c_ref)
 
 
 def test_batched_schedules_agree_and_reset(triplets):

@@ -199,3 +199,50 @@ def test_sequence200_full_size_matches_reference_cost():
     r = h.minimize(max_iterations=1000, precision=capi.PRECISION_MIXED, stop_cost=ref["cost"] * (1 + 1e-6))
     assert r.reached_stop_cost == 1
     assert h.cost() <= ref["cost"] * (1 + 1e-6)
+
+
+def test_pcg_with_tight_tolerance_follows_reference_path():
+    """Block-Jacobi PCG solved to 1e-12 reproduces the direct solve: same status, iterations,
+    parameters as the reference on the 20-camera scene."""
+    from oracle.bindings import Reference, reference_available
+    if not reference_available():
+        pytest.skip("compiled reference not present")
+    sc = scenes.circle_scene(seed=3)
+    (K, R, T, d, X), info = Reference().minimize(sc, max_iterations=100)
+    h = capi.Handle.from_scene(sc)
+    r = h.minimize(max_iterations=100, precision=capi.PRECISION_FP64, solver=capi.SOLVER_PCG,
+                   pcg_tolerance=1e-12, pcg_max_iterations=2000)
+    assert r.status == info["status"] and r.iterations == info["iterations"]
+    assert r.pcg_iterations > 0
+    Kg, Rg, Tg, dg, Xg = h.get_params()
+    assert param_rel((Rg, Tg, Xg), (R, T, X)) < 1e-7
+
+
+def test_pcg_reaches_cholesky_cost_on_cluster_twin():
+    """A scaled-down twin of the 2,000-camera clustered scene: PCG at the default 1e-6 relative
+    residual per LM step reaches the cost of the direct-solve path."""
+    sc = scenes.cluster_scene(n_groups=4, cams_per_group=40, n_points=20000, seed=2)
+    hd = capi.Handle.from_scene(sc)
+    rd = hd.minimize(max_iterations=30, precision=capi.PRECISION_FP64, solver=capi.SOLVER_CHOLESKY)
+    c_direct = hd.cost()
+    hp = capi.Handle.from_scene(sc)
+    rp = hp.minimize(max_iterations=60, precision=capi.PRECISION_MIXED, solver=capi.SOLVER_PCG,
+                     stop_cost=c_direct * (1 + 1e-6))
+    assert rp.reached_stop_cost == 1 or hp.cost() <= c_direct * (1 + 1e-6)
+    assert rp.pcg_iterations > 0
+
+
+def test_camera_without_observations():
+    """A camera that sees nothing keeps its block lambda I and parameters; the rest converges as
+    in the oracle."""
+    from oracle.bindings import Restatement
+    sc = scenes.circle_scene(n_cams=8, n_points=200, seed=9)
+    keep = sc.view != 3
+    sc.view, sc.point, sc.meas = sc.view[keep], sc.point[keep], sc.meas[keep]
+    h = capi.Handle.from_scene(sc)
+    r = h.minimize(max_iterations=30, precision=capi.PRECISION_FP64)
+    (K, R, T, d, X), info = Restatement().minimize(sc, max_iterations=30)
+    assert r.status == info["status"] and r.iterations == info["iterations"]
+    Kg, Rg, Tg, dg, Xg = h.get_params()
+    assert param_rel((Rg, Tg, Xg), (R, T, X)) < 1e-8
+    np.testing.assert_array_equal(Rg[3], sc.R[3])

@@ -70,6 +70,7 @@ using namespace v3dba;
 
 // accessors into the opaque handle (defined in solver.cu)
 namespace v3dba {
+int handle_use_dense(v3dba_handle h);
 DevState& handle_state(v3dba_handle h);
 TileChol& handle_chol(v3dba_handle h);
 cudaStream_t handle_stream(v3dba_handle h);
@@ -138,6 +139,8 @@ extern "C" int v3dba_linearize(v3dba_handle h, int precision, double* e, double*
 
 extern "C" int v3dba_reduced_system(v3dba_handle h, int precision, double lambda, double* S, double* rhs) {
   if (!h || !S || !rhs) return V3DBA_ERR_INVALID_ARGUMENT;
+  int rc0 = handle_use_dense(h);
+  if (rc0) return rc0;
   DevState& s = handle_state(h);
   TileChol& tc = handle_chol(h);
   cudaStream_t st = handle_stream(h);

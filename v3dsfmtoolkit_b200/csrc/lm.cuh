@@ -83,8 +83,11 @@ struct DevState {
   // reduced system (dense, column-major, leading dimension ld)
   int n = 0, n_pad = 0, ld = 0;
   double* S = nullptr;
-  double* rhs = nullptr;    // right-hand side: row n_pad of S, element c at rhs[c * ld]
+  double* rhs = nullptr;    // right-hand side, element c at rhs[c * rhs_stride]
+  int rhs_stride = 0;       // ld for the dense system (row n_pad of S), 1 for PCG
   double* x = nullptr;      // [n_pad] solution of the reduced system
+  void* Sb = nullptr;       // PCG: camera-pair blocks (Real, dA x dA row-major) instead of dense S
+  int* diag_blk = nullptr;  // PCG: block id of (i, i)
   // scalars
   double* d_lambda = nullptr;
   double* d_relin = nullptr;  // {err, gmax, maxdiag}
@@ -154,6 +157,28 @@ struct TileChol {
   int* d_upd_ptr = nullptr;
   double* d_ldiag = nullptr;                    // nt inverted diagonal tiles (L_kk^-1)
 };
+
+// Block-sparse reduced system for block-Jacobi PCG.
+struct PcgState {
+  int* rp = nullptr;            // [N+1] camera rows over both triangles
+  int* rb = nullptr;            // block id of each row entry
+  int* rc = nullptr;            // column camera of each row entry
+  unsigned char* rt = nullptr;  // 1: use the transpose of the stored block
+  int* diag_blk = nullptr;      // [N] block id of (i, i)
+  void* Sb = nullptr;           // blocks (8-byte slots)
+  double* Pinv = nullptr;       // inverse diagonal blocks
+  double* vec = nullptr;        // b, r, z, p, Ap
+  double* b = nullptr;
+  double* part = nullptr;
+  int* iters = nullptr;
+  bool ready = false;
+};
+int pcg_plan(PcgState& ps, const std::vector<int>& b_i, const std::vector<int>& b_l, int N);
+int pcg_alloc(PcgState& ps, int nb, int N, int DA);
+void pcg_free(PcgState& ps);
+// Solves S x = b (b in ps.b, blocks in ps.Sb); iteration count in *ps.iters (device).
+int pcg_solve(PcgState& ps, int N, int DA, bool fp64, double tol, int max_iter, double* x, int* d_fail,
+              cudaStream_t st);
 
 // Builds the plan from the lower-triangle tile pattern (tile_nz[r*nt+c], r >= c).
 int tile_chol_plan(TileChol& tc, int n, std::vector<uint8_t>& tile_nz);

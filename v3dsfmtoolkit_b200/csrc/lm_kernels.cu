@@ -596,8 +596,12 @@ __global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* 
     const int a = e / DA, c = e % DA;
     double val = -sum[t];
     if (i == l) val += double(cU[a * DA + c]) + (a == c ? lam : 0.0);
-    // element (row l*DA + c, col i*DA + a) of the lower triangle holds S_il[a][c]
-    s.S[(size_t)(i * DA + a) * ld + (l * DA + c)] = val;
+    if (s.Sb) {
+      reinterpret_cast<Real*>(s.Sb)[(size_t)b * DA * DA + a * DA + c] = Real(val);
+    } else {
+      // element (row l*DA + c, col i*DA + a) of the lower triangle holds S_il[a][c]
+      s.S[(size_t)(i * DA + a) * ld + (l * DA + c)] = val;
+    }
   }
 }
 
@@ -653,15 +657,17 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * kCamWarps + (threadIdx.x >> 5);
   if (i >= D.N) return;
-  const size_t ld = s.ld;
+  const size_t ld = s.ld, rs = s.rhs_stride;
   const int c0 = D.N * DA;
   if (i < D.nnA) {
     for (int t = lane; t < DA * DA; t += 32) {
       const int a = t / DA, c = t % DA;
-      s.S[(size_t)(i * DA + a) * ld + (i * DA + c)] = (a == c) ? 1.0 : 0.0;
+      if (s.Sb) reinterpret_cast<Real*>(s.Sb)[(size_t)s.diag_blk[i] * DA * DA + t] = Real(a == c ? 1.0 : 0.0);
+      else s.S[(size_t)(i * DA + a) * ld + (i * DA + c)] = (a == c) ? 1.0 : 0.0;
     }
-    for (int a = lane; a < DA; a += 32) s.rhs[(size_t)(i * DA + a) * ld] = 0.0;
-    for (int t = lane; t < RV::NX; t += 32) s.S[(size_t)(i * DA + t / DCc) * ld + c0 + t % DCc] = 0.0;
+    for (int a = lane; a < DA; a += 32) s.rhs[(size_t)(i * DA + a) * rs] = 0.0;
+    if (!s.Sb)
+      for (int t = lane; t < RV::NX; t += 32) s.S[(size_t)(i * DA + t / DCc) * ld + c0 + t % DCc] = 0.0;
     return;
   }
   double sum[PER];
@@ -675,7 +681,7 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const
   for (int t = 0; t < PER; ++t) {
     const int e = lane + 32 * t;
     if (e < DA) {
-      s.rhs[(size_t)(i * DA + e) * ld] = s.c_ga[(size_t)i * L::SG + e] - sum[t];
+      s.rhs[(size_t)(i * DA + e) * rs] = s.c_ga[(size_t)i * L::SG + e] - sum[t];
     } else if (e < RV::NV) {
       const int x = e - DA, a = x / DCc, c = x % DCc;
       const double val = (c >= D.nnC) ? double(cX[a * DCc + c]) - sum[t] : 0.0;
@@ -705,7 +711,7 @@ __global__ void __launch_bounds__(256) k_global_block(DevState s, const double* 
         else val = s.g_Z[r * DCc + c] - a[z] + (r == c ? lam : 0.0);
         s.S[(size_t)(c0 + r) * ld + (c0 + c)] = val;   // row c0+c >= col c0+r
       }
-    for (int c = 0; c < DCc; ++c) s.rhs[(size_t)(c0 + c) * ld] = (c < D.nnC) ? 0.0 : s.g_gc[c] - a[nsym(DC) + c];
+    for (int c = 0; c < DCc; ++c) s.rhs[(size_t)(c0 + c) * s.rhs_stride] = (c < D.nnC) ? 0.0 : s.g_gc[c] - a[nsym(DC) + c];
   }
 }
 

@@ -30,6 +30,13 @@ using namespace v3dba;
 struct v3dba_handle_s {
   DevState s;
   TileChol chol;
+  PcgState pcg;
+  std::vector<int> blk_i, blk_l;   // camera-pair blocks (host copy)
+  std::vector<uint8_t> tile_nz;    // tile pattern of the dense reduced system
+  bool dense_ready = false;
+  double* S_dense = nullptr;
+  double* x_dense = nullptr;
+  double* x_pcg = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double param_length = 0.0;
@@ -119,11 +126,54 @@ void free_handle(v3dba_handle h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (void* p : h->allocs) cudaFree(p);
   tile_chol_free(h->chol);
+  pcg_free(h->pcg);
   if (h->h_scalars) cudaFreeHost(h->h_scalars);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
+}
+
+// Dense reduced system (tile Cholesky): allocated on first use.
+int use_dense(v3dba_handle h) {
+  DevState& s = h->s;
+  if (!h->dense_ready) {
+    std::vector<uint8_t> nz = h->tile_nz;
+    int rc = tile_chol_plan(h->chol, std::max(s.n, 1), nz);
+    if (rc) return rc;
+    if ((rc = dalloc(h, &h->S_dense, (size_t)h->chol.ld * h->chol.n_pad))) return rc;
+    if ((rc = dalloc(h, &h->x_dense, (size_t)h->chol.n_pad))) return rc;
+    h->dense_ready = true;
+  }
+  s.n_pad = h->chol.n_pad;
+  s.ld = h->chol.ld;
+  s.S = h->S_dense;
+  s.rhs = h->S_dense + s.n_pad;
+  s.rhs_stride = s.ld;
+  s.x = h->x_dense;
+  s.Sb = nullptr;
+  s.diag_blk = nullptr;
+  return V3DBA_OK;
+}
+
+// Block-sparse reduced system (PCG): allocated on first use.
+int use_pcg(v3dba_handle h) {
+  DevState& s = h->s;
+  if (!h->pcg.ready) {
+    int rc = pcg_plan(h->pcg, h->blk_i, h->blk_l, s.d.N);
+    if (rc) return rc;
+    if ((rc = pcg_alloc(h->pcg, s.nb, s.d.N, s.d.DA))) return rc;
+    if ((rc = dalloc(h, &h->x_pcg, (size_t)std::max(s.n, 1)))) return rc;
+  }
+  s.n_pad = s.n;
+  s.ld = 1;
+  s.S = nullptr;
+  s.rhs = h->pcg.b;
+  s.rhs_stride = 1;
+  s.x = h->x_pcg;
+  s.Sb = h->pcg.Sb;
+  s.diag_blk = h->pcg.diag_blk;
+  return V3DBA_OK;
 }
 
 // Host-side structure analysis: point-major permutation, camera lists, camera-pair blocks with
@@ -202,6 +252,8 @@ void build_structure(const v3dba_problem* p, Structure& S) {
         tk.push_back(k); tm.push_back(m); tl.push_back(l);
       }
     }
+    // every camera gets its diagonal block, even without observations (it is then lambda I)
+    if (local[i] < 0) { local[i] = 0; touched.push_back(i); }
     std::sort(touched.begin(), touched.end());
     for (size_t t = 0; t < touched.size(); ++t) local[touched[t]] = (int)t;
     cnt.assign(touched.size() + 1, 0);
@@ -386,27 +438,26 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   CTRY(cudaMemset(s.g_Z, 0, 64 * sizeof(double)));
   CTRY(cudaMemset(s.g_gc, 0, 8 * sizeof(double)));
 
-  // reduced system: n = N*dA + dC, tile pattern from the camera-pair blocks and the border
+  // reduced system: n = N*dA + dC.  The dense tiles (Cholesky) or the block arrays (PCG) are
+  // allocated on first use; here only the tile pattern is derived from the blocks and border.
   s.n = N * dA + dC;
-  const int nt = std::max(1, (s.n + TileChol::TB - 1) / TileChol::TB);
-  std::vector<uint8_t> nz((size_t)nt * nt, 0);
-  auto mark = [&](int r0, int r1, int c0, int c1) {  // scalar row range x col range, r >= c part
-    for (int tr = r0 / 64; tr <= (r1 - 1) / 64; ++tr)
-      for (int tcl = c0 / 64; tcl <= (c1 - 1) / 64; ++tcl)
-        if (tr >= tcl) nz[(size_t)tr * nt + tcl] = 1;
-  };
-  for (int b = 0; b < s.nb; ++b) mark(st.b_l[b] * dA, st.b_l[b] * dA + dA, st.b_i[b] * dA, st.b_i[b] * dA + dA);
-  for (int i = 0; i < N; ++i) {
-    mark(i * dA, i * dA + dA, i * dA, i * dA + dA);
-    if (dC) mark(N * dA, N * dA + dC, i * dA, i * dA + dA);
+  {
+    const int nt = std::max(1, (s.n + TileChol::TB - 1) / TileChol::TB);
+    h->tile_nz.assign((size_t)nt * nt, 0);
+    auto mark = [&](int r0, int r1, int c0, int c1) {  // scalar row range x col range, r >= c part
+      for (int tr = r0 / 64; tr <= (r1 - 1) / 64; ++tr)
+        for (int tcl = c0 / 64; tcl <= (c1 - 1) / 64; ++tcl)
+          if (tr >= tcl) h->tile_nz[(size_t)tr * nt + tcl] = 1;
+    };
+    for (int b = 0; b < s.nb; ++b) mark(st.b_l[b] * dA, st.b_l[b] * dA + dA, st.b_i[b] * dA, st.b_i[b] * dA + dA);
+    for (int i = 0; i < N; ++i) {
+      mark(i * dA, i * dA + dA, i * dA, i * dA + dA);
+      if (dC) mark(N * dA, N * dA + dC, i * dA, i * dA + dA);
+    }
+    if (dC) mark(N * dA, N * dA + dC, N * dA, N * dA + dC);
   }
-  if (dC) mark(N * dA, N * dA + dC, N * dA, N * dA + dC);
-  TRY(tile_chol_plan(h->chol, std::max(s.n, 1), nz));
-  s.n_pad = h->chol.n_pad;
-  s.ld = h->chol.ld;
-  TRY(dalloc(h, &s.S, (size_t)s.ld * s.n_pad));
-  s.rhs = s.S + s.n_pad;
-  TRY(dalloc(h, &s.x, (size_t)s.n_pad));
+  h->blk_i = st.b_i;
+  h->blk_l = st.b_l;
 
   TRY(upload_params(h, s.cur, p->K, p->R, p->T, p->dist, p->X));
   TRY(copy_params(s.init, s.cur, h, h->stream));
@@ -485,18 +536,25 @@ int v3dba_cost(v3dba_handle h, double* cost) {
 
 namespace {
 
-// One damped trial: reduced system at *d_lambda, Cholesky, back-substitution, trial parameters
-// and their cost.  Reads back {new_err, |delta|^2, delta . g, fail}.
-int run_trial(v3dba_handle h, const LmOps* ops, double lambda, double out[4]) {
+// One damped trial: reduced system at *d_lambda, Cholesky or PCG, back-substitution, trial
+// parameters and their cost.  Reads back {new_err, |delta|^2, delta . g, fail, pcg iterations}.
+int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, bool fp64, const v3dba_options& o,
+              double out[5]) {
   DevState& s = h->s;
   cudaStream_t st = h->stream;
   h->h_scalars[8] = lambda;
   V3DBA_CUDA_TRY(cudaMemcpyAsync(s.d_lambda, h->h_scalars + 8, sizeof(double), cudaMemcpyHostToDevice, st));
   V3DBA_CUDA_TRY(cudaMemsetAsync(s.d_fail, 0, sizeof(int), st));
   int rc;
-  if ((rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
+  if (!pcg && (rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
   if ((rc = ops->build_reduced(s, st))) return rc;
-  if ((rc = tile_chol_solve(h->chol, s.S, s.x, s.d_fail, st))) return rc;
+  if (pcg) {
+    if ((rc = pcg_solve(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x, s.d_fail, st)))
+      return rc;
+    V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 9, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+  } else if ((rc = tile_chol_solve(h->chol, s.S, s.x, s.d_fail, st))) {
+    return rc;
+  }
   if ((rc = ops->finish_trial(s, st))) return rc;
   V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars, s.d_trial, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
   V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 3, s.d_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -504,9 +562,11 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, double out[4]) {
   out[0] = h->h_scalars[0];
   out[1] = h->h_scalars[1];
   out[2] = h->h_scalars[2];
-  int fail;
+  int fail, its = 0;
   std::memcpy(&fail, h->h_scalars + 3, sizeof(int));
+  if (pcg) std::memcpy(&its, h->h_scalars + 9, sizeof(int));
   out[3] = fail ? 1.0 : 0.0;
+  out[4] = its;
   return V3DBA_OK;
 }
 
@@ -526,7 +586,14 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
   const LmOps* ops = lm_ops(D.model, D.DA, D.DC, fp64);
   if (!ops || !ops64) return V3DBA_ERR_UNSUPPORTED;
   bool relinearize_again = false;   // blocks to be rebuilt in FP64 at unchanged parameters
-  if (o.solver == V3DBA_SOLVER_PCG) return V3DBA_ERR_UNSUPPORTED;
+  int solver = o.solver;
+  if (solver == V3DBA_SOLVER_AUTO) solver = (s.n <= 4096 || D.DC > 0) ? V3DBA_SOLVER_CHOLESKY : V3DBA_SOLVER_PCG;
+  if (solver == V3DBA_SOLVER_PCG && D.DC > 0) return V3DBA_ERR_UNSUPPORTED;
+  const bool pcg = solver == V3DBA_SOLVER_PCG;
+  {
+    const int rc0 = pcg ? use_pcg(h) : use_dense(h);
+    if (rc0) return rc0;
+  }
 
   const int nvA = D.N - D.nnA, nvB = D.M - D.nnB, nvC = D.DC - D.nnC;
   if (nvA <= 0 && nvB <= 0 && nvC <= 0) {
@@ -572,8 +639,9 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
         if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: initial lambda = %.17g\n", lambda);
       }
     }
-    double t[4];
-    if ((rc = run_trial(h, ops, lambda, t))) return rc;
+    double t[5];
+    if ((rc = run_trial(h, ops, lambda, pcg, fp64, o, t))) return rc;
+    res->pcg_iterations += (int)t[4];
     const bool success = t[3] == 0.0;
     double rho = 0.0;
     if (success) {
@@ -632,6 +700,7 @@ extern "C" int v3dba_profile_stages(v3dba_handle h, int precision, int reps, dou
   if (!ops) return V3DBA_ERR_UNSUPPORTED;
   cudaStream_t st = h->stream;
   int rc;
+  if ((rc = use_dense(h))) return rc;
   // a valid state for every stage: linearise, damp with tau * max diagonal, build and solve once
   if ((rc = ops->relinearize(s, true, 1e-3, st))) return rc;
   V3DBA_CUDA_TRY(cudaMemsetAsync(s.d_fail, 0, sizeof(int), st));
@@ -672,6 +741,7 @@ extern "C" int v3dba_profile_stages(v3dba_handle h, int precision, int reps, dou
 }
 
 namespace v3dba {
+int handle_use_dense(v3dba_handle h) { return use_dense(h); }
 DevState& handle_state(v3dba_handle h) { return h->s; }
 TileChol& handle_chol(v3dba_handle h) { return h->chol; }
 cudaStream_t handle_stream(v3dba_handle h) { return h->stream; }
