@@ -255,6 +255,15 @@ int v3dba_batch_autotune(v3dba_batch_t b, const v3dba_options* opts, int* large_
 int v3dba_batch_get_params(v3dba_batch_t b, int index, double* R, double* T, double* X);
 int v3dba_batch_get_all_params(v3dba_batch_t b, double* R, double* T, double* X);
 
+/* FP64 tensor-core (DMMA) throughput of the current GPU in TFLOP/s, measured by a short kernel
+ * of independent mma.sync f64 chains on every SM (benchmark support). */
+int v3dba_measure_fp64_mma_peak(double* tflops);
+
+/* FLOPs the tile Cholesky executes per factor + solve of this problem's dense reduced system
+ * (64^3 GEMM tiles of its panel and trailing tasks plus the diagonal factors; benchmark
+ * support). */
+int v3dba_cholesky_flops(v3dba_handle h, double* flops);
+
 /* Kernel launches issued by this library in the calling process so far. */
 uint64_t v3dba_launch_count(void);
 

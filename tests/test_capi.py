@@ -17,7 +17,7 @@ def _declared_symbols():
     for h in os.listdir(os.path.join(ROOT, "include")):
         if h.endswith(".h"):
             txt = open(os.path.join(ROOT, "include", h)).read()
-            syms |= set(re.findall(r"\b(v3dba_[a-z_]+)\s*\(", txt))
+            syms |= set(re.findall(r"\b(v3dba_\w+)\s*\(", txt))
     return syms
 
 

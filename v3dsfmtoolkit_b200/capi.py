@@ -30,7 +30,8 @@ EXPORTS = (
     "v3dba_dense_cholesky_solve", "v3dba_minimize_batched", "v3dba_launch_count",
     "v3dba_error_string", "v3dba_profile_stages", "v3dba_batch_create", "v3dba_batch_destroy",
     "v3dba_batch_minimize", "v3dba_batch_reset", "v3dba_batch_set_schedule", "v3dba_batch_autotune",
-    "v3dba_batch_get_params", "v3dba_batch_get_all_params",
+    "v3dba_batch_get_params", "v3dba_batch_get_all_params", "v3dba_measure_fp64_mma_peak",
+    "v3dba_cholesky_flops", "v3dba_dense_cholesky_solve_noalloc",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -102,6 +103,8 @@ def _lib():
         L.v3dba_batch_autotune.argtypes = [C.c_void_p, C.POINTER(Options)] + [C.POINTER(C.c_int)] * 3
         L.v3dba_batch_get_params.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
         L.v3dba_batch_get_all_params.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.v3dba_measure_fp64_mma_peak.argtypes = [_dp]
+        L.v3dba_cholesky_flops.argtypes = [C.c_void_p, _dp]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -140,6 +143,12 @@ def dims(model, mode):
     a, c = C.c_int(), C.c_int()
     check(_lib().v3dba_dims(model, mode, C.byref(a), C.byref(c)), "v3dba_dims")
     return a.value, c.value
+
+
+def fp64_mma_peak_tflops() -> float:
+    t = C.c_double()
+    check(_lib().v3dba_measure_fp64_mma_peak(C.byref(t)), "v3dba_measure_fp64_mma_peak")
+    return t.value
 
 
 def launch_count() -> int:
@@ -225,6 +234,11 @@ class Handle:
         ms = np.zeros(len(STAGES))
         check(_lib().v3dba_profile_stages(self.h, precision, reps, _d(ms)), "v3dba_profile_stages")
         return dict(zip(STAGES, ms.tolist()))
+
+    def cholesky_flops(self) -> float:
+        f = C.c_double()
+        check(_lib().v3dba_cholesky_flops(self.h, C.byref(f)), "v3dba_cholesky_flops")
+        return f.value
 
     def reduced_system(self, lam, precision=PRECISION_FP64):
         n = self.n_cams * self.dA + self.dC

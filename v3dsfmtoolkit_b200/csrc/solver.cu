@@ -740,6 +740,24 @@ extern "C" int v3dba_profile_stages(v3dba_handle h, int precision, int reps, dou
   return V3DBA_OK;
 }
 
+extern "C" int v3dba_cholesky_flops(v3dba_handle h, double* flops) {
+  if (!h || !flops) return V3DBA_ERR_INVALID_ARGUMENT;
+  const int rc = use_dense(h);
+  if (rc) return rc;
+  const TileChol& tc = h->chol;
+  const double gemm = 2.0 * 64.0 * 64.0 * 64.0;
+  // per tile column: the diagonal factor (L and L^-1, about 2/3 + 1/3 of 64^3) and one GEMM per
+  // panel tile and per trailing tile
+  double f = 0.0;
+  for (int k = 0; k < tc.nt; ++k) {
+    f += 64.0 * 64.0 * 64.0;
+    f += gemm * (tc.h_panel_ptr[k + 1] - tc.h_panel_ptr[k]);
+    f += gemm * (tc.h_upd_ptr[k + 1] - tc.h_upd_ptr[k]);
+  }
+  *flops = f;
+  return V3DBA_OK;
+}
+
 namespace v3dba {
 int handle_use_dense(v3dba_handle h) { return use_dense(h); }
 DevState& handle_state(v3dba_handle h) { return h->s; }
