@@ -51,7 +51,8 @@ enum {
   V3DBA_ERR_OUT_OF_MEMORY = 4,      /* device allocation failed                            */
   V3DBA_ERR_NO_DEVICE = 5,          /* no CUDA device                                       */
   V3DBA_ERR_UNSUPPORTED = 6,        /* a configuration this build does not handle           */
-  V3DBA_ERR_TIMEOUT = 7             /* a bounded device-side wait gave up                   */
+  V3DBA_ERR_TIMEOUT = 7,            /* a bounded device-side wait gave up                   */
+  V3DBA_ERR_NUMERICAL = 8           /* training of the learned preconditioner diverged       */
 };
 
 /* models (the three optimizer classes) */
@@ -89,7 +90,16 @@ enum {
 enum {
   V3DBA_SOLVER_AUTO = 0,            /* dense Cholesky up to a size limit, else PCG          */
   V3DBA_SOLVER_CHOLESKY = 1,        /* tile-sparse dense FP64 Cholesky                      */
-  V3DBA_SOLVER_PCG = 2              /* block-Jacobi preconditioned conjugate gradients     */
+  V3DBA_SOLVER_PCG = 2              /* preconditioned conjugate gradients                  */
+};
+
+/* preconditioner of the PCG solver */
+enum {
+  V3DBA_PRECOND_BLOCK_JACOBI = 0,   /* inverses of the 6x6 diagonal camera blocks           */
+  V3DBA_PRECOND_LEARNED = 1,        /* block-Jacobi corrected by the learned model attached with
+                                       v3dba_set_precond_model, plus the gauge coarse space;
+                                       plain block-Jacobi is the fallback                      */
+  V3DBA_PRECOND_GAUGE = 2           /* block-Jacobi plus the gauge coarse space (no network) */
 };
 
 typedef struct v3dba_problem {
@@ -121,6 +131,7 @@ typedef struct v3dba_options {
   int mixed_escalation;             /* MIXED only: 1 (default) switches the blocks to FP64 for
                                        the rest of the call at the first rejected step or gain
                                        ratio below 0.1; 0 keeps FP32 blocks throughout         */
+  int preconditioner;               /* V3DBA_PRECOND_* (PCG solver)                         */
 } v3dba_options;
 
 typedef struct v3dba_result {
@@ -135,6 +146,8 @@ typedef struct v3dba_result {
   int pcg_iterations;               /* total PCG iterations (PCG solver)                    */
   int reached_stop_cost;            /* 1 when stop_cost ended the call                      */
   int fp64_from_iteration;          /* MIXED: iteration at which FP64 blocks took over, or -1 */
+  int pcg_fallbacks;                /* LEARNED / GAUGE: trials re-solved with plain block-Jacobi
+                                       because the preconditioned solve failed or stalled     */
 } v3dba_result;
 
 typedef struct v3dba_handle_s* v3dba_handle;
@@ -254,6 +267,67 @@ int v3dba_batch_autotune(v3dba_batch_t b, const v3dba_options* opts, int* large_
                          int* split);
 int v3dba_batch_get_params(v3dba_batch_t b, int index, double* R, double* T, double* X);
 int v3dba_batch_get_all_params(v3dba_batch_t b, double* R, double* T, double* X);
+
+/* ---- Learned preconditioner ----------------------------------------------------------------
+ * No reference counterpart: the reference factors the damped normal equations directly
+ * (V3D/src/Math/v3d_optimization.cpp:1096-1145).  These entry points replace block-Jacobi in the
+ * PCG reduced-camera solve by M^-1 = G^T G + Z (Z^T S Z)^-1 Z^T.  G = (I + E) C^-1, where C C^T
+ * are the Cholesky factors of the 6x6 diagonal camera blocks and E is strictly block-lower on the
+ * camera co-visibility pattern; Z spans the 7 similarity-gauge motions of the cameras.  With F the
+ * normalised off-diagonal blocks of C^-1 S C^-T, each edge's block is
+ * E = -c0 F + c1 (F F)|pattern + c2 (F F^T)|pattern, and a message-passing network over the
+ * co-visibility graph (3 layers, hidden 64, inputs the three 6x6 blocks of every edge) predicts
+ * (c0, c1, c2) - 1.  Training minimises the probe estimate of |P - I|_F^2 / n, P the normalised
+ * preconditioned system, with V3DBA_PRECOND_PROBES Rademacher probes per system. */
+#define V3DBA_PRECOND_PROBES 16
+typedef struct v3dba_precond_model_s* v3dba_precond_model;
+typedef struct v3dba_precond_set_s* v3dba_precond_set;
+
+/* Number of float weights of the network. */
+int v3dba_precond_model_size(void);
+/* weights == NULL: seeded initial weights whose output layer is zero (c = 1). */
+int v3dba_precond_model_create(const float* weights, uint32_t seed, v3dba_precond_model* out);
+int v3dba_precond_model_destroy(v3dba_precond_model m);
+int v3dba_precond_model_get_weights(v3dba_precond_model m, float* weights);
+/* Attaches a model to a handle for V3DBA_PRECOND_LEARNED (NULL detaches).  The model must
+ * outlive the handle's minimize() calls that use it; a model serves one call at a time. */
+int v3dba_set_precond_model(v3dba_handle h, v3dba_precond_model m);
+
+/* A device-resident set of damped reduced camera systems (6-parameter cameras only). */
+int v3dba_precond_set_create(v3dba_precond_set* out);
+int v3dba_precond_set_destroy(v3dba_precond_set s);
+int v3dba_precond_set_count(v3dba_precond_set s);
+/* Adds a system given as 6x6 blocks S_{i,l}, i <= l, row-major (rows of camera i), every
+ * diagonal block present. */
+int v3dba_precond_set_add_blocks(v3dba_precond_set s, int n_cameras, int n_blocks, const int32_t* blk_i,
+                                 const int32_t* blk_l, const double* blocks);
+/* Adds the handle's reduced system (FP32 blocks) at its current parameters, damped by lambda,
+ * with the cameras' frames for the gauge coarse space. */
+int v3dba_precond_set_capture(v3dba_precond_set s, v3dba_handle h, double lambda);
+int v3dba_precond_set_info(v3dba_precond_set s, int index, int* n_cameras, int* n_edges);
+/* Graph and normalised inputs of system `index`: edges (a < b) with features [F, FF, FF^T]
+ * (ne x 108, row-major 6x6 blocks of the lower position (b, a)), node features (N x 4) and
+ * the inverse Cholesky factors of the diagonal blocks (N x 36). */
+int v3dba_precond_set_features(v3dba_precond_set s, int index, int32_t* edge_a, int32_t* edge_b, float* edge_feat,
+                               float* node_feat, float* cinv);
+/* Probe loss of system `index` and its gradient with respect to every weight (FP32 training
+ * kernels). */
+int v3dba_precond_loss_grad(v3dba_precond_model m, v3dba_precond_set s, int index, uint32_t probe_seed,
+                            double* loss, float* grad);
+/* Network outputs c - 1 (ne x 3) of system `index`: bf16 != 0 runs the BF16 tensor-core
+ * inference kernels, else the FP32 training kernels. */
+int v3dba_precond_coefficients(v3dba_precond_model m, v3dba_precond_set s, int index, int bf16, float* coeffs);
+/* Adam over the set for `epochs` passes in seeded order, one step per system, with probe
+ * seeds drawn from `seed`; mean loss of each epoch in loss_per_epoch (may be NULL). */
+int v3dba_precond_train(v3dba_precond_model m, v3dba_precond_set s, int epochs, double learning_rate, uint32_t seed,
+                        double* loss_per_epoch);
+/* PCG on system `index` (FP32 blocks, FP64 vectors) with a seeded right-hand side: iterations
+ * to |r| <= tol |b| with iters[0] block-Jacobi, [1] block-Jacobi + gauge space, [2] the learned
+ * factor alone, [3] the learned factor + gauge space (BF16 inference).  Entries that do not
+ * apply are -1 (no model: [2], [3]; a system added from blocks has no camera frames: [1], [3]).
+ * A count equal to max_iter means no convergence. */
+int v3dba_precond_pcg_iterations(v3dba_precond_model m, v3dba_precond_set s, int index, double tol, int max_iter,
+                                 uint32_t rhs_seed, int* iters);
 
 /* FP64 tensor-core (DMMA) throughput of the current GPU in TFLOP/s, measured by a short kernel
  * of independent mma.sync f64 chains on every SM (benchmark support). */

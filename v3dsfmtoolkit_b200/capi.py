@@ -14,10 +14,13 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "_lib", "libv3dba.so")
 
 OK = 0
-ERR_INVALID_ARGUMENT, ERR_INVALID_INPUT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NO_DEVICE, ERR_UNSUPPORTED, ERR_TIMEOUT = range(1, 8)
+(ERR_INVALID_ARGUMENT, ERR_INVALID_INPUT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NO_DEVICE, ERR_UNSUPPORTED, ERR_TIMEOUT,
+ ERR_NUMERICAL) = range(1, 9)
 STATUS_TIMEOUT, STATUS_SMALL_UPDATE, STATUS_CONVERGED = 0, 1, 2
 PRECISION_MIXED, PRECISION_FP64 = 0, 1
 SOLVER_AUTO, SOLVER_CHOLESKY, SOLVER_PCG = 0, 1, 2
+PRECOND_BLOCK_JACOBI, PRECOND_LEARNED, PRECOND_GAUGE = 0, 1, 2
+PRECOND_PROBES = 16
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -31,7 +34,12 @@ EXPORTS = (
     "v3dba_error_string", "v3dba_profile_stages", "v3dba_batch_create", "v3dba_batch_destroy",
     "v3dba_batch_minimize", "v3dba_batch_reset", "v3dba_batch_set_schedule", "v3dba_batch_autotune",
     "v3dba_batch_get_params", "v3dba_batch_get_all_params", "v3dba_measure_fp64_mma_peak",
-    "v3dba_cholesky_flops", "v3dba_dense_cholesky_solve_noalloc",
+    "v3dba_cholesky_flops", "v3dba_dense_cholesky_solve_noalloc", "v3dba_precond_model_size",
+    "v3dba_precond_model_create", "v3dba_precond_model_destroy", "v3dba_precond_model_get_weights",
+    "v3dba_set_precond_model", "v3dba_precond_set_create", "v3dba_precond_set_destroy", "v3dba_precond_set_count",
+    "v3dba_precond_set_add_blocks", "v3dba_precond_set_capture", "v3dba_precond_set_info",
+    "v3dba_precond_set_features", "v3dba_precond_loss_grad", "v3dba_precond_coefficients", "v3dba_precond_train",
+    "v3dba_precond_pcg_iterations",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -48,14 +56,14 @@ class Options(C.Structure):
     _fields_ = [("tau", C.c_double), ("max_iterations", C.c_int), ("gradient_threshold", C.c_double),
                 ("update_threshold", C.c_double), ("verbosity", C.c_int), ("precision", C.c_int),
                 ("solver", C.c_int), ("pcg_tolerance", C.c_double), ("pcg_max_iterations", C.c_int),
-                ("stop_cost", C.c_double), ("mixed_escalation", C.c_int)]
+                ("stop_cost", C.c_double), ("mixed_escalation", C.c_int), ("preconditioner", C.c_int)]
 
 
 class Result(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("n_relinearizations", C.c_int),
                 ("n_rejected", C.c_int), ("initial_cost", C.c_double), ("cost", C.c_double),
                 ("lambda_", C.c_double), ("device_ms", C.c_double), ("pcg_iterations", C.c_int),
-                ("reached_stop_cost", C.c_int), ("fp64_from_iteration", C.c_int)]
+                ("reached_stop_cost", C.c_int), ("fp64_from_iteration", C.c_int), ("pcg_fallbacks", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -105,6 +113,24 @@ def _lib():
         L.v3dba_batch_get_all_params.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.v3dba_measure_fp64_mma_peak.argtypes = [_dp]
         L.v3dba_cholesky_flops.argtypes = [C.c_void_p, _dp]
+        _fp = C.POINTER(C.c_float)
+        L.v3dba_precond_model_size.argtypes = []
+        L.v3dba_precond_model_create.argtypes = [_fp, C.c_uint32, C.POINTER(C.c_void_p)]
+        L.v3dba_precond_model_destroy.argtypes = [C.c_void_p]
+        L.v3dba_precond_model_get_weights.argtypes = [C.c_void_p, _fp]
+        L.v3dba_set_precond_model.argtypes = [C.c_void_p, C.c_void_p]
+        L.v3dba_precond_set_create.argtypes = [C.POINTER(C.c_void_p)]
+        L.v3dba_precond_set_destroy.argtypes = [C.c_void_p]
+        L.v3dba_precond_set_count.argtypes = [C.c_void_p]
+        L.v3dba_precond_set_add_blocks.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, _dp]
+        L.v3dba_precond_set_capture.argtypes = [C.c_void_p, C.c_void_p, C.c_double]
+        L.v3dba_precond_set_info.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.v3dba_precond_set_features.argtypes = [C.c_void_p, C.c_int, _ip, _ip, _fp, _fp, _fp]
+        L.v3dba_precond_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, _dp, _fp]
+        L.v3dba_precond_coefficients.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, _fp]
+        L.v3dba_precond_train.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_uint32, _dp]
+        L.v3dba_precond_pcg_iterations.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_uint32,
+                                                   C.POINTER(C.c_int)]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -203,6 +229,11 @@ class Handle:
         r = Result()
         check(_lib().v3dba_minimize(self.h, C.byref(o), C.byref(r)), "v3dba_minimize")
         return r
+
+    def set_precond_model(self, model):
+        """Attaches a PrecondModel for preconditioner=PRECOND_LEARNED (kept alive by the handle)."""
+        check(_lib().v3dba_set_precond_model(self.h, model.h if model is not None else None), "v3dba_set_precond_model")
+        self._precond = model
 
     def get_params(self):
         out = [np.zeros(s) for s in self.shapes]
@@ -313,3 +344,116 @@ class Batch:
         R, T, X = np.zeros((sc.n_cams, 3, 3)), np.zeros((sc.n_cams, 3)), np.zeros((sc.n_points, 3))
         check(_lib().v3dba_batch_get_params(self.h, i, _d(R), _d(T), _d(X)), "v3dba_batch_get_params")
         return R, T, X
+
+
+def _f32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+class PrecondModel:
+    """The learned preconditioner network (weights on the device)."""
+
+    def __init__(self, weights=None, seed=0):
+        self.h = C.c_void_p()
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+        if w is not None and w.size != self.size():
+            raise ValueError(f"expected {self.size()} weights, got {w.size}")
+        check(_lib().v3dba_precond_model_create(_f32p(w), seed, C.byref(self.h)), "v3dba_precond_model_create")
+
+    @staticmethod
+    def size() -> int:
+        return int(_lib().v3dba_precond_model_size())
+
+    @classmethod
+    def load(cls, path):
+        return cls(np.load(path).astype(np.float32))
+
+    def weights(self):
+        w = np.zeros(self.size(), dtype=np.float32)
+        check(_lib().v3dba_precond_model_get_weights(self.h, _f32p(w)), "v3dba_precond_model_get_weights")
+        return w
+
+    def close(self):
+        if self.h:
+            _lib().v3dba_precond_model_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def loss_grad(self, pset, index, probe_seed):
+        loss = C.c_double()
+        g = np.zeros(self.size(), dtype=np.float32)
+        check(_lib().v3dba_precond_loss_grad(self.h, pset.h, index, probe_seed, C.byref(loss), _f32p(g)),
+              "v3dba_precond_loss_grad")
+        return loss.value, g
+
+    def coefficients(self, pset, index, bf16=True):
+        ne = pset.info(index)[1]
+        c = np.zeros((max(ne, 1), 3), dtype=np.float32)
+        check(_lib().v3dba_precond_coefficients(self.h, pset.h, index, 1 if bf16 else 0, _f32p(c)),
+              "v3dba_precond_coefficients")
+        return c[:ne]
+
+    def train(self, pset, epochs, learning_rate=1e-3, seed=0):
+        hist = np.zeros(max(epochs, 1))
+        check(_lib().v3dba_precond_train(self.h, pset.h, epochs, learning_rate, seed, _d(hist)), "v3dba_precond_train")
+        return hist[:epochs]
+
+
+class PrecondSet:
+    """A device-resident set of damped reduced camera systems."""
+
+    def __init__(self):
+        self.h = C.c_void_p()
+        check(_lib().v3dba_precond_set_create(C.byref(self.h)), "v3dba_precond_set_create")
+
+    def __len__(self):
+        return int(_lib().v3dba_precond_set_count(self.h))
+
+    def add_blocks(self, n_cams, blk_i, blk_l, blocks):
+        bi = np.ascontiguousarray(blk_i, dtype=np.int32)
+        bl = np.ascontiguousarray(blk_l, dtype=np.int32)
+        b = _f64(blocks)
+        check(_lib().v3dba_precond_set_add_blocks(self.h, n_cams, bi.size, bi.ctypes.data_as(_ip),
+                                                  bl.ctypes.data_as(_ip), _d(b)), "v3dba_precond_set_add_blocks")
+
+    def capture(self, handle, lam):
+        check(_lib().v3dba_precond_set_capture(self.h, handle.h, lam), "v3dba_precond_set_capture")
+
+    def info(self, index):
+        n, e = C.c_int(), C.c_int()
+        check(_lib().v3dba_precond_set_info(self.h, index, C.byref(n), C.byref(e)), "v3dba_precond_set_info")
+        return n.value, e.value
+
+    def features(self, index):
+        N, ne = self.info(index)
+        ea, eb = np.zeros(max(ne, 1), np.int32), np.zeros(max(ne, 1), np.int32)
+        xe = np.zeros((max(ne, 1), 108), np.float32)
+        xn, cinv = np.zeros((N, 4), np.float32), np.zeros((N, 6, 6), np.float32)
+        check(_lib().v3dba_precond_set_features(self.h, index, ea.ctypes.data_as(_ip), eb.ctypes.data_as(_ip),
+                                                _f32p(xe), _f32p(xn), _f32p(cinv)), "v3dba_precond_set_features")
+        return ea[:ne], eb[:ne], xe[:ne], xn, cinv
+
+    def pcg_iterations(self, index, model=None, tol=1e-6, max_iter=2000, rhs_seed=0):
+        """PCG iterations of system `index`: dict with keys jacobi, jacobi_gauge, learned,
+        learned_gauge (None where a variant does not apply)."""
+        it = (C.c_int * 4)()
+        check(_lib().v3dba_precond_pcg_iterations(model.h if model is not None else None, self.h, index, tol, max_iter,
+                                                  rhs_seed, it), "v3dba_precond_pcg_iterations")
+        keys = ("jacobi", "jacobi_gauge", "learned", "learned_gauge")
+        return {k: (int(v) if v >= 0 else None) for k, v in zip(keys, it)}
+
+    def close(self):
+        if self.h:
+            _lib().v3dba_precond_set_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

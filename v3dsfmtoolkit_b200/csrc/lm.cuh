@@ -170,6 +170,8 @@ struct PcgState {
   double* vec = nullptr;        // b, r, z, p, Ap
   double* b = nullptr;
   double* part = nullptr;
+  double* gauge_rows = nullptr;  // [N x 28] per-camera terms of Z^T S Z
+  double* gauge_L = nullptr;     // packed Cholesky factor of Z^T S Z and its ok flag
   int* iters = nullptr;
   bool ready = false;
 };

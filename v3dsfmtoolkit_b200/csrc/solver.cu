@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "lm.cuh"
 #include "model.cuh"
+#include "precond.cuh"
 
 namespace v3dba {
 
@@ -45,6 +46,16 @@ struct v3dba_handle_s {
   double* h_scalars = nullptr;   // pinned readback area
   std::vector<void*> allocs;
   size_t nK = 0, nD = 0;
+  // learned preconditioner and gauge space (PCG solver): attached model, camera graph, inputs
+  v3dba_precond_model precond = nullptr;
+  bool gnn_ready = false;
+  GnnGraph gnn;
+  float* gnn_cinv = nullptr;
+  float* gnn_xe = nullptr;
+  float* gnn_xn = nullptr;
+  float* gnn_ehat = nullptr;
+  int* gnn_fail = nullptr;
+  double* gauge_frames = nullptr;   // [N x 12] camera frames of the gauge coarse space
 };
 
 namespace {
@@ -127,6 +138,7 @@ void free_handle(v3dba_handle h) {
   for (void* p : h->allocs) cudaFree(p);
   tile_chol_free(h->chol);
   pcg_free(h->pcg);
+  gnn_graph_free(h->gnn);
   if (h->h_scalars) cudaFreeHost(h->h_scalars);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -173,6 +185,25 @@ int use_pcg(v3dba_handle h) {
   s.x = h->x_pcg;
   s.Sb = h->pcg.Sb;
   s.diag_blk = h->pcg.diag_blk;
+  return V3DBA_OK;
+}
+
+// Gauge frames, and for the learned preconditioner its camera graph and input buffers: built
+// on first use.
+int use_gnn(v3dba_handle h, bool learned) {
+  if (!h->gauge_frames) {
+    int rc0 = dalloc(h, &h->gauge_frames, (size_t)std::max(h->s.d.N, 1) * 12);
+    if (rc0 || (rc0 = dalloc(h, &h->gnn_fail, 1))) return rc0;
+  }
+  if (h->gnn_ready || !learned) return V3DBA_OK;
+  const int N = h->s.d.N;
+  int rc;
+  if ((rc = gnn_graph_build(h->gnn, N, h->blk_i, h->blk_l))) return rc;
+  const size_t ne = (size_t)std::max(h->gnn.ne, 1);
+  if ((rc = dalloc(h, &h->gnn_cinv, (size_t)N * 36)) || (rc = dalloc(h, &h->gnn_xe, ne * kGnnEdgeIn)) ||
+      (rc = dalloc(h, &h->gnn_xn, (size_t)N * kGnnNodeIn)) || (rc = dalloc(h, &h->gnn_ehat, (size_t)h->s.nb * 36)))
+    return rc;
+  h->gnn_ready = true;
   return V3DBA_OK;
 }
 
@@ -296,6 +327,7 @@ void v3dba_default_options(v3dba_options* o) {
   o->pcg_max_iterations = 500;
   o->stop_cost = 0.0;
   o->mixed_escalation = 1;
+  o->preconditioner = V3DBA_PRECOND_BLOCK_JACOBI;
 }
 
 int v3dba_dims(int model, int mode, int* dA, int* dC) {
@@ -313,6 +345,7 @@ const char* v3dba_error_string(int code) {
     case V3DBA_ERR_NO_DEVICE: return "no CUDA device";
     case V3DBA_ERR_UNSUPPORTED: return "unsupported configuration";
     case V3DBA_ERR_TIMEOUT: return "device-side wait timed out";
+    case V3DBA_ERR_NUMERICAL: return "training diverged";
   }
   return "unknown error";
 }
@@ -538,8 +571,8 @@ namespace {
 
 // One damped trial: reduced system at *d_lambda, Cholesky or PCG, back-substitution, trial
 // parameters and their cost.  Reads back {new_err, |delta|^2, delta . g, fail, pcg iterations}.
-int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, bool fp64, const v3dba_options& o,
-              double out[5]) {
+int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int precond, bool fp64,
+              const v3dba_options& o, double out[6]) {
   DevState& s = h->s;
   cudaStream_t st = h->stream;
   h->h_scalars[8] = lambda;
@@ -548,7 +581,42 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, bool fp
   int rc;
   if (!pcg && (rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
   if ((rc = ops->build_reduced(s, st))) return rc;
-  if (pcg) {
+  int fallback = 0;
+  if (pcg && precond != V3DBA_PRECOND_BLOCK_JACOBI) {
+    // learned factor (+ gauge space) or block-Jacobi + gauge space; plain block-Jacobi re-solves
+    // the trial when that fails or stalls
+    const bool learned = precond == V3DBA_PRECOND_LEARNED;
+    V3DBA_CUDA_TRY(cudaMemsetAsync(h->gnn_fail, 0, sizeof(int), st));
+    if ((rc = gauge_frames(s.cur.R, s.cur.T, s.d.N, s.d.nnA, h->gauge_frames, st))) return rc;
+    if (learned &&
+        ((rc = gnn_features(h->gnn, s.Sb, fp64, s.diag_blk, h->gnn_cinv, h->gnn_xe, h->gnn_xn, h->gnn_fail, st)) ||
+         (rc = gnn_precond_blocks(h->precond, h->gnn, h->gnn_cinv, h->gnn_xe, h->gnn_xn, h->gnn_ehat, st))))
+      return rc;
+    int ffail = 0;
+    V3DBA_CUDA_TRY(cudaMemcpyAsync(&ffail, h->gnn_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+    V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+    int its = 0;
+    if (!ffail) {
+      PcgPrecond P;
+      if (learned) { P.cinv = h->gnn_cinv; P.ehat = h->gnn_ehat; }
+      P.frames = h->gauge_frames;
+      if ((rc = pcg_solve_precond(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x,
+                                  h->gnn_fail, st, P)))
+        return rc;
+      V3DBA_CUDA_TRY(cudaMemcpyAsync(&its, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+      V3DBA_CUDA_TRY(cudaMemcpyAsync(&ffail, h->gnn_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+      V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    h->h_scalars[10] = its;
+    if (ffail || its >= o.pcg_max_iterations) {
+      fallback = 1;
+      if ((rc = pcg_solve(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x, s.d_fail, st)))
+        return rc;
+      V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 9, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+    } else {
+      std::memcpy(h->h_scalars + 9, &its, sizeof(int));
+    }
+  } else if (pcg) {
     if ((rc = pcg_solve(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x, s.d_fail, st)))
       return rc;
     V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 9, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -566,7 +634,8 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, bool fp
   std::memcpy(&fail, h->h_scalars + 3, sizeof(int));
   if (pcg) std::memcpy(&its, h->h_scalars + 9, sizeof(int));
   out[3] = fail ? 1.0 : 0.0;
-  out[4] = its;
+  out[4] = its + (fallback ? h->h_scalars[10] : 0.0);   // iterations of a failed attempt count too
+  out[5] = fallback;
   return V3DBA_OK;
 }
 
@@ -590,9 +659,19 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
   if (solver == V3DBA_SOLVER_AUTO) solver = (s.n <= 4096 || D.DC > 0) ? V3DBA_SOLVER_CHOLESKY : V3DBA_SOLVER_PCG;
   if (solver == V3DBA_SOLVER_PCG && D.DC > 0) return V3DBA_ERR_UNSUPPORTED;
   const bool pcg = solver == V3DBA_SOLVER_PCG;
+  const bool learned = pcg && o.preconditioner == V3DBA_PRECOND_LEARNED;
+  const bool gauge = pcg && o.preconditioner != V3DBA_PRECOND_BLOCK_JACOBI;
+  if (o.preconditioner < V3DBA_PRECOND_BLOCK_JACOBI || o.preconditioner > V3DBA_PRECOND_GAUGE)
+    return V3DBA_ERR_INVALID_ARGUMENT;
+  if (learned && !h->precond) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (gauge && D.DA != 6) return V3DBA_ERR_UNSUPPORTED;
   {
     const int rc0 = pcg ? use_pcg(h) : use_dense(h);
     if (rc0) return rc0;
+    if (gauge) {
+      const int rc1 = use_gnn(h, learned);
+      if (rc1) return rc1;
+    }
   }
 
   const int nvA = D.N - D.nnA, nvB = D.M - D.nnB, nvC = D.DC - D.nnC;
@@ -639,9 +718,11 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
         if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: initial lambda = %.17g\n", lambda);
       }
     }
-    double t[5];
-    if ((rc = run_trial(h, ops, lambda, pcg, fp64, o, t))) return rc;
+    double t[6];
+    if ((rc = run_trial(h, ops, lambda, pcg, pcg ? o.preconditioner : V3DBA_PRECOND_BLOCK_JACOBI, fp64, o, t)))
+      return rc;
     res->pcg_iterations += (int)t[4];
+    res->pcg_fallbacks += (int)t[5];
     const bool success = t[3] == 0.0;
     double rho = 0.0;
     if (success) {
@@ -763,4 +844,16 @@ int handle_use_dense(v3dba_handle h) { return use_dense(h); }
 DevState& handle_state(v3dba_handle h) { return h->s; }
 TileChol& handle_chol(v3dba_handle h) { return h->chol; }
 cudaStream_t handle_stream(v3dba_handle h) { return h->stream; }
+const std::vector<int>& handle_blk_i(v3dba_handle h) { return h->blk_i; }
+const std::vector<int>& handle_blk_l(v3dba_handle h) { return h->blk_l; }
+int handle_use_pcg(v3dba_handle h) { return use_pcg(h); }
+PcgState& handle_pcg(v3dba_handle h) { return h->pcg; }
+const double* handle_cur_R(v3dba_handle h) { return h->s.cur.R; }
+const double* handle_cur_T(v3dba_handle h) { return h->s.cur.T; }
 }  // namespace v3dba
+
+extern "C" int v3dba_set_precond_model(v3dba_handle h, v3dba_precond_model m) {
+  if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
+  h->precond = m;
+  return V3DBA_OK;
+}

@@ -316,39 +316,42 @@ def cluster_scene(n_groups=20, cams_per_group=100, n_points=1_000_000, seed=0, n
 
     p = 1.0 / (mean_track - min_track + 1)
     lengths = min_track - 1 + rng.geometric(p, size=n_points)
-    cross = rng.uniform(size=n_points) < cross_frac
+    cross = (rng.uniform(size=n_points) < cross_frac) & (n_groups > 1)
     pg = rng.integers(0, n_groups - 1 if n_groups > 1 else 1, size=n_points)
     base = gc[pg].copy()
     base[cross, 0] += 6.0
     X = base + rng.uniform(-2.5, 2.5, size=(n_points, 3))
 
-    views = np.empty(int(lengths.sum()) + n_points * 4, dtype=np.int64)
-    pts = np.empty_like(views)
-    n = 0
+    views_l, pts_l = [], []
     chunk = 20000
-    order = np.arange(n_points)
     kept = np.zeros(n_points, dtype=bool)
+    ncand = 48
+    big = np.iinfo(np.int64).max
     for c0 in range(0, n_points, chunk):
-        idx = order[c0:c0 + chunk]
+        idx = np.arange(c0, min(c0 + chunk, n_points))
         # candidate cameras: the point's group, plus the next group for cross points
         cand_g = np.stack([pg[idx], np.where(cross[idx], pg[idx] + 1, pg[idx])], axis=1)
-        ncand = 48
         cams = (cand_g[:, rng.integers(0, 2, size=ncand)] * cams_per_group
                 + rng.integers(0, cams_per_group, size=(idx.size, ncand)))
         q, z = project_pinhole(K[cams], R[cams], T[cams], X[idx][:, None, :])
         vis = (z > 0.5) & (q[..., 0] >= 0) & (q[..., 0] < 640) & (q[..., 1] >= 0) & (q[..., 1] < 480)
-        for r in range(idx.size):
-            j = idx[r]
-            c = np.unique(cams[r][vis[r]])
-            if c.size < min_track:
-                continue
-            L = min(int(lengths[j]), c.size)
-            sel = np.sort(rng.choice(c, size=L, replace=False))
-            views[n:n + L] = sel
-            pts[n:n + L] = j
-            n += L
-            kept[j] = True
-    views, pts = views[:n], pts[:n]
+        # distinct visible candidates, then a random subset of the track length, sorted
+        o = np.argsort(cams, axis=1, kind="stable")
+        cs = np.take_along_axis(cams, o, 1)
+        vs = np.take_along_axis(vis, o, 1)
+        vs[:, 1:] &= cs[:, 1:] != cs[:, :-1]
+        cnt = vs.sum(axis=1)
+        ok = cnt >= min_track
+        L = np.where(ok, np.minimum(lengths[idx], cnt), 0)
+        key = np.where(vs, rng.uniform(size=vs.shape), 2.0)
+        pick = np.take_along_axis(cs, np.argsort(key, axis=1), 1)
+        take = np.arange(ncand)[None, :] < L[:, None]
+        sel = np.sort(np.where(take, pick, big), axis=1)
+        take = np.sort(take, axis=1)[:, ::-1]
+        views_l.append(sel[take])
+        pts_l.append(np.repeat(idx, L))
+        kept[idx[ok]] = True
+    views, pts = np.concatenate(views_l), np.concatenate(pts_l)
     remap = -np.ones(n_points, dtype=np.int64)
     remap[kept] = np.arange(int(kept.sum()))
     X = X[kept]
