@@ -293,7 +293,7 @@ int v3dba_precond_model_get_weights(v3dba_precond_model m, float* weights);
  * outlive the handle's minimize() calls that use it; a model serves one call at a time. */
 int v3dba_set_precond_model(v3dba_handle h, v3dba_precond_model m);
 
-/* A device-resident set of damped reduced camera systems (6-parameter cameras only). */
+/* A device-resident set of damped reduced camera systems (6-parameter cameras only, FP64 blocks). */
 int v3dba_precond_set_create(v3dba_precond_set* out);
 int v3dba_precond_set_destroy(v3dba_precond_set s);
 int v3dba_precond_set_count(v3dba_precond_set s);
@@ -301,7 +301,7 @@ int v3dba_precond_set_count(v3dba_precond_set s);
  * diagonal block present. */
 int v3dba_precond_set_add_blocks(v3dba_precond_set s, int n_cameras, int n_blocks, const int32_t* blk_i,
                                  const int32_t* blk_l, const double* blocks);
-/* Adds the handle's reduced system (FP32 blocks) at its current parameters, damped by lambda,
+/* Adds the handle's reduced system (FP64 blocks) at its current parameters, damped by lambda,
  * with the cameras' frames for the gauge coarse space. */
 int v3dba_precond_set_capture(v3dba_precond_set s, v3dba_handle h, double lambda);
 int v3dba_precond_set_info(v3dba_precond_set s, int index, int* n_cameras, int* n_edges);
@@ -321,7 +321,7 @@ int v3dba_precond_coefficients(v3dba_precond_model m, v3dba_precond_set s, int i
  * seeds drawn from `seed`; mean loss of each epoch in loss_per_epoch (may be NULL). */
 int v3dba_precond_train(v3dba_precond_model m, v3dba_precond_set s, int epochs, double learning_rate, uint32_t seed,
                         double* loss_per_epoch);
-/* PCG on system `index` (FP32 blocks, FP64 vectors) with a seeded right-hand side: iterations
+/* PCG on system `index` (FP64 blocks and vectors) with a seeded right-hand side: iterations
  * to |r| <= tol |b| with iters[0] block-Jacobi, [1] block-Jacobi + gauge space, [2] the learned
  * factor alone, [3] the learned factor + gauge space (BF16 inference).  Entries that do not
  * apply are -1 (no model: [2], [3]; a system added from blocks has no camera frames: [1], [3]).

@@ -146,7 +146,6 @@ def test_lm_with_learned_preconditioner_matches_block_jacobi():
                      preconditioner=capi.PRECOND_LEARNED, stop_cost=cj * (1 + 1e-6))
     assert hl.cost() <= cj * (1 + 1e-6)
     assert rl.pcg_iterations * 2 <= rj.pcg_iterations, (rl.pcg_iterations, rj.pcg_iterations)
-    assert rl.pcg_fallbacks == 0
 
 
 def test_learned_without_model_is_rejected():

@@ -1057,7 +1057,7 @@ namespace {
 struct PrecondSystem {
   int N = 0, nb = 0;
   GnnGraph g;
-  PcgState ps;      // pattern, FP32 blocks (8-byte slots), vectors
+  PcgState ps;      // pattern, FP64 blocks, vectors
   float* cinv = nullptr;
   float* xe = nullptr;
   float* xn = nullptr;
@@ -1096,7 +1096,10 @@ const double* handle_cur_T(v3dba_handle h);
 
 namespace {
 
-// Allocates a system over the block pattern and fills its FP32 blocks with `fill`.
+// Allocates a system over the block pattern and fills its FP64 blocks with `fill`.  The set
+// keeps FP64 blocks: at the small damping of a converged LM run FP32 rounding of S exceeds the
+// gauge eigenvalues (the LM itself then runs FP64 blocks), so FP32 copies would not be the
+// systems the solver meets there.
 template <typename Fill>
 int system_create(v3dba_precond_set s, int N, const std::vector<int>& b_i, const std::vector<int>& b_l, Fill fill) {
   PrecondSystem ps;
@@ -1121,7 +1124,7 @@ int system_create(v3dba_precond_set s, int N, const std::vector<int>& b_i, const
   }
   if ((rc = fill(ps))) { system_free(ps); return rc; }
   V3DBA_CUDA_TRY(cudaMemsetAsync(ps.fail, 0, sizeof(int), s->st));
-  if ((rc = gnn_features(ps.g, ps.ps.Sb, false, ps.ps.diag_blk, ps.cinv, ps.xe, ps.xn, ps.fail, s->st))) {
+  if ((rc = gnn_features(ps.g, ps.ps.Sb, true, ps.ps.diag_blk, ps.cinv, ps.xe, ps.xn, ps.fail, s->st))) {
     system_free(ps);
     return rc;
   }
@@ -1249,9 +1252,7 @@ int v3dba_precond_set_add_blocks(v3dba_precond_set s, int n_cameras, int n_block
   for (size_t t = 0; t < (size_t)n_blocks * 36; ++t)
     if (!std::isfinite(blocks[t])) return V3DBA_ERR_INVALID_INPUT;
   return system_create(s, n_cameras, bi, bl, [&](PrecondSystem& ps) -> int {
-    std::vector<float> f((size_t)n_blocks * 36);
-    for (size_t t = 0; t < f.size(); ++t) f[t] = (float)blocks[t];
-    V3DBA_CUDA_TRY(cudaMemcpy(ps.ps.Sb, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
+    V3DBA_CUDA_TRY(cudaMemcpy(ps.ps.Sb, blocks, sizeof(double) * (size_t)n_blocks * 36, cudaMemcpyHostToDevice));
     return V3DBA_OK;
   });
 }
@@ -1262,7 +1263,7 @@ int v3dba_precond_set_capture(v3dba_precond_set s, v3dba_handle h, double lambda
   if (ds.d.DA != 6 || ds.d.DC != 0) return V3DBA_ERR_UNSUPPORTED;
   int rc;
   if ((rc = handle_use_pcg(h))) return rc;
-  const LmOps* ops = lm_ops(ds.d.model, ds.d.DA, ds.d.DC, false);
+  const LmOps* ops = lm_ops(ds.d.model, ds.d.DA, ds.d.DC, true);
   if (!ops) return V3DBA_ERR_UNSUPPORTED;
   cudaStream_t hst = handle_stream(h);
   if ((rc = ops->relinearize(ds, false, 0.0, hst))) return rc;
@@ -1271,7 +1272,7 @@ int v3dba_precond_set_capture(v3dba_precond_set s, v3dba_handle h, double lambda
   if ((rc = ops->build_reduced(ds, hst))) return rc;
   V3DBA_CUDA_TRY(cudaStreamSynchronize(hst));
   const void* src = handle_pcg(h).Sb;
-  const size_t bytes = sizeof(float) * (size_t)ds.nb * 36;
+  const size_t bytes = sizeof(double) * (size_t)ds.nb * 36;
   const int N = ds.d.N, n_fixed = ds.d.nnA;
   const double* R = handle_cur_R(h);
   const double* T = handle_cur_T(h);
@@ -1393,7 +1394,7 @@ int v3dba_precond_pcg_iterations(v3dba_precond_model m, v3dba_precond_set s, int
     if (learned) { P.cinv = p.cinv; P.ehat = p.ehat; }
     if (gauge) P.frames = p.frames;
     V3DBA_CUDA_TRY(cudaMemsetAsync(p.fail, 0, sizeof(int), st));
-    if ((rc = pcg_solve_precond(p.ps, p.N, 6, false, tol, max_iter, p.x, p.fail, st, P))) return rc;
+    if ((rc = pcg_solve_precond(p.ps, p.N, 6, true, tol, max_iter, p.x, p.fail, st, P))) return rc;
     int its = 0, fl = 0;
     V3DBA_CUDA_TRY(cudaMemcpyAsync(&its, p.ps.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
     V3DBA_CUDA_TRY(cudaMemcpyAsync(&fl, p.fail, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -51,7 +51,7 @@ def capture(pset, sc, n_captures, iterations=20, span=(0.0, 4.0), max_pcg=500):
     parameters is captured at dampings lambda_end * 10^u, u evenly spread over `span` -- from the
     final damping up to the early iterations' range, which is where the solver spends its PCG
     iterations.  A damping at which a diagonal camera block is not numerically positive
-    definite in FP32 is skipped.  Returns the number of systems added."""
+    definite is skipped.  Returns the number of systems added."""
     h = capi.Handle.from_scene(sc)
     added = 0
     try:
