@@ -97,9 +97,9 @@ enum {
 enum {
   V3DBA_PRECOND_BLOCK_JACOBI = 0,   /* inverses of the 6x6 diagonal camera blocks           */
   V3DBA_PRECOND_LEARNED = 1,        /* block-Jacobi corrected by the learned model attached with
-                                       v3dba_set_precond_model, plus the gauge coarse space;
-                                       plain block-Jacobi is the fallback                      */
-  V3DBA_PRECOND_GAUGE = 2           /* block-Jacobi plus the gauge coarse space (no network) */
+                                       v3dba_set_precond_model; plain block-Jacobi is the
+                                       fallback                                               */
+  V3DBA_PRECOND_GAUGE = 2           /* block-Jacobi plus the gauge coarse space (no network)  */
 };
 
 typedef struct v3dba_problem {
@@ -147,7 +147,7 @@ typedef struct v3dba_result {
   int reached_stop_cost;            /* 1 when stop_cost ended the call                      */
   int fp64_from_iteration;          /* MIXED: iteration at which FP64 blocks took over, or -1 */
   int pcg_fallbacks;                /* LEARNED / GAUGE: trials re-solved with plain block-Jacobi
-                                       because the preconditioned solve failed or stalled     */
+                                       because the preconditioned solve broke down            */
 } v3dba_result;
 
 typedef struct v3dba_handle_s* v3dba_handle;
@@ -271,9 +271,10 @@ int v3dba_batch_get_all_params(v3dba_batch_t b, double* R, double* T, double* X)
 /* ---- Learned preconditioner ----------------------------------------------------------------
  * No reference counterpart: the reference factors the damped normal equations directly
  * (V3D/src/Math/v3d_optimization.cpp:1096-1145).  These entry points replace block-Jacobi in the
- * PCG reduced-camera solve by M^-1 = G^T G + Z (Z^T S Z)^-1 Z^T.  G = (I + E) C^-1, where C C^T
- * are the Cholesky factors of the 6x6 diagonal camera blocks and E is strictly block-lower on the
- * camera co-visibility pattern; Z spans the 7 similarity-gauge motions of the cameras.  With F the
+ * PCG reduced-camera solve by M^-1 = G^T G.  G = (I + E) C^-1, where C C^T are the Cholesky
+ * factors of the 6x6 diagonal camera blocks and E is strictly block-lower on the camera
+ * co-visibility pattern (the gauge coarse space, Z (Z^T S Z)^-1 Z^T with Z spanning the 7
+ * similarity-gauge motions of the cameras, is a separate option).  With F the
  * normalised off-diagonal blocks of C^-1 S C^-T, each edge's block is
  * E = -c0 F + c1 (F F)|pattern + c2 (F F^T)|pattern, and a message-passing network over the
  * co-visibility graph (3 layers, hidden 64, inputs the three 6x6 blocks of every edge) predicts
@@ -298,11 +299,12 @@ int v3dba_precond_set_create(v3dba_precond_set* out);
 int v3dba_precond_set_destroy(v3dba_precond_set s);
 int v3dba_precond_set_count(v3dba_precond_set s);
 /* Adds a system given as 6x6 blocks S_{i,l}, i <= l, row-major (rows of camera i), every
- * diagonal block present. */
+ * diagonal block present.  R (n_cameras x 9) and T (n_cameras x 3), when not NULL, are the
+ * cameras the system was linearised at, for the gauge coarse space. */
 int v3dba_precond_set_add_blocks(v3dba_precond_set s, int n_cameras, int n_blocks, const int32_t* blk_i,
-                                 const int32_t* blk_l, const double* blocks);
+                                 const int32_t* blk_l, const double* blocks, const double* R, const double* T);
 /* Adds the handle's reduced system (FP64 blocks) at its current parameters, damped by lambda,
- * with the cameras' frames for the gauge coarse space. */
+ * with its right-hand side and the cameras' frames for the gauge coarse space. */
 int v3dba_precond_set_capture(v3dba_precond_set s, v3dba_handle h, double lambda);
 int v3dba_precond_set_info(v3dba_precond_set s, int index, int* n_cameras, int* n_edges);
 /* Graph and normalised inputs of system `index`: edges (a < b) with features [F, FF, FF^T]
@@ -321,13 +323,15 @@ int v3dba_precond_coefficients(v3dba_precond_model m, v3dba_precond_set s, int i
  * seeds drawn from `seed`; mean loss of each epoch in loss_per_epoch (may be NULL). */
 int v3dba_precond_train(v3dba_precond_model m, v3dba_precond_set s, int epochs, double learning_rate, uint32_t seed,
                         double* loss_per_epoch);
-/* PCG on system `index` (FP64 blocks and vectors) with a seeded right-hand side: iterations
- * to |r| <= tol |b| with iters[0] block-Jacobi, [1] block-Jacobi + gauge space, [2] the learned
- * factor alone, [3] the learned factor + gauge space (BF16 inference).  Entries that do not
- * apply are -1 (no model: [2], [3]; a system added from blocks has no camera frames: [1], [3]).
- * A count equal to max_iter means no convergence. */
+/* PCG on system `index` (FP64 blocks and vectors): iterations to |r| <= tol |b| with iters[0]
+ * block-Jacobi, [1] block-Jacobi + gauge space, [2] the learned factor alone, [3] the learned
+ * factor + gauge space (BF16 inference).  rhs_seed == 0 solves with the system's own right-hand
+ * side (the LM's reduced gradient, for captured systems), else with a seeded N(0,1) vector.
+ * Entries that do not apply are -1 (no model: [2], [3]; no camera frames: [1], [3]).  A count
+ * equal to max_iter means no convergence.  ms (may be NULL) receives the device time of each
+ * solve in ms (its preconditioner set-up included) and, in ms[4], of the network inference. */
 int v3dba_precond_pcg_iterations(v3dba_precond_model m, v3dba_precond_set s, int index, double tol, int max_iter,
-                                 uint32_t rhs_seed, int* iters);
+                                 uint32_t rhs_seed, int* iters, double* ms);
 
 /* FP64 tensor-core (DMMA) throughput of the current GPU in TFLOP/s, measured by a short kernel
  * of independent mma.sync f64 chains on every SM (benchmark support). */

@@ -122,7 +122,7 @@ def _lib():
         L.v3dba_precond_set_create.argtypes = [C.POINTER(C.c_void_p)]
         L.v3dba_precond_set_destroy.argtypes = [C.c_void_p]
         L.v3dba_precond_set_count.argtypes = [C.c_void_p]
-        L.v3dba_precond_set_add_blocks.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, _dp]
+        L.v3dba_precond_set_add_blocks.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, _dp, _dp, _dp]
         L.v3dba_precond_set_capture.argtypes = [C.c_void_p, C.c_void_p, C.c_double]
         L.v3dba_precond_set_info.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.v3dba_precond_set_features.argtypes = [C.c_void_p, C.c_int, _ip, _ip, _fp, _fp, _fp]
@@ -130,7 +130,7 @@ def _lib():
         L.v3dba_precond_coefficients.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, _fp]
         L.v3dba_precond_train.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_uint32, _dp]
         L.v3dba_precond_pcg_iterations.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_uint32,
-                                                   C.POINTER(C.c_int)]
+                                                   C.POINTER(C.c_int), _dp]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -414,12 +414,15 @@ class PrecondSet:
     def __len__(self):
         return int(_lib().v3dba_precond_set_count(self.h))
 
-    def add_blocks(self, n_cams, blk_i, blk_l, blocks):
+    def add_blocks(self, n_cams, blk_i, blk_l, blocks, R=None, T=None):
         bi = np.ascontiguousarray(blk_i, dtype=np.int32)
         bl = np.ascontiguousarray(blk_l, dtype=np.int32)
         b = _f64(blocks)
+        R = None if R is None else _f64(R)
+        T = None if T is None else _f64(T)
         check(_lib().v3dba_precond_set_add_blocks(self.h, n_cams, bi.size, bi.ctypes.data_as(_ip),
-                                                  bl.ctypes.data_as(_ip), _d(b)), "v3dba_precond_set_add_blocks")
+                                                  bl.ctypes.data_as(_ip), _d(b), _d(R), _d(T)),
+              "v3dba_precond_set_add_blocks")
 
     def capture(self, handle, lam):
         check(_lib().v3dba_precond_set_capture(self.h, handle.h, lam), "v3dba_precond_set_capture")
@@ -438,14 +441,19 @@ class PrecondSet:
                                                 _f32p(xe), _f32p(xn), _f32p(cinv)), "v3dba_precond_set_features")
         return ea[:ne], eb[:ne], xe[:ne], xn, cinv
 
-    def pcg_iterations(self, index, model=None, tol=1e-6, max_iter=2000, rhs_seed=0):
+    def pcg_iterations(self, index, model=None, tol=1e-6, max_iter=2000, rhs_seed=0, times=False):
         """PCG iterations of system `index`: dict with keys jacobi, jacobi_gauge, learned,
-        learned_gauge (None where a variant does not apply)."""
+        learned_gauge (None where a variant does not apply); with times=True also the device ms
+        of each solve and of the network inference."""
         it = (C.c_int * 4)()
+        ms = np.zeros(5)
         check(_lib().v3dba_precond_pcg_iterations(model.h if model is not None else None, self.h, index, tol, max_iter,
-                                                  rhs_seed, it), "v3dba_precond_pcg_iterations")
+                                                  rhs_seed, it, _d(ms)), "v3dba_precond_pcg_iterations")
         keys = ("jacobi", "jacobi_gauge", "learned", "learned_gauge")
-        return {k: (int(v) if v >= 0 else None) for k, v in zip(keys, it)}
+        out = {k: (int(v) if v >= 0 else None) for k, v in zip(keys, it)}
+        if times:
+            out["ms"] = {k: (float(v) if v >= 0 else None) for k, v in zip(keys + ("inference",), ms)}
+        return out
 
     def close(self):
         if self.h:

@@ -60,6 +60,7 @@ struct PcgArgs {
   const double* b;                 // rhs (n)
   double* x;                       // solution (n)
   double* r; double* z; double* p; double* p2; double* Ap;
+  double* r2;                      // learned: the next residual (double buffer)
   double* part;                    // [2 * gridDim * kPartStride] partials
   double tol;
   int max_iter;
@@ -157,10 +158,12 @@ __device__ __forceinline__ void gauge_solve(const double* L, const double* y, do
   }
 }
 
-// Grid-wide deterministic sums of NV values: per-block partials, then every block folds them in
-// block order.  The partials alternate between two buffers, so one barrier per reduction
-// suffices (a buffer is rewritten only two reductions later, after every block has passed the
-// barrier of the reduction in between).  Must be called by all threads of all blocks.
+// Grid-wide deterministic sums of NV values: per-block partials, then every block folds them:
+// warp 0 reads the partials with its lanes striding over the blocks and combines the lanes by a
+// fixed shuffle tree, so every block computes the same sums bit for bit.  The partials
+// alternate between two buffers, so one barrier per reduction suffices (a buffer is rewritten
+// only two reductions later, after every block has passed the barrier of the reduction in
+// between).  Must be called by all threads of all blocks.
 template <int NV>
 __device__ __forceinline__ void grid_sums(double (&v)[NV], double* part, int& parity, cg::grid_group& grid) {
   static_assert(NV <= kPartStride, "partial stride");
@@ -170,9 +173,23 @@ __device__ __forceinline__ void grid_sums(double (&v)[NV], double* part, int& pa
   if (threadIdx.x == 0)
     for (int t = 0; t < NV; ++t) pb[(size_t)blockIdx.x * kPartStride + t] = v[t];
   grid.sync();
-  for (int t = 0; t < NV; ++t) v[t] = 0.0;
-  for (int bk = 0; bk < (int)gridDim.x; ++bk)
-    for (int t = 0; t < NV; ++t) v[t] += pb[(size_t)bk * kPartStride + t];
+  if (threadIdx.x < 32) {
+    double s[NV];
+#pragma unroll
+    for (int t = 0; t < NV; ++t) s[t] = 0.0;
+    for (int bk = threadIdx.x; bk < (int)gridDim.x; bk += 32)
+#pragma unroll
+      for (int t = 0; t < NV; ++t) s[t] += pb[(size_t)bk * kPartStride + t];
+#pragma unroll
+    for (int t = 0; t < NV; ++t) s[t] = warp_sum(s[t]);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int t = 0; t < NV; ++t) red[t] = s[t];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < NV; ++t) v[t] = red[t];
+  __syncthreads();   // red is reused by the next reduction's block_reduce
   parity ^= 1;
 }
 
@@ -192,6 +209,30 @@ __device__ __forceinline__ void learned_lower_row(const PcgArgs& a, int i, int l
     const float* Ci = a.cinv + (size_t)i * 36 + lane * 6;
     const double* v = r + (size_t)i * 6;
     for (int c = 0; c <= lane; ++c) acc[lane] += double(Ci[c]) * v[c];
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
+  if (lane < 6) t[(size_t)i * 6 + lane] = acc[lane];
+}
+
+// The same first half for the residual of the step being taken, r - alpha Ap, formed on the fly
+// from the previous residual and Ap of every row it reads (they are not overwritten in this
+// phase: the new residual goes to a second buffer).
+__device__ __forceinline__ void learned_lower_row_step(const PcgArgs& a, int i, int lane, const double* r,
+                                                       const double* Ap, double alpha, double* t) {
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int e = a.rp[i] + lane; e < a.rp[i + 1]; e += 32) {
+    if (!a.rt[e]) continue;
+    double v[6];
+    const size_t o = (size_t)a.rc[e] * 6;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) v[c] = r[o + c] - alpha * Ap[o + c];
+    block_mv_mem<float, 6>(a.ehat + (size_t)a.rb[e] * 36, false, v, acc);
+  }
+  if (lane < 6) {
+    const float* Ci = a.cinv + (size_t)i * 36 + lane * 6;
+    const size_t o = (size_t)i * 6;
+    for (int c = 0; c <= lane; ++c) acc[lane] += double(Ci[c]) * (r[o + c] - alpha * Ap[o + c]);
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
@@ -243,7 +284,8 @@ __device__ __forceinline__ double jacobi_row(const PcgArgs& a, int i, int lane, 
 //                                                                              -- 1 barrier
 //   B: x += alpha p, r -= alpha Ap, z_f = fine preconditioner of r, sums r.z_f, r.r and, with
 //      the gauge space, y = Z^T r                                              -- 1 barrier
-//      (the learned factor needs its two triangular halves first: 2 more barriers)
+//      (the learned factor needs its lower triangular half first, fed with r - alpha Ap formed
+//      on the fly: 1 more barrier; r is double-buffered)
 // With the gauge space, z = z_f + Z c with c = (Z^T S Z)^-1 y is never stored: every reader
 // forms it from z_f, the camera frames and c (r.z = r.z_f + y.c).  p alternates between two
 // buffers so that phase A never overwrites a p_old that a neighbour reads.
@@ -371,15 +413,18 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs a) {
 #pragma unroll
       for (int k = 0; k < 2 + kGauge; ++k) u[k] = 0.0;
       if constexpr (LEARNED) {
-        for (int i = warp; i < N; i += nwarps)
+        for (int i = warp; i < N; i += nwarps) {
+          learned_lower_row_step(a, i, lane, a.r, a.Ap, alpha, a.t);
           if (lane < DA) {
             const size_t q = (size_t)i * DA + lane;
             a.x[q] += alpha * p_new[q];
-            a.r[q] -= alpha * a.Ap[q];
+            a.r2[q] = a.r[q] - alpha * a.Ap[q];
           }
+        }
         grid.sync();
-        for (int i = warp; i < N; i += nwarps) learned_lower_row(a, i, lane, a.r, a.t);
-        grid.sync();
+        double* tr = a.r;
+        a.r = a.r2;
+        a.r2 = tr;
         for (int i = warp; i < N; i += nwarps) fine_and_sums(i, lane < DA ? a.r[(size_t)i * DA + lane] : 0.0, u);
       } else {
         for (int i = warp; i < N; i += nwarps) {
@@ -556,7 +601,7 @@ int pcg_alloc(PcgState& ps, int nb, int N, int DA) {
   const size_t n = (size_t)N * DA;
   V3DBA_CUDA_TRY(cudaMalloc(&ps.Sb, sizeof(double) * (size_t)std::max(nb, 1) * DA * DA));
   V3DBA_CUDA_TRY(cudaMalloc(&ps.Pinv, sizeof(double) * (size_t)std::max(N, 1) * DA * DA));
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.vec, sizeof(double) * 7 * std::max<size_t>(n, 1)));   // b r z p Ap t p2
+  V3DBA_CUDA_TRY(cudaMalloc(&ps.vec, sizeof(double) * 8 * std::max<size_t>(n, 1)));   // b r z p Ap t p2 r2
   V3DBA_CUDA_TRY(cudaMalloc(&ps.part, sizeof(double) * 2 * kPartStride * kPcgMaxGrid));
   V3DBA_CUDA_TRY(cudaMalloc(&ps.gauge_rows, sizeof(double) * kGaugeTri * (size_t)std::max(N, 1)));
   V3DBA_CUDA_TRY(cudaMalloc(&ps.gauge_L, sizeof(double) * (kGaugeTri + 1)));
@@ -599,7 +644,7 @@ PcgArgs make_args(PcgState& ps, int N, int DA, double tol, int max_iter, double*
   a.rp = ps.rp; a.rb = ps.rb; a.rc = ps.rc; a.rt = ps.rt; a.Sb = ps.Sb;
   a.Pinv = ps.Pinv; a.b = ps.b; a.x = x;
   a.r = ps.vec + n; a.z = ps.vec + 2 * n; a.p = ps.vec + 3 * n; a.Ap = ps.vec + 4 * n;
-  a.t = ps.vec + 5 * n; a.p2 = ps.vec + 6 * n;
+  a.t = ps.vec + 5 * n; a.p2 = ps.vec + 6 * n; a.r2 = ps.vec + 7 * n;
   a.cinv = P.cinv;
   a.ehat = P.ehat;
   a.frames = P.frames;

@@ -183,64 +183,61 @@ __global__ void k_gnn_edge_norm(const Real* __restrict__ Sb, GnnGraph g, const f
     }
 }
 
-__global__ void k_gnn_two_hop(GnnGraph g, float* xe) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+// Two-hop products of every edge: 72 threads per edge, one per output entry (36 of (F F), 36 of
+// (F F^T)); the threads of an edge walk its triangles together and share their loads.
+__global__ void __launch_bounds__(288) k_gnn_two_hop(GnnGraph g, float* xe) {
+  const int e = blockIdx.x * 4 + threadIdx.y;
   if (e >= g.ne) return;
-  float p2[36], pt[36];
-#pragma unroll
-  for (int t = 0; t < 36; ++t) { p2[t] = 0.f; pt[t] = 0.f; }
+  const int o = threadIdx.x;                 // 0..71
+  const int kind = o >= 36 ? 1 : 0;
+  const int r = (o % 36) / 6, c = o % 6;
+  float acc = 0.f;
   for (int t = g.tri_ptr[e]; t < g.tri_ptr[e + 1]; ++t) {
-    const float* A = xe + (size_t)g.tri_1[t] * kGnnEdgeIn;
+    if (g.tri_t[t] != kind) continue;
+    const float* A = xe + (size_t)g.tri_1[t] * kGnnEdgeIn + r * 6;
     const float* B = xe + (size_t)g.tri_2[t] * kGnnEdgeIn;
-    if (g.tri_t[t] == 0) {
+    if (kind == 0) {
 #pragma unroll
-      for (int r = 0; r < 6; ++r)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          float v = 0.f;
-#pragma unroll
-          for (int k = 0; k < 6; ++k) v += A[r * 6 + k] * B[k * 6 + c];
-          p2[r * 6 + c] += v;
-        }
+      for (int k = 0; k < 6; ++k) acc += A[k] * B[k * 6 + c];
     } else {
 #pragma unroll
-      for (int r = 0; r < 6; ++r)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          float v = 0.f;
-#pragma unroll
-          for (int k = 0; k < 6; ++k) v += A[r * 6 + k] * B[c * 6 + k];
-          pt[r * 6 + c] += v;
-        }
+      for (int k = 0; k < 6; ++k) acc += A[k] * B[c * 6 + k];
     }
   }
-  float* o = xe + (size_t)e * kGnnEdgeIn;
-#pragma unroll
-  for (int t = 0; t < 36; ++t) { o[36 + t] = p2[t]; o[72 + t] = pt[t]; }
+  xe[(size_t)e * kGnnEdgeIn + 36 + o] = acc;
 }
 
 __device__ __forceinline__ int node_degree(const GnnGraph& g, int i) {
   return (g.lo_ptr[i + 1] - g.lo_ptr[i]) + (g.up_ptr[i + 1] - g.up_ptr[i]);
 }
 
+// Node statistics, one warp per node (lanes over its incident edges).
 __global__ void k_gnn_node_feat(GnnGraph g, const float* __restrict__ xe, float* xn) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= g.N) return;
-  float sum = 0.f, mx = 0.f;
-  auto visit = [&](int e) {
-    const float* F = xe + (size_t)e * kGnnEdgeIn;
-    float s = 0.f;
-    for (int t = 0; t < 36; ++t) s += F[t] * F[t];
-    sum += s;
-    mx = fmaxf(mx, s);
-  };
-  for (int q = g.lo_ptr[i]; q < g.lo_ptr[i + 1]; ++q) visit(g.lo_e[q]);
-  for (int q = g.up_ptr[i]; q < g.up_ptr[i + 1]; ++q) visit(g.up_e[q]);
+  const int nlo = g.lo_ptr[i + 1] - g.lo_ptr[i];
   const int deg = node_degree(g, i);
-  xn[(size_t)i * 4 + 0] = 1.f;
-  xn[(size_t)i * 4 + 1] = log1pf((float)deg);
-  xn[(size_t)i * 4 + 2] = deg ? sum / deg : 0.f;
-  xn[(size_t)i * 4 + 3] = mx;
+  float sum = 0.f, mx = 0.f;
+  for (int q = lane; q < deg; q += 32) {
+    const int e = q < nlo ? g.lo_e[g.lo_ptr[i] + q] : g.up_e[g.up_ptr[i] + q - nlo];
+    const float4* F = reinterpret_cast<const float4*>(xe + (size_t)e * kGnnEdgeIn);
+    float v = 0.f;
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const float4 f = F[t];
+      v += f.x * f.x + f.y * f.y + f.z * f.z + f.w * f.w;
+    }
+    sum += v;
+    mx = fmaxf(mx, v);
+  }
+  sum = warp_sum(sum);
+  mx = warp_max(mx);
+  if (lane == 0) {
+    xn[(size_t)i * 4 + 0] = 1.f;
+    xn[(size_t)i * 4 + 1] = log1pf((float)deg);
+    xn[(size_t)i * 4 + 2] = deg ? sum / deg : 0.f;
+    xn[(size_t)i * 4 + 3] = mx;
+  }
 }
 
 // --------------------------------------------------------------------------------------------
@@ -400,15 +397,30 @@ __global__ void __launch_bounds__(128) k_rowgemm_bf16(RowGemm g, const __nv_bflo
   __nv_bfloat16* a_s = reinterpret_cast<__nv_bfloat16*>(smb);
   __nv_bfloat16* b_s = a_s + 64 * ld;
   const int r0 = blockIdx.x * 64;
-  for (int t = threadIdx.x; t < 64 * Kp; t += blockDim.x) {
-    const int n = t / Kp, k = t - n * Kp;
-    b_s[n * ld + k] = Wt[t];
+  // weights: 8 bf16 per 16-byte copy (Kp is a multiple of 16, rows of b_s 16-byte aligned)
+  const int kq8 = Kp / 8;
+  for (int t = threadIdx.x; t < 64 * kq8; t += blockDim.x) {
+    const int n = t / kq8, k = (t - n * kq8) * 8;
+    *reinterpret_cast<uint4*>(b_s + n * ld + k) = *reinterpret_cast<const uint4*>(Wt + (size_t)n * Kp + k);
   }
-  for (int t = threadIdx.x; t < 64 * Kp; t += blockDim.x) {
-    const int r = t / Kp, k = t - r * Kp;
+  // inputs: 4 floats per 16-byte load (segment widths and leading dimensions are multiples of 4)
+  const int kq4 = Kp / 4;
+  for (int t = threadIdx.x; t < 64 * kq4; t += blockDim.x) {
+    const int r = t / kq4, k = (t - r * kq4) * 4;
     const int row = r0 + r;
-    const float v = (row < g.rows && k < g.K) ? seg_load(g.seg, g.nseg, row, k) : 0.f;
-    a_s[r * ld + k] = __float2bfloat16_rn(v);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (row < g.rows && k < g.K) {
+      int sgi = 0, kk = k;
+      while (sgi + 1 < g.nseg && kk >= g.seg[sgi].width) { kk -= g.seg[sgi].width; ++sgi; }
+      const Seg& sg = g.seg[sgi];
+      const int src_row = sg.idx ? sg.idx[row] : row;
+      v = *reinterpret_cast<const float4*>(sg.src + (size_t)src_row * sg.ld + kk);
+    }
+    __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
+    uint2 pk;
+    pk.x = *reinterpret_cast<uint32_t*>(&lo);
+    pk.y = *reinterpret_cast<uint32_t*>(&hi);
+    *reinterpret_cast<uint2*>(a_s + r * ld + k) = pk;
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -687,6 +699,7 @@ __global__ void k_pack_bf16(const float* __restrict__ W, int K, int Kp, __nv_bfl
 int gnn_features(const GnnGraph& g, const void* Sb, bool fp64, const int* diag_blk, float* cinv, float* xe, float* xn,
                  int* d_fail, cudaStream_t st) {
   const int N = g.N, ne = g.ne;
+  if (reinterpret_cast<uintptr_t>(xe) & 15) return V3DBA_ERR_UNSUPPORTED;   // 16-byte loads of edge rows
   if (fp64) k_gnn_cinv<double><<<cdiv(N, 128), 128, 0, st>>>((const double*)Sb, diag_blk, N, cinv, d_fail);
   else k_gnn_cinv<float><<<cdiv(N, 128), 128, 0, st>>>((const float*)Sb, diag_blk, N, cinv, d_fail);
   V3DBA_LAUNCH_CHECK();
@@ -694,10 +707,10 @@ int gnn_features(const GnnGraph& g, const void* Sb, bool fp64, const int* diag_b
     if (fp64) k_gnn_edge_norm<double><<<cdiv(ne, 128), 128, 0, st>>>((const double*)Sb, g, cinv, xe);
     else k_gnn_edge_norm<float><<<cdiv(ne, 128), 128, 0, st>>>((const float*)Sb, g, cinv, xe);
     V3DBA_LAUNCH_CHECK();
-    k_gnn_two_hop<<<cdiv(ne, 128), 128, 0, st>>>(g, xe);
+    k_gnn_two_hop<<<cdiv(ne, 4), dim3(72, 4), 0, st>>>(g, xe);
     V3DBA_LAUNCH_CHECK();
   }
-  k_gnn_node_feat<<<cdiv(N, 128), 128, 0, st>>>(g, xe, xn);
+  k_gnn_node_feat<<<cdiv(N, 8), 256, 0, st>>>(g, xe, xn);
   V3DBA_LAUNCH_CHECK();
   return V3DBA_OK;
 }
@@ -822,7 +835,12 @@ int rowgemm_bf16(v3dba_precond_model_s* m, cudaStream_t st, int rows, std::initi
   if (rows <= 0) return V3DBA_OK;
   RowGemm g;
   g.rows = rows;
-  for (const Seg& s : in) { g.seg[g.nseg++] = s; g.K += s.width; }
+  for (const Seg& s : in) {
+    // the kernel stages its inputs with 16-byte loads
+    if ((reinterpret_cast<uintptr_t>(s.src) & 15) || (s.ld & 3) || (s.width & 3)) return V3DBA_ERR_UNSUPPORTED;
+    g.seg[g.nseg++] = s;
+    g.K += s.width;
+  }
   g.bias = bias; g.Nout = kGnnH; g.out = out; g.ldo = kGnnH; g.resid = resid; g.relu = relu ? 1 : 0;
   const int Kp = kPackK[layer];
   const size_t smem = sizeof(__nv_bfloat16) * 2 * 64 * (size_t)(Kp + 8);
@@ -1062,7 +1080,8 @@ struct PrecondSystem {
   float* xe = nullptr;
   float* xn = nullptr;
   float* ehat = nullptr;
-  double* frames = nullptr;   // camera frames of the gauge space (captured systems only)
+  double* frames = nullptr;   // camera frames of the gauge space
+  double* rhs = nullptr;      // the LM's reduced right-hand side (captured systems only)
   double* x = nullptr;
   int* fail = nullptr;
 };
@@ -1070,7 +1089,8 @@ struct PrecondSystem {
 void system_free(PrecondSystem& s) {
   gnn_graph_free(s.g);
   pcg_free(s.ps);
-  cudaFree(s.cinv); cudaFree(s.xe); cudaFree(s.xn); cudaFree(s.ehat); cudaFree(s.frames); cudaFree(s.x);
+  cudaFree(s.cinv); cudaFree(s.xe); cudaFree(s.xn); cudaFree(s.ehat); cudaFree(s.frames); cudaFree(s.rhs);
+  cudaFree(s.x);
   cudaFree(s.fail);
   s = PrecondSystem();
 }
@@ -1234,7 +1254,8 @@ int v3dba_precond_set_destroy(v3dba_precond_set s) {
 int v3dba_precond_set_count(v3dba_precond_set s) { return s ? (int)s->sys.size() : 0; }
 
 int v3dba_precond_set_add_blocks(v3dba_precond_set s, int n_cameras, int n_blocks, const int32_t* blk_i,
-                                 const int32_t* blk_l, const double* blocks) {
+                                 const int32_t* blk_l, const double* blocks, const double* R, const double* T) {
+  if ((R == nullptr) != (T == nullptr)) return V3DBA_ERR_INVALID_ARGUMENT;
   if (!s || n_cameras <= 0 || n_blocks <= 0 || !blk_i || !blk_l || !blocks) return V3DBA_ERR_INVALID_ARGUMENT;
   std::vector<int> bi(n_blocks), bl(n_blocks);
   std::vector<uint8_t> seen_diag(n_cameras, 0);
@@ -1253,6 +1274,15 @@ int v3dba_precond_set_add_blocks(v3dba_precond_set s, int n_cameras, int n_block
     if (!std::isfinite(blocks[t])) return V3DBA_ERR_INVALID_INPUT;
   return system_create(s, n_cameras, bi, bl, [&](PrecondSystem& ps) -> int {
     V3DBA_CUDA_TRY(cudaMemcpy(ps.ps.Sb, blocks, sizeof(double) * (size_t)n_blocks * 36, cudaMemcpyHostToDevice));
+    if (R) {
+      std::vector<double> f((size_t)n_cameras * 12);
+      for (int i = 0; i < n_cameras; ++i) {
+        for (int q = 0; q < 9; ++q) f[(size_t)i * 12 + q] = R[(size_t)i * 9 + q];
+        for (int q = 0; q < 3; ++q) f[(size_t)i * 12 + 9 + q] = T[(size_t)i * 3 + q];
+      }
+      V3DBA_CUDA_TRY(cudaMalloc(&ps.frames, sizeof(double) * f.size()));
+      V3DBA_CUDA_TRY(cudaMemcpy(ps.frames, f.data(), sizeof(double) * f.size(), cudaMemcpyHostToDevice));
+    }
     return V3DBA_OK;
   });
 }
@@ -1272,12 +1302,15 @@ int v3dba_precond_set_capture(v3dba_precond_set s, v3dba_handle h, double lambda
   if ((rc = ops->build_reduced(ds, hst))) return rc;
   V3DBA_CUDA_TRY(cudaStreamSynchronize(hst));
   const void* src = handle_pcg(h).Sb;
+  const double* src_rhs = handle_pcg(h).b;
   const size_t bytes = sizeof(double) * (size_t)ds.nb * 36;
   const int N = ds.d.N, n_fixed = ds.d.nnA;
   const double* R = handle_cur_R(h);
   const double* T = handle_cur_T(h);
   return system_create(s, N, handle_blk_i(h), handle_blk_l(h), [&](PrecondSystem& ps) -> int {
     V3DBA_CUDA_TRY(cudaMemcpy(ps.ps.Sb, src, bytes, cudaMemcpyDeviceToDevice));
+    V3DBA_CUDA_TRY(cudaMalloc(&ps.rhs, sizeof(double) * 6 * (size_t)std::max(N, 1)));
+    V3DBA_CUDA_TRY(cudaMemcpy(ps.rhs, src_rhs, sizeof(double) * 6 * (size_t)N, cudaMemcpyDeviceToDevice));
     V3DBA_CUDA_TRY(cudaMalloc(&ps.frames, sizeof(double) * 12 * (size_t)std::max(N, 1)));
     int rc2 = gauge_frames(R, T, N, n_fixed, ps.frames, s->st);
     if (rc2) return rc2;
@@ -1370,21 +1403,39 @@ int v3dba_precond_train(v3dba_precond_model m, v3dba_precond_set s, int epochs, 
 }
 
 int v3dba_precond_pcg_iterations(v3dba_precond_model m, v3dba_precond_set s, int index, double tol, int max_iter,
-                                 uint32_t rhs_seed, int* iters) {
+                                 uint32_t rhs_seed, int* iters, double* ms) {
   if (!valid_index(s, index) || !(tol > 0.0) || max_iter <= 0 || !iters) return V3DBA_ERR_INVALID_ARGUMENT;
   PrecondSystem& p = s->sys[index];
   const int n = p.N * 6;
-  std::vector<double> b(n);
-  std::mt19937_64 rng(rhs_seed);
-  std::normal_distribution<double> nd(0.0, 1.0);
-  for (double& v : b) v = nd(rng);
   cudaStream_t st = s->st;
-  V3DBA_CUDA_TRY(cudaMemcpyAsync(p.ps.b, b.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  std::vector<double> b(n);
+  if (rhs_seed == 0 && p.rhs) {
+    V3DBA_CUDA_TRY(cudaMemcpyAsync(p.ps.b, p.rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  } else {
+    std::mt19937_64 rng(rhs_seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    for (double& v : b) v = nd(rng);
+    V3DBA_CUDA_TRY(cudaMemcpyAsync(p.ps.b, b.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  }
   int rc;
+  cudaEvent_t e0, e1;
+  V3DBA_CUDA_TRY(cudaEventCreate(&e0));
+  V3DBA_CUDA_TRY(cudaEventCreate(&e1));
+  auto elapsed = [&](double* out) -> int {
+    float t = 0.f;
+    V3DBA_CUDA_TRY(cudaEventSynchronize(e1));
+    V3DBA_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+    if (out) *out = t;
+    return V3DBA_OK;
+  };
+  if (ms)
+    for (int v = 0; v < 5; ++v) ms[v] = -1.0;
   if (m) {
     V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+    V3DBA_CUDA_TRY(cudaEventRecord(e0, m->st));
     if ((rc = gnn_precond_blocks(m, p.g, p.cinv, p.xe, p.xn, p.ehat, m->st))) return rc;
-    V3DBA_CUDA_TRY(cudaStreamSynchronize(m->st));
+    V3DBA_CUDA_TRY(cudaEventRecord(e1, m->st));
+    if ((rc = elapsed(ms ? ms + 4 : nullptr))) return rc;
   }
   for (int v = 0; v < 4; ++v) {
     iters[v] = -1;
@@ -1394,13 +1445,18 @@ int v3dba_precond_pcg_iterations(v3dba_precond_model m, v3dba_precond_set s, int
     if (learned) { P.cinv = p.cinv; P.ehat = p.ehat; }
     if (gauge) P.frames = p.frames;
     V3DBA_CUDA_TRY(cudaMemsetAsync(p.fail, 0, sizeof(int), st));
+    V3DBA_CUDA_TRY(cudaEventRecord(e0, st));
     if ((rc = pcg_solve_precond(p.ps, p.N, 6, true, tol, max_iter, p.x, p.fail, st, P))) return rc;
+    V3DBA_CUDA_TRY(cudaEventRecord(e1, st));
+    if ((rc = elapsed(ms ? ms + v : nullptr))) return rc;
     int its = 0, fl = 0;
     V3DBA_CUDA_TRY(cudaMemcpyAsync(&its, p.ps.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
     V3DBA_CUDA_TRY(cudaMemcpyAsync(&fl, p.fail, sizeof(int), cudaMemcpyDeviceToHost, st));
     V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
     iters[v] = fl ? max_iter : its;
   }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return V3DBA_OK;
 }
 

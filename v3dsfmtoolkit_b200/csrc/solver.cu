@@ -77,11 +77,30 @@ bool all_finite(const double* p, size_t n) {
   return true;
 }
 
+// Handle buffers come from the device's stream-ordered pool, which keeps freed memory for the
+// next handle (release threshold raised once per device): creating and destroying handles in a
+// loop then neither maps nor unmaps device memory, and destroy does not stall on cudaFree.
+int ensure_pool() {
+  static std::atomic<uint64_t> done_mask{0};
+  int dev = 0;
+  V3DBA_CUDA_TRY(cudaGetDevice(&dev));
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done_mask.load() & bit) return V3DBA_OK;
+  cudaMemPool_t pool;
+  V3DBA_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t thr = UINT64_MAX;
+  V3DBA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  done_mask.fetch_or(bit);
+  return V3DBA_OK;
+}
+
 template <typename T>
 int dalloc(v3dba_handle h, T** p, size_t count) {
   void* q = nullptr;
   const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-  cudaError_t e = cudaMalloc(&q, bytes);
+  int rc0 = ensure_pool();
+  if (rc0) return rc0;
+  cudaError_t e = cudaMallocAsync(&q, bytes, h->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? V3DBA_ERR_OUT_OF_MEMORY : V3DBA_ERR_CUDA;
@@ -128,14 +147,17 @@ template <typename T>
 int upload(v3dba_handle h, T** d, const std::vector<T>& v) {
   int rc = dalloc(h, d, v.size());
   if (rc) return rc;
-  if (!v.empty()) V3DBA_CUDA_TRY(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  if (!v.empty())
+    V3DBA_CUDA_TRY(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, h->stream));
   return V3DBA_OK;
 }
 
 void free_handle(v3dba_handle h) {
   if (!h) return;
-  if (h->stream) cudaStreamSynchronize(h->stream);
-  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) {
+    for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
+    cudaStreamSynchronize(h->stream);
+  }
   tile_chol_free(h->chol);
   pcg_free(h->pcg);
   gnn_graph_free(h->gnn);
@@ -583,8 +605,8 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
   if ((rc = ops->build_reduced(s, st))) return rc;
   int fallback = 0;
   if (pcg && precond != V3DBA_PRECOND_BLOCK_JACOBI) {
-    // learned factor (+ gauge space) or block-Jacobi + gauge space; plain block-Jacobi re-solves
-    // the trial when that fails or stalls
+    // learned factor or block-Jacobi + gauge space; plain block-Jacobi re-solves the trial when
+    // that breaks down
     const bool learned = precond == V3DBA_PRECOND_LEARNED;
     V3DBA_CUDA_TRY(cudaMemsetAsync(h->gnn_fail, 0, sizeof(int), st));
     if ((rc = gauge_frames(s.cur.R, s.cur.T, s.d.N, s.d.nnA, h->gauge_frames, st))) return rc;
@@ -599,7 +621,7 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
     if (!ffail) {
       PcgPrecond P;
       if (learned) { P.cinv = h->gnn_cinv; P.ehat = h->gnn_ehat; }
-      P.frames = h->gauge_frames;
+      else P.frames = h->gauge_frames;
       if ((rc = pcg_solve_precond(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x,
                                   h->gnn_fail, st, P)))
         return rc;
@@ -608,7 +630,9 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
       V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
     }
     h->h_scalars[10] = its;
-    if (ffail || its >= o.pcg_max_iterations) {
+    // an iteration-capped solve is an inexact step, as with block-Jacobi; only a breakdown (a
+    // diagonal block that is not positive definite, or p.Ap <= 0) falls back
+    if (ffail) {
       fallback = 1;
       if ((rc = pcg_solve(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x, s.d_fail, st)))
         return rc;

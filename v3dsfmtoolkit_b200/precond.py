@@ -74,12 +74,14 @@ def train(pset, epochs=30, lr=1e-3, seed=0, model=None):
     return model, hist
 
 
-def evaluate(pset, model, tol=1e-6, max_iter=3000, rhs_seed=1):
+def evaluate(pset, model, tol=1e-6, max_iter=5000, rhs_seed=0):
     """PCG iteration counts of every system in `pset`: an (n, 4) array over VARIANTS; -1 where
-    a variant does not apply."""
+    a variant does not apply.  rhs_seed 0 solves with each captured system's own right-hand side
+    (the LM's reduced gradient, which has no component along the gauge motions); a positive seed
+    uses seeded random right-hand sides instead (seed + index)."""
     out = []
     for i in range(len(pset)):
-        d = pset.pcg_iterations(i, model, tol=tol, max_iter=max_iter, rhs_seed=rhs_seed + i)
+        d = pset.pcg_iterations(i, model, tol=tol, max_iter=max_iter, rhs_seed=rhs_seed + i if rhs_seed else 0)
         out.append([(-1 if d[k] is None else d[k]) for k in VARIANTS])
     return np.array(out, dtype=np.int64).reshape(-1, 4)
 
@@ -133,8 +135,9 @@ def _main():
     for s in range(a.eval_seed_base, a.eval_seed_base + a.eval_scenes):
         capture(eset, training_scenes(s, n_max=a.n_max), 4)
     report["eval_systems"] = len(eset)
-    report["trained"] = summarize(evaluate(eset, model))
-    report["untrained"] = summarize(evaluate(eset, untrained))
+    report["lm_rhs"] = {"trained": summarize(evaluate(eset, model)), "untrained": summarize(evaluate(eset, untrained))}
+    report["random_rhs"] = {"trained": summarize(evaluate(eset, model, rhs_seed=1)),
+                            "untrained": summarize(evaluate(eset, untrained, rhs_seed=1))}
     print(json.dumps(report), flush=True)
     if a.report:
         with open(a.report, "w") as f:
