@@ -579,7 +579,7 @@ def run_cluster(args, rank, world, local_rank):
         "config": {"workload": "cluster2000", "n_cameras": sc.n_cams, "n_points": sc.n_points,
                    "n_observations": sc.n_obs, "model": "StdMetricBundleOptimizer",
                    "solver": "PCG, relative residual 1e-6 per LM step",
-                   "preconditioner": ("learned factor + gauge coarse space" if model is not None
+                   "preconditioner": ("learned factor" if model is not None
                                       else "block-Jacobi + gauge coarse space"),
                    "stop": f"cost <= direct-solve cost after 25 iterations * (1 + {REL_TOL})",
                    "l2": "flushed (256 MiB write) before every step",
