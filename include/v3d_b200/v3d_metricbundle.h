@@ -49,6 +49,10 @@ namespace V3D
 {
    using std::vector;
 
+   // The C-ABI reads measurements and points in place from the caller's vectors.
+   static_assert(sizeof(Vector2d) == 2 * sizeof(double), "Vector2d must be two packed doubles");
+   static_assert(sizeof(Vector3d) == 3 * sizeof(double), "Vector3d must be three packed doubles");
+
    enum
    {
       FULL_BUNDLE_NO_ROTATIONS = V3DBA_FULL_BUNDLE_NO_ROTATIONS,
@@ -76,16 +80,16 @@ namespace V3D
               _distortions(distortions), _handle(0), _nnA(0), _nnB(0), _nnC(0)
          {
             int const N = cams.size(), M = Xs.size(), Kn = measurements.size();
-            std::vector<double> Kb, R, T, D, X, meas(2 * (size_t)Kn);
-            pack(Kb, R, T, D, X);
-            for (int k = 0; k < Kn; ++k) { meas[2 * k] = measurements[k][0]; meas[2 * k + 1] = measurements[k][1]; }
+            std::vector<double> Kb, R, T, D;
+            pack(Kb, R, T, D);
             v3dba_problem p;
             p.model = model; p.mode = mode;
             p.n_cameras = N; p.n_points = M; p.n_measurements = Kn;
             p.inlier_threshold = inlierThreshold;
             p.K = Kb.data(); p.R = R.data(); p.T = T.data();
-            p.dist = D.empty() ? 0 : D.data(); p.X = X.data();
-            p.measurements = meas.data();
+            p.dist = D.empty() ? 0 : D.data(); p.X = points();
+            // the measurements are passed in place: a vector<Vector2d> is 2 doubles per element
+            p.measurements = Kn ? measurements[0].begin() : 0;
             p.view = corrspondingView.data(); p.point = corrspondingPoint.data();
             lastError = v3dba_create(&p, &_handle);
             if (lastError != V3DBA_OK)
@@ -111,9 +115,9 @@ namespace V3D
          {
             status = LEVENBERG_OPTIMIZER_TIMEOUT;
             if (!_handle) return;
-            std::vector<double> Kb, R, T, D, X;
-            pack(Kb, R, T, D, X);
-            int rc = v3dba_set_params(_handle, Kb.data(), R.data(), T.data(), D.empty() ? 0 : D.data(), X.data());
+            std::vector<double> Kb, R, T, D;
+            pack(Kb, R, T, D);
+            int rc = v3dba_set_params(_handle, Kb.data(), R.data(), T.data(), D.empty() ? 0 : D.data(), points());
             if (rc == V3DBA_OK) rc = v3dba_set_nonvarying(_handle, _nnA, _nnB, _nnC);
             if (rc == V3DBA_OK) rc = v3dba_set_lambda(_handle, lambda);
             v3dba_options o;
@@ -124,14 +128,14 @@ namespace V3D
             o.precision = precision;
             v3dba_result r;
             if (rc == V3DBA_OK) rc = v3dba_minimize(_handle, &o, &r);
-            if (rc == V3DBA_OK) rc = v3dba_get_params(_handle, Kb.data(), R.data(), T.data(), D.empty() ? 0 : D.data(), X.data());
+            if (rc == V3DBA_OK) rc = v3dba_get_params(_handle, Kb.data(), R.data(), T.data(), D.empty() ? 0 : D.data(), points());
             lastError = rc;
             if (rc != V3DBA_OK)
             {
                std::fprintf(stderr, "v3dba_minimize failed: %s\n", v3dba_error_string(rc));
                return;
             }
-            unpack(Kb, R, T, D, X);
+            unpack(Kb, R, T, D);
             status = r.status;
             currentIteration = r.iterations;
             lambda = r.lambda;
@@ -143,11 +147,14 @@ namespace V3D
          v3dba_result lastResult;
 
       protected:
+         // The points are read and written in place: a vector<Vector3d> is 3 doubles per element.
+         double* points() { return _Xs.empty() ? 0 : _Xs[0].begin(); }
+
          void pack(std::vector<double>& Kb, std::vector<double>& R, std::vector<double>& T,
-                   std::vector<double>& D, std::vector<double>& X) const
+                   std::vector<double>& D) const
          {
-            int const N = _cams.size(), M = _Xs.size();
-            R.resize(9 * (size_t)N); T.resize(3 * (size_t)N); X.resize(3 * (size_t)M);
+            int const N = _cams.size();
+            R.resize(9 * (size_t)N); T.resize(3 * (size_t)N);
             Kb.resize(_model == V3DBA_MODEL_COMMON ? 9 : 9 * (size_t)N);
             for (int i = 0; i < N; ++i)
             {
@@ -179,14 +186,12 @@ namespace V3D
                   StdDistortionFunction const& d = (*_distortions)[i];
                   D.push_back(d.k1); D.push_back(d.k2); D.push_back(d.p1); D.push_back(d.p2);
                }
-            for (int j = 0; j < M; ++j)
-               for (int r = 0; r < 3; ++r) X[3 * j + r] = _Xs[j][r];
          }
 
          void unpack(std::vector<double> const& Kb, std::vector<double> const& R, std::vector<double> const& T,
-                     std::vector<double> const& D, std::vector<double> const& X)
+                     std::vector<double> const& D)
          {
-            int const N = _cams.size(), M = _Xs.size();
+            int const N = _cams.size();
             for (int i = 0; i < N; ++i)
             {
                Matrix3x3d Ri;
@@ -214,8 +219,6 @@ namespace V3D
                   for (int c = 0; c < 3; ++c) (*_K)[r][c] = Kb[3 * r + c];
                _distortion->k1 = D[0]; _distortion->k2 = D[1]; _distortion->p1 = D[2]; _distortion->p2 = D[3];
             }
-            for (int j = 0; j < M; ++j)
-               for (int r = 0; r < 3; ++r) _Xs[j][r] = X[3 * j + r];
          }
 
          int const _model, _mode;

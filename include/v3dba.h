@@ -333,6 +333,15 @@ int v3dba_precond_train(v3dba_precond_model m, v3dba_precond_set s, int epochs, 
 int v3dba_precond_pcg_iterations(v3dba_precond_model m, v3dba_precond_set s, int index, double tol, int max_iter,
                                  uint32_t rhs_seed, int* iters, double* ms);
 
+/* The structure v3dba_create built on the device (inspection): the number of observation pairs
+ * and camera-pair blocks, and, for every pointer that is not NULL, o_orig [K] (caller's index of
+ * each point-major observation), c_ptr [N+1] / c_obs [K] (observations of each camera), b_i,
+ * b_l [nb] / b_ptr [nb+1] (blocks (i <= l) and their pairs), pr_k, pr_m [P] (the pairs).  Replaces
+ * the host-side pattern analysis of SparseLevenbergOptimizer::setupSparseJtJ
+ * (V3D/src/Math/v3d_optimization.cpp:301-554). */
+int v3dba_structure(v3dba_handle h, int64_t* n_pairs, int* n_blocks, int32_t* o_orig, int32_t* c_ptr, int32_t* c_obs,
+                    int32_t* b_i, int32_t* b_l, int32_t* b_ptr, int32_t* pr_k, int32_t* pr_m);
+
 /* FP64 tensor-core (DMMA) throughput of the current GPU in TFLOP/s, measured by a short kernel
  * of independent mma.sync f64 chains on every SM (benchmark support). */
 int v3dba_measure_fp64_mma_peak(double* tflops);

@@ -39,7 +39,7 @@ EXPORTS = (
     "v3dba_set_precond_model", "v3dba_precond_set_create", "v3dba_precond_set_destroy", "v3dba_precond_set_count",
     "v3dba_precond_set_add_blocks", "v3dba_precond_set_capture", "v3dba_precond_set_info",
     "v3dba_precond_set_features", "v3dba_precond_loss_grad", "v3dba_precond_coefficients", "v3dba_precond_train",
-    "v3dba_precond_pcg_iterations",
+    "v3dba_precond_pcg_iterations", "v3dba_structure",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -113,6 +113,7 @@ def _lib():
         L.v3dba_batch_get_all_params.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.v3dba_measure_fp64_mma_peak.argtypes = [_dp]
         L.v3dba_cholesky_flops.argtypes = [C.c_void_p, _dp]
+        L.v3dba_structure.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int)] + [_ip] * 8
         _fp = C.POINTER(C.c_float)
         L.v3dba_precond_model_size.argtypes = []
         L.v3dba_precond_model_create.argtypes = [_fp, C.c_uint32, C.POINTER(C.c_void_p)]
@@ -229,6 +230,18 @@ class Handle:
         r = Result()
         check(_lib().v3dba_minimize(self.h, C.byref(o), C.byref(r)), "v3dba_minimize")
         return r
+
+    def structure(self):
+        """The device-built structure: dict of o_orig, c_ptr, c_obs, b_i, b_l, b_ptr, pr_k, pr_m."""
+        P, nb = C.c_int64(), C.c_int()
+        L = _lib()
+        check(L.v3dba_structure(self.h, C.byref(P), C.byref(nb), *([None] * 8)), "v3dba_structure")
+        K, N = self.n_obs, self.n_cams
+        sizes = {"o_orig": K, "c_ptr": N + 1, "c_obs": K, "b_i": nb.value, "b_l": nb.value, "b_ptr": nb.value + 1,
+                 "pr_k": P.value, "pr_m": P.value}
+        out = {k: np.zeros(max(v, 1), dtype=np.int32) for k, v in sizes.items()}
+        check(L.v3dba_structure(self.h, None, None, *[out[k].ctypes.data_as(_ip) for k in sizes]), "v3dba_structure")
+        return {k: out[k][:v] for k, v in sizes.items()}
 
     def set_precond_model(self, model):
         """Attaches a PrecondModel for preconditioner=PRECOND_LEARNED (kept alive by the handle)."""

@@ -203,3 +203,26 @@ extern "C" int v3dba_dense_cholesky_solve(int n, const double* S, const double* 
   tile_chol_free(tc);
   return rc;
 }
+
+// The structure built by v3dba_create: sizes always; every array pointer that is not NULL
+// receives its array (o_orig, c_ptr, c_obs [K], [N+1], [K]; b_i, b_l [nb], b_ptr [nb+1];
+// pr_k, pr_m [P]).
+extern "C" int v3dba_structure(v3dba_handle h, int64_t* n_pairs, int* n_blocks, int* o_orig, int* c_ptr, int* c_obs,
+                               int* b_i, int* b_l, int* b_ptr, int* pr_k, int* pr_m) {
+  if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
+  DevState& s = handle_state(h);
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(handle_stream(h)));
+  const size_t K = s.d.K, N = s.d.N, nb = s.nb, P = (size_t)s.P;
+  if (n_pairs) *n_pairs = s.P;
+  if (n_blocks) *n_blocks = s.nb;
+  auto get = [](int* dst, const int* src, size_t n) -> int {
+    if (dst && n) V3DBA_CUDA_TRY(cudaMemcpy(dst, src, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    return V3DBA_OK;
+  };
+  int rc;
+  if ((rc = get(o_orig, s.o_orig, K)) || (rc = get(c_ptr, s.c_ptr, N + 1)) || (rc = get(c_obs, s.c_obs, K)) ||
+      (rc = get(b_i, s.b_i, nb)) || (rc = get(b_l, s.b_l, nb)) || (rc = get(b_ptr, s.b_ptr, nb + 1)) ||
+      (rc = get(pr_k, s.pr_k, P)) || (rc = get(pr_m, s.pr_m, P)))
+    return rc;
+  return V3DBA_OK;
+}

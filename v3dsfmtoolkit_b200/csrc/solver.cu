@@ -6,6 +6,8 @@
 // accept / reject decision with the reference's exact tests.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -16,6 +18,7 @@
 #include "lm.cuh"
 #include "model.cuh"
 #include "precond.cuh"
+#include "structure.cuh"
 
 namespace v3dba {
 
@@ -229,107 +232,47 @@ int use_gnn(v3dba_handle h, bool learned) {
   return V3DBA_OK;
 }
 
-// Host-side structure analysis: point-major permutation, camera lists, camera-pair blocks with
-// their observation pairs (sorted by block, then by point), and the tile pattern of S.
-struct Structure {
-  std::vector<int> o_cam, o_pt, o_orig, p_ptr, c_ptr, c_obs;
-  std::vector<double> o_meas;
-  std::vector<int> b_i, b_l, b_ptr, pr_k, pr_m;
+// Phase timings of v3dba_create on stderr when V3DBA_TRACE_CREATE is set (diagnostics).
+struct CreateTrace {
+  bool on = std::getenv("V3DBA_TRACE_CREATE") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const char* phase, cudaStream_t st = nullptr) {
+    if (!on) return;
+    if (st) cudaStreamSynchronize(st);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "v3dba_create %-12s %8.3f ms\n", phase,
+                 std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
+
+// Work chunks over the camera observation lists and the camera-pair blocks: long lists are cut
+// into chunks of 64 observations / 128 pairs, one warp per chunk.
+struct Chunks {
   std::vector<int> cc_beg, cc_end, cam_cc_ptr, bc_beg, bc_end, blk_bc_ptr;
 };
 
 constexpr int kCamChunk = 64;     // observations per camera work chunk
 constexpr int kPairChunk = 128;   // observation pairs per camera-pair work chunk
 
-void build_chunks(Structure& S, int N) {
+void build_chunks(const std::vector<int>& c_ptr, const std::vector<int>& b_ptr, int N, Chunks& S) {
   S.cam_cc_ptr.assign(1, 0);
   for (int i = 0; i < N; ++i) {
-    for (int b = S.c_ptr[i]; b < S.c_ptr[i + 1]; b += kCamChunk) {
+    for (int b = c_ptr[i]; b < c_ptr[i + 1]; b += kCamChunk) {
       S.cc_beg.push_back(b);
-      S.cc_end.push_back(std::min(b + kCamChunk, S.c_ptr[i + 1]));
+      S.cc_end.push_back(std::min(b + kCamChunk, c_ptr[i + 1]));
     }
     S.cam_cc_ptr.push_back((int)S.cc_beg.size());
   }
-  const int nb = (int)S.b_i.size();
+  const int nb = (int)b_ptr.size() - 1;
   S.blk_bc_ptr.assign(1, 0);
   for (int b = 0; b < nb; ++b) {
-    for (int p = S.b_ptr[b]; p < S.b_ptr[b + 1]; p += kPairChunk) {
+    for (int p = b_ptr[b]; p < b_ptr[b + 1]; p += kPairChunk) {
       S.bc_beg.push_back(p);
-      S.bc_end.push_back(std::min(p + kPairChunk, S.b_ptr[b + 1]));
+      S.bc_end.push_back(std::min(p + kPairChunk, b_ptr[b + 1]));
     }
     S.blk_bc_ptr.push_back((int)S.bc_beg.size());
   }
-}
-
-void build_structure(const v3dba_problem* p, Structure& S) {
-  const int N = p->n_cameras, M = p->n_points, K = p->n_measurements;
-  // point-major permutation (stable: keeps the caller's order inside a track)
-  S.p_ptr.assign(M + 1, 0);
-  for (int k = 0; k < K; ++k) S.p_ptr[p->point[k] + 1]++;
-  for (int j = 0; j < M; ++j) S.p_ptr[j + 1] += S.p_ptr[j];
-  std::vector<int> fill(S.p_ptr.begin(), S.p_ptr.end() - 1);
-  S.o_orig.resize(K);
-  for (int k = 0; k < K; ++k) S.o_orig[fill[p->point[k]]++] = k;
-  S.o_cam.resize(K);
-  S.o_pt.resize(K);
-  S.o_meas.resize(2 * (size_t)K);
-  for (int k = 0; k < K; ++k) {
-    const int o = S.o_orig[k];
-    S.o_cam[k] = p->view[o];
-    S.o_pt[k] = p->point[o];
-    S.o_meas[2 * k] = p->measurements[2 * o];
-    S.o_meas[2 * k + 1] = p->measurements[2 * o + 1];
-  }
-  // camera lists over permuted observations
-  S.c_ptr.assign(N + 1, 0);
-  for (int k = 0; k < K; ++k) S.c_ptr[S.o_cam[k] + 1]++;
-  for (int i = 0; i < N; ++i) S.c_ptr[i + 1] += S.c_ptr[i];
-  S.c_obs.resize(K);
-  fill.assign(S.c_ptr.begin(), S.c_ptr.end() - 1);
-  for (int k = 0; k < K; ++k) S.c_obs[fill[S.o_cam[k]]++] = k;
-  // camera-pair blocks: for camera i, every observation k of i and every observation m of the
-  // same point seen by a camera l >= i gives the pair (k, m) of block (i, l)
-  std::vector<int> local(N, -1), touched;
-  std::vector<int> cnt;
-  std::vector<int> tk, tm, tl;
-  S.b_ptr.assign(1, 0);
-  for (int i = 0; i < N; ++i) {
-    tk.clear(); tm.clear(); tl.clear(); touched.clear();
-    for (int idx = S.c_ptr[i]; idx < S.c_ptr[i + 1]; ++idx) {
-      const int k = S.c_obs[idx];
-      const int j = S.o_pt[k];
-      for (int m = S.p_ptr[j]; m < S.p_ptr[j + 1]; ++m) {
-        const int l = S.o_cam[m];
-        if (l < i) continue;
-        if (local[l] < 0) { local[l] = 0; touched.push_back(l); }
-        tk.push_back(k); tm.push_back(m); tl.push_back(l);
-      }
-    }
-    // every camera gets its diagonal block, even without observations (it is then lambda I)
-    if (local[i] < 0) { local[i] = 0; touched.push_back(i); }
-    std::sort(touched.begin(), touched.end());
-    for (size_t t = 0; t < touched.size(); ++t) local[touched[t]] = (int)t;
-    cnt.assign(touched.size() + 1, 0);
-    for (int l : tl) cnt[local[l] + 1]++;
-    for (size_t t = 0; t < touched.size(); ++t) cnt[t + 1] += cnt[t];
-    const size_t base = S.pr_k.size();
-    S.pr_k.resize(base + tk.size());
-    S.pr_m.resize(base + tk.size());
-    std::vector<int> pos(cnt.begin(), cnt.end() - 1);
-    for (size_t t = 0; t < tk.size(); ++t) {
-      const int b = local[tl[t]];
-      S.pr_k[base + pos[b]] = tk[t];
-      S.pr_m[base + pos[b]] = tm[t];
-      pos[b]++;
-    }
-    for (size_t t = 0; t < touched.size(); ++t) {
-      S.b_i.push_back(i);
-      S.b_l.push_back(touched[t]);
-      S.b_ptr.push_back((int)(base + cnt[t + 1]));
-      local[touched[t]] = -1;
-    }
-  }
-  build_chunks(S, N);
 }
 
 }  // namespace
@@ -376,6 +319,7 @@ uint64_t v3dba_launch_count(void) { return g_launches.load(); }
 
 int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   if (!p || !out) return V3DBA_ERR_INVALID_ARGUMENT;
+  CreateTrace trace;
   *out = nullptr;
   int dA, dC;
   int rc = dims_of(p->model, p->mode, &dA, &dC);
@@ -398,6 +342,7 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
     return V3DBA_ERR_INVALID_INPUT;
   if (p->model == V3DBA_MODEL_COMMON && p->K[0] == 0.0) return V3DBA_ERR_INVALID_INPUT;
 
+  trace.mark("validate");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -432,22 +377,27 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   CTRY(cudaEventCreate(&h->ev1));
   CTRY(cudaMallocHost(&h->h_scalars, 16 * sizeof(double)));
 
-  Structure st;
-  build_structure(p, st);
-  TRY(upload(h, &s.o_cam, st.o_cam));
-  TRY(upload(h, &s.o_pt, st.o_pt));
-  TRY(upload(h, &s.o_orig, st.o_orig));
-  TRY(upload(h, &s.o_meas, st.o_meas));
-  TRY(upload(h, &s.p_ptr, st.p_ptr));
-  TRY(upload(h, &s.c_ptr, st.c_ptr));
-  TRY(upload(h, &s.c_obs, st.c_obs));
-  s.nb = (int)st.b_i.size();
-  s.P = (int64_t)st.pr_k.size();
-  TRY(upload(h, &s.b_i, st.b_i));
-  TRY(upload(h, &s.b_l, st.b_l));
-  TRY(upload(h, &s.b_ptr, st.b_ptr));
-  TRY(upload(h, &s.pr_k, st.pr_k));
-  TRY(upload(h, &s.pr_m, st.pr_m));
+  trace.mark("stream");
+  DeviceStructure ds;
+  const DevAlloc alloc = [h](void** q, size_t bytes) { return dalloc(h, reinterpret_cast<char**>(q), bytes); };
+  TRY(build_structure_device(p, alloc, h->stream, ds));
+  s.o_cam = ds.o_cam;
+  s.o_pt = ds.o_pt;
+  s.o_orig = ds.o_orig;
+  s.o_meas = ds.o_meas;
+  s.p_ptr = ds.p_ptr;
+  s.c_ptr = ds.c_ptr;
+  s.c_obs = ds.c_obs;
+  s.nb = (int)ds.h_b_i.size();
+  s.P = ds.P;
+  s.b_i = ds.b_i;
+  s.b_l = ds.b_l;
+  s.b_ptr = ds.b_ptr;
+  s.pr_k = ds.pr_k;
+  s.pr_m = ds.pr_m;
+  trace.mark("structure", h->stream);
+  Chunks st;
+  build_chunks(ds.h_c_ptr, ds.h_b_ptr, N, st);
   s.nch_cam = (int)st.cc_beg.size();
   s.nch_blk = (int)st.bc_beg.size();
   TRY(upload(h, &s.cc_beg, st.cc_beg));
@@ -459,6 +409,7 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   TRY(dalloc(h, &s.part_cc, (size_t)std::max(s.nch_cam, 1) * camera_chunk_values(dA, dC)));
   TRY(dalloc(h, &s.part_bc, (size_t)std::max(s.nch_blk, 1) * block_chunk_values(dA)));
 
+  trace.mark("chunks", h->stream);
   TRY(alloc_params(h, s.cur, N, M));
   TRY(alloc_params(h, s.trial, N, M));
   TRY(alloc_params(h, s.init, N, M));
@@ -490,9 +441,10 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   TRY(dalloc(h, &s.d_fail, 1));
   s.part_cap = partial_doubles(s);
   TRY(dalloc(h, &s.part, s.part_cap));
-  CTRY(cudaMemset(s.g_Z, 0, 64 * sizeof(double)));
-  CTRY(cudaMemset(s.g_gc, 0, 8 * sizeof(double)));
+  CTRY(cudaMemsetAsync(s.g_Z, 0, 64 * sizeof(double), h->stream));
+  CTRY(cudaMemsetAsync(s.g_gc, 0, 8 * sizeof(double), h->stream));
 
+  trace.mark("buffers", h->stream);
   // reduced system: n = N*dA + dC.  The dense tiles (Cholesky) or the block arrays (PCG) are
   // allocated on first use; here only the tile pattern is derived from the blocks and border.
   s.n = N * dA + dC;
@@ -504,20 +456,22 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
         for (int tcl = c0 / 64; tcl <= (c1 - 1) / 64; ++tcl)
           if (tr >= tcl) h->tile_nz[(size_t)tr * nt + tcl] = 1;
     };
-    for (int b = 0; b < s.nb; ++b) mark(st.b_l[b] * dA, st.b_l[b] * dA + dA, st.b_i[b] * dA, st.b_i[b] * dA + dA);
+    for (int b = 0; b < s.nb; ++b) mark(ds.h_b_l[b] * dA, ds.h_b_l[b] * dA + dA, ds.h_b_i[b] * dA, ds.h_b_i[b] * dA + dA);
     for (int i = 0; i < N; ++i) {
       mark(i * dA, i * dA + dA, i * dA, i * dA + dA);
       if (dC) mark(N * dA, N * dA + dC, i * dA, i * dA + dA);
     }
     if (dC) mark(N * dA, N * dA + dC, N * dA, N * dA + dC);
   }
-  h->blk_i = st.b_i;
-  h->blk_l = st.b_l;
+  h->blk_i = ds.h_b_i;
+  h->blk_l = ds.h_b_l;
 
+  trace.mark("pattern");
   TRY(upload_params(h, s.cur, p->K, p->R, p->T, p->dist, p->X));
   TRY(copy_params(s.init, s.cur, h, h->stream));
   TRY(copy_params(s.trial, s.cur, h, h->stream));
   CTRY(cudaStreamSynchronize(h->stream));
+  trace.mark("params");
 #undef TRY
 #undef CTRY
   *out = h;
