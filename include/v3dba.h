@@ -15,6 +15,10 @@
  *   v3dba_set_params /
  *   v3dba_get_params       <- the optimizer's in-place mutation of the caller's cameras, points,
  *                             K and distortion references (v3d_metricbundle.h:94-95, 232-233, 316)
+ *   v3dba_refine_consistent_rotations / v3dba_rotations_*
+ *                          <- V3D::refineConsistentRotations and its SparseRotationOptimizer
+ *                             (V3D/include/Geometry/v3d_mviewutilities.h:359-362,
+ *                              V3D/src/Geometry/v3d_mviewutilities.cpp:470-611)
  *   v3dba_minimize_batched <- the sequential loop of independent triplet / submodel adjustments
  *                             (SfM/generate_triples/src/generate_triples.cpp:403-415,
  *                              SfM/generate_submodels_L1/src/generate_submodels_L1.cpp:330-337)
@@ -350,6 +354,36 @@ int v3dba_measure_fp64_mma_peak(double* tflops);
  * (64^3 GEMM tiles of its panel and trailing tasks plus the diagonal factors; benchmark
  * support). */
 int v3dba_cholesky_flops(v3dba_handle h, double* flops);
+
+/* ---- Rotation averaging ----------------------------------------------------------------
+ * V3D::refineConsistentRotations (V3D/include/Geometry/v3d_mviewutilities.h:359-362): refines
+ * n_views absolute rotations from n_pairs relative rotations R_ij ~ R_j R_i^T by the
+ * SparseRotationOptimizer LM (V3D/src/Geometry/v3d_mviewutilities.cpp:470-582; residuals
+ * R_j - R_ij R_i, counted once per view of the pair; updates R_i <- R_i Rodrigues(delta_i);
+ * maxIterations 200).  relative_rotations: n_pairs*9, view_pairs: n_pairs*2 (first, second),
+ * rotations: n_views*9 (row-major; in/out).  opts may be NULL (reference defaults, 200
+ * iterations); of the options only tau, max_iterations, the two thresholds, verbosity and
+ * stop_cost apply.  result may be NULL; its cost fields are sum |R_j - R_ij R_i|^2_F over the
+ * 2*n_pairs measurements: initial_cost at the given rotations, cost at the last relinearisation
+ * (the last value the reference's verbose trace prints; at the accepted rotations when stop_cost
+ * ended the call). */
+int v3dba_refine_consistent_rotations(int n_views, int n_pairs, const double* relative_rotations,
+                                      const int32_t* view_pairs, double* rotations, const v3dba_options* opts,
+                                      v3dba_result* result);
+
+/* The same on a device-resident problem: create uploads the graph and builds the per-view
+ * measurement lists on the GPU; minimize runs the LM in one persistent launch (the _nu state
+ * carries over between calls, as on the reference object); get / set transfer the rotations;
+ * reset restores the rotations passed to create; cost evaluates sum |R_j - R_ij R_i|^2_F. */
+typedef struct v3dba_rotations_s* v3dba_rotations;
+int v3dba_rotations_create(int n_views, int n_pairs, const double* relative_rotations, const int32_t* view_pairs,
+                           const double* rotations, v3dba_rotations* out);
+int v3dba_rotations_destroy(v3dba_rotations h);
+int v3dba_rotations_minimize(v3dba_rotations h, const v3dba_options* opts, v3dba_result* result);
+int v3dba_rotations_get(v3dba_rotations h, double* rotations);
+int v3dba_rotations_set(v3dba_rotations h, const double* rotations);
+int v3dba_rotations_reset(v3dba_rotations h);
+int v3dba_rotations_cost(v3dba_rotations h, double* cost);
 
 /* Kernel launches issued by this library in the calling process so far. */
 uint64_t v3dba_launch_count(void);

@@ -70,6 +70,8 @@ class Reference:
         L.v3dref_linearize.argtypes = [C.c_int] * 5 + [C.c_double] + [_dp] * 5 + [_dp, _ip, _ip] + [_dp] * 5
         L.v3dref_cost.restype = C.c_double
         L.v3dref_cost.argtypes = [C.c_int] * 5 + [C.c_double] + [_dp] * 5 + [_dp, _ip, _ip]
+        L.v3dref_refine_rotations.restype = C.c_int
+        L.v3dref_refine_rotations.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, _dp, C.c_int, _ip]
 
     def _head(self, sc):
         return (sc.model, sc.mode, sc.n_cams, sc.n_points, sc.n_obs, float(sc.inlier_threshold))
@@ -113,6 +115,16 @@ class Reference:
         return self.lib.v3dref_cost(*self._head(scene), _d(_f64(K)), _d(_f64(R)), _d(_f64(T)),
                                     _d(_f64(dist)), _d(_f64(X)), _d(_f64(scene.meas)),
                                     _i(_i32(scene.view)), _i(_i32(scene.point)))
+
+
+    def refine_rotations(self, graph, rotations=None, trace_cap=512):
+        """V3D::refineConsistentRotations on a copy of the graph's initial rotations; returns
+        (rotations (n, 3, 3), err per relinearization as printed by the reference)."""
+        R = np.array(graph.R0 if rotations is None else rotations, dtype=np.float64, copy=True)
+        tr, tlen = np.zeros(trace_cap), C.c_int()
+        self.lib.v3dref_refine_rotations(graph.n_views, graph.n_pairs, _d(_f64(graph.rel)), _i(_i32(graph.pairs)),
+                                         _d(R), _d(tr), trace_cap, C.byref(tlen))
+        return R, tr[:min(tlen.value, trace_cap)].copy()
 
 
 class _OrcProblem(C.Structure):
@@ -159,6 +171,10 @@ class Restatement:
         L.orc_pcg.restype = C.c_int
         L.orc_pcg.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, C.c_int, _dp]
         L.orc_rodrigues.argtypes = [_dp, _dp]
+        L.orc_rotations_minimize.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, C.POINTER(_OrcOptions),
+                                             C.POINTER(_OrcResult), _dp, C.c_int]
+        L.orc_rotations_cost.restype = C.c_double
+        L.orc_rotations_cost.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp]
 
     @staticmethod
     def _problem(scene, nonvarying=(0, 0, 0)):
@@ -266,3 +282,23 @@ class Restatement:
         it = self.lib.orc_pcg(S.shape[0], bs, _d(_f64(S)), _d(_f64(b)),
                               _d(_f64(Minv)) if Minv is not None else None, rel_tol, max_iter, _d(x))
         return x, it
+
+    def rotations_minimize(self, graph, rotations=None, tau=1e-3, max_iterations=200, lambda0=1e-3,
+                           gradient_threshold=1e-10, update_threshold=1e-10, trace_cap=512):
+        """The restated SparseRotationOptimizer run; returns (rotations (n, 3, 3), info)."""
+        R = np.array(graph.R0 if rotations is None else rotations, dtype=np.float64, copy=True)
+        opt = _OrcOptions(tau, max_iterations, gradient_threshold, update_threshold, 0.0, 0.0, lambda0, 2.0)
+        res = _OrcResult()
+        te = np.zeros(trace_cap)
+        self.lib.orc_rotations_minimize(graph.n_views, graph.n_pairs, _d(_f64(graph.rel)), _i(_i32(graph.pairs)),
+                                        _d(R), C.byref(opt), C.byref(res), _d(te), trace_cap)
+        n = min(res.n_relinearizations, trace_cap)
+        info = dict(status=res.status, iterations=res.iterations, lambda_=opt.lambda_,
+                    n_relinearizations=res.n_relinearizations, n_rejected=res.n_rejected,
+                    final_err=res.final_err, trace_cost=te[:n].copy())
+        return R, info
+
+    def rotations_cost(self, graph, rotations):
+        return self.lib.orc_rotations_cost(graph.n_views, graph.n_pairs, _d(_f64(graph.rel)),
+                                           _i(_i32(graph.pairs)), _d(_f64(rotations)))
+

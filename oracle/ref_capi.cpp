@@ -7,7 +7,9 @@
 //   * V3D::StdMetricBundleOptimizer             (V3D/include/Geometry/v3d_metricbundle.h:107-136)
 //   * V3D::CommonInternalsMetricBundleOptimizer (V3D/include/Geometry/v3d_metricbundle.h:150-238)
 //   * V3D::VaryingInternalsMetricBundleOptimizer(V3D/include/Geometry/v3d_metricbundle.h:242-320)
-// all running V3D::SparseLevenbergOptimizer::minimize (V3D/src/Math/v3d_optimization.cpp:719-1250).
+// all running V3D::SparseLevenbergOptimizer::minimize (V3D/src/Math/v3d_optimization.cpp:719-1250),
+// and the rotation averaging V3D::refineConsistentRotations (V3D/src/Geometry/
+// v3d_mviewutilities.cpp:470-613), which runs the same minimize() on SparseRotationOptimizer.
 //
 // Parameter layout (row-major, doubles), shared with the product C-ABI:
 //   K    : model 0/2 -> nCams*9 per-camera intrinsics; model 1 -> 9 (the shared K)
@@ -16,9 +18,13 @@
 //   meas : nObs*2,  view/point : nObs (0-based)
 
 #include "Geometry/v3d_metricbundle.h"
+#include "Geometry/v3d_mviewutilities.h"
 
 #include <cmath>
 #include <cstring>
+#include <iostream>
+#include <sstream>
+#include <string>
 #include <vector>
 
 using namespace V3D;
@@ -290,6 +296,54 @@ double v3dref_cost(int model, int mode, int nCams, int nPoints, int nObs, double
    for (int k = 0; k < nObs; ++k)
       err += w[k] * w[k] * (e[2 * k] * e[2 * k] + e[2 * k + 1] * e[2 * k + 1]);
    return err;
+}
+
+// V3D::refineConsistentRotations on nViews row-major 3x3 rotations (updated in place), nPairs
+// relative rotations and view pairs (2 ints each).  The function sets optimizerVerbosenessLevel
+// to 1, so minimize() prints "|residual|^2 = <err>" once per relinearization
+// (v3d_optimization.cpp:791); std::cout is redirected to a buffer at full precision for the
+// call and those values are returned as the cost trace (traceErr[0..*traceLen), up to traceCap).
+int v3dref_refine_rotations(int nViews, int nPairs, double const* relR, int const* pairs, double* R,
+                            double* traceErr, int traceCap, int* traceLen)
+{
+   std::vector<Matrix3x3d> rel(nPairs), rots(nViews);
+   std::vector<std::pair<int, int> > vp(nPairs);
+   for (int k = 0; k < nPairs; ++k)
+   {
+      for (int r = 0; r < 3; ++r)
+         for (int c = 0; c < 3; ++c) rel[k][r][c] = relR[9 * k + 3 * r + c];
+      vp[k] = std::make_pair(pairs[2 * k], pairs[2 * k + 1]);
+   }
+   for (int i = 0; i < nViews; ++i)
+      for (int r = 0; r < 3; ++r)
+         for (int c = 0; c < 3; ++c) rots[i][r][c] = R[9 * i + 3 * r + c];
+
+   std::ostringstream captured;
+   captured.precision(17);
+   std::streambuf* saved = std::cout.rdbuf(captured.rdbuf());
+   std::streamsize savedPrec = std::cout.precision(17);
+   refineConsistentRotations(nViews, rel, vp, rots);
+   std::cout.precision(savedPrec);
+   std::cout.rdbuf(saved);
+   V3D::optimizerVerbosenessLevel = 0;
+
+   for (int i = 0; i < nViews; ++i)
+      for (int r = 0; r < 3; ++r)
+         for (int c = 0; c < 3; ++c) R[9 * i + 3 * r + c] = rots[i][r][c];
+
+   int len = 0;
+   std::istringstream lines(captured.str());
+   std::string line;
+   std::string const tag = "|residual|^2 = ";
+   while (std::getline(lines, line))
+   {
+      size_t const at = line.find(tag);
+      if (at == std::string::npos) continue;
+      if (len < traceCap && traceErr) traceErr[len] = std::strtod(line.c_str() + at + tag.size(), 0);
+      ++len;
+   }
+   if (traceLen) *traceLen = len;
+   return 0;
 }
 
 } // extern "C"

@@ -769,3 +769,165 @@ done:
   if (Mi) free(Mi);
   return it;
 }
+
+/* ---- Rotation averaging (SparseRotationOptimizer, v3d_mviewutilities.cpp:470-582) ---------- */
+
+/* e = R_j - R_ij R_i (evalResidual, v3d_mviewutilities.cpp:486-508). */
+static void rot_residual(const double* Ri, const double* Rj, const double* Rij, double* e)
+{
+  double P[9];
+  matmul(Rij, Ri, P, 3, 3, 3);
+  for (int t = 0; t < 9; ++t) e[t] = Rj[t] - P[t];
+}
+
+/* 9x3 Jacobian of vec(A (I + [w]x)) at w = 0 (fillJacobians, :510-553): A = -R_ij R_i for the
+ * first view of the pair, R_j for the second. */
+static void rot_jacobian(const double* A, double* J)
+{
+  for (int r = 0; r < 3; ++r) {
+    const double* a = A + 3 * r;
+    double* j0 = J + 9 * r;          /* rows 3r, 3r+1, 3r+2 of the 9x3 matrix */
+    j0[0] = 0.0;   j0[1] = -a[2]; j0[2] = a[1];
+    j0[3] = a[2];  j0[4] = 0.0;   j0[5] = -a[0];
+    j0[6] = -a[1]; j0[7] = a[0];  j0[8] = 0.0;
+  }
+}
+
+double orc_rotations_cost(int n_views, int n_pairs, const double* rel, const int* pairs, const double* R)
+{
+  (void)n_views;
+  double err = 0.0, e[9];
+  for (int k = 0; k < 2 * n_pairs; ++k) {
+    int q = k < n_pairs ? k : k - n_pairs;
+    rot_residual(R + 9 * pairs[2 * q], R + 9 * pairs[2 * q + 1], rel + 9 * q, e);
+    for (int t = 0; t < 9; ++t) err += e[t] * e[t];
+  }
+  return err;
+}
+
+/* Solve (U + lambda I) d = g for one 3x3 block by the up-looking LDL^T of LDL_numeric /
+ * LDL_lsolve / LDL_dsolve / LDL_ltsolve (v3d_optimization.cpp:102-230) in natural order.
+ * Returns 1 when a pivot D(k,k) is exactly zero (the reference then rejects the step). */
+static int rot_ldl_solve(const double* U, double lambda, const double* g, double* d)
+{
+  double a00 = U[0] + lambda, a11 = U[4] + lambda, a22 = U[8] + lambda;
+  double a01 = U[1], a02 = U[2], a12 = U[5];
+  double D0 = a00;
+  if (D0 == 0.0) return 1;
+  double L10 = a01 / D0;
+  double D1 = a11 - L10 * a01;
+  if (D1 == 0.0) return 1;
+  double y1 = a12 - L10 * a02;          /* Y[1] -= L10 * y0 while processing column 0 of row 2 */
+  double L20 = a02 / D0;
+  double D2 = a22 - L20 * a02;
+  double L21 = y1 / D1;
+  D2 -= L21 * y1;
+  if (D2 == 0.0) return 1;
+  double x0 = g[0], x1 = g[1], x2 = g[2];
+  x1 -= L10 * x0; x2 -= L20 * x0; x2 -= L21 * x1;
+  x0 /= D0; x1 /= D1; x2 /= D2;
+  x1 -= L21 * x2; x0 -= L10 * x1; x0 -= L20 * x2;
+  d[0] = x0; d[1] = x1; d[2] = x2;
+  return 0;
+}
+
+int orc_rotations_minimize(int n_views, int n_pairs, const double* rel, const int* pairs, double* R,
+                           orc_options* opt, orc_result* res, double* trace_err, int trace_cap)
+{
+  int N = n_views, P = n_pairs, K = 2 * n_pairs;
+  memset(res, 0, sizeof(*res));
+  res->status = ORC_TIMEOUT;
+  if (N <= 0) { res->status = ORC_CONVERGED; return 0; }
+  double *U = calloc((size_t)9 * N, sizeof(double)), *g = calloc((size_t)3 * N, sizeof(double));
+  double *d = calloc((size_t)3 * N, sizeof(double)), *Rs = malloc(sizeof(double) * 9 * N);
+  double plen = sqrt(3.0 * N);
+  int compute_derivatives = 1, it;
+  double err = 0.0, lambda = opt->lambda;
+  for (it = 0; it < opt->max_iterations; ++it) {
+    if (compute_derivatives) {
+      memset(U, 0, sizeof(double) * 9 * N);
+      memset(g, 0, sizeof(double) * 3 * N);
+      err = 0.0;
+      double e[9], J[27], A[9];
+      for (int k = 0; k < K; ++k) {
+        int q = k < P ? k : k - P;
+        const double *Ri = R + 9 * pairs[2 * q], *Rj = R + 9 * pairs[2 * q + 1], *Rij = rel + 9 * q;
+        rot_residual(Ri, Rj, Rij, e);
+        for (int t = 0; t < 9; ++t) err += e[t] * e[t];
+      }
+      for (int k = 0; k < K; ++k) {
+        int q = k < P ? k : k - P;
+        int view = k < P ? pairs[2 * q] : pairs[2 * q + 1];
+        const double *Ri = R + 9 * pairs[2 * q], *Rj = R + 9 * pairs[2 * q + 1], *Rij = rel + 9 * q;
+        rot_residual(Ri, Rj, Rij, e);
+        if (k < P) { matmul(Rij, Ri, A, 3, 3, 3); for (int t = 0; t < 9; ++t) A[t] = -A[t]; }
+        else memcpy(A, Rj, sizeof(A));
+        rot_jacobian(A, J);
+        double* Uv = U + 9 * (size_t)view;
+        double* gv = g + 3 * (size_t)view;
+        for (int a = 0; a < 3; ++a) {
+          double s = 0.0;
+          for (int r = 0; r < 9; ++r) s += J[3 * r + a] * -e[r];
+          gv[a] += s;
+          for (int b = 0; b < 3; ++b) {
+            double u = 0.0;
+            for (int r = 0; r < 9; ++r) u += J[3 * r + a] * J[3 * r + b];
+            Uv[3 * a + b] += u;
+          }
+        }
+      }
+      res->n_relinearizations++;
+      res->final_err = err;
+      if (trace_cap > 0 && res->n_relinearizations <= trace_cap) trace_err[res->n_relinearizations - 1] = err;
+      double gmax = 0.0;
+      for (int t = 0; t < 3 * N; ++t) gmax = fmax(gmax, fabs(g[t]));
+      if (gmax < opt->gradient_threshold) { res->status = ORC_CONVERGED; break; }
+      if (it == 0) {
+        double m = -1e30;
+        for (int i = 0; i < N; ++i)
+          for (int l = 0; l < 3; ++l) m = fmax(m, U[9 * (size_t)i + 4 * l]);
+        lambda = opt->tau * m;
+      }
+    }
+    int success = 1;
+    for (int i = 0; i < N && success; ++i)
+      if (rot_ldl_solve(U + 9 * (size_t)i, lambda, g + 3 * (size_t)i, d + 3 * (size_t)i)) success = 0;
+    double rho = 0.0;
+    if (success) {
+      double d2 = 0.0, dg = 0.0;
+      for (int t = 0; t < 3 * N; ++t) d2 += d[t] * d[t];
+      if (sqrt(d2) < opt->update_threshold * (plen + opt->update_threshold)) {
+        res->status = ORC_SMALL_UPDATE;
+        break;
+      }
+      memcpy(Rs, R, sizeof(double) * 9 * N);
+      for (int i = 0; i < N; ++i) {
+        double dR[9];
+        orc_rodrigues(d + 3 * i, dR);
+        matmul(Rs + 9 * i, dR, R + 9 * i, 3, 3, 3);
+      }
+      double new_err = orc_rotations_cost(N, P, rel, pairs, R);
+      for (int t = 0; t < 3 * N; ++t) dg += d[t] * g[t];
+      rho = (err - new_err) / (lambda * d2 + dg);
+    }
+    if (success && rho > 0.0) {
+      double r = 2.0 * rho - 1.0;
+      double f = 1.0 - r * r * r;
+      lambda *= (f > 1.0 / 3.0 ? f : 1.0 / 3.0);
+      if (lambda < 1e-10) lambda = 1e-10;
+      opt->nu = 2.0;
+      compute_derivatives = 1;
+    } else {
+      if (success) memcpy(R, Rs, sizeof(double) * 9 * N);
+      res->n_rejected++;
+      lambda *= opt->nu;
+      opt->nu *= 2.0;
+      compute_derivatives = 0;
+    }
+  }
+  res->iterations = it;
+  opt->lambda = lambda;
+  free(U); free(g); free(d); free(Rs);
+  return 0;
+}
+

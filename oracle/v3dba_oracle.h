@@ -113,6 +113,20 @@ int orc_minimize(const orc_problem* p, orc_params* x, orc_options* opt, orc_resu
 int orc_pcg(int n, int bs, const double* S, const double* b, const double* Minv, double rel_tol,
             int max_iter, double* x);
 
+/* ---- Rotation averaging ---------------------------------------------------------------
+ * SparseRotationOptimizer (V3D/src/Geometry/v3d_mviewutilities.cpp:470-582) minimised by the LM
+ * loop above, as refineConsistentRotations (:589-611) runs it: 2*n_pairs 9-D residuals
+ * e_k = R_j - R_ij R_i of pair k' = k mod n_pairs (i = pairs[2k'], j = pairs[2k'+1]); measurement
+ * k < n_pairs is attached to view i with Jacobian d/domega_i of -R_ij R_i (I + [omega_i]x), the
+ * second copy to view j with d/domega_j of R_j (I + [omega_j]x); no point parameters (dimension 0),
+ * so the damped normal matrix is block diagonal (3x3 per view) and each block is factored by the
+ * reference's sparse LDL^T in natural order.  Update R_i <- R_i Rodrigues(delta_i); |p| = sqrt(3 n).
+ * rel: n_pairs*9, pairs: n_pairs*2, R: n_views*9 (in/out).  opt->max_iterations is used as given
+ * (the reference sets 200).  The optional trace receives err per relinearization. */
+int orc_rotations_minimize(int n_views, int n_pairs, const double* rel, const int* pairs, double* R,
+                           orc_options* opt, orc_result* res, double* trace_err, int trace_cap);
+/* sum over the 2*n_pairs measurements of |R_j - R_ij R_i|^2_F. */
+double orc_rotations_cost(int n_views, int n_pairs, const double* rel, const int* pairs, const double* R);
 #ifdef __cplusplus
 }
 #endif

@@ -35,3 +35,18 @@ def param_rel(pa, pb):
             continue
         out = max(out, rel(a, b))
     return out
+
+
+ROT_GOLDEN = os.path.join(GOLDEN, "rotations")
+
+
+def rotation_golden_names():
+    return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(ROT_GOLDEN, "*.npz")))
+
+
+def load_rotation_golden(name):
+    """(RotationGraph, fixture) of a rotation-averaging fixture."""
+    g = np.load(os.path.join(ROT_GOLDEN, name + ".npz"))
+    graph = scenes.RotationGraph(g["rel"].copy(), g["pairs"].copy(), g["R0"].copy(), g["R"].copy(), name=name)
+    return graph, g
+

@@ -39,7 +39,9 @@ EXPORTS = (
     "v3dba_set_precond_model", "v3dba_precond_set_create", "v3dba_precond_set_destroy", "v3dba_precond_set_count",
     "v3dba_precond_set_add_blocks", "v3dba_precond_set_capture", "v3dba_precond_set_info",
     "v3dba_precond_set_features", "v3dba_precond_loss_grad", "v3dba_precond_coefficients", "v3dba_precond_train",
-    "v3dba_precond_pcg_iterations", "v3dba_structure",
+    "v3dba_precond_pcg_iterations", "v3dba_structure", "v3dba_refine_consistent_rotations",
+    "v3dba_rotations_create", "v3dba_rotations_destroy", "v3dba_rotations_minimize", "v3dba_rotations_get",
+    "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -132,6 +134,15 @@ def _lib():
         L.v3dba_precond_train.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_uint32, _dp]
         L.v3dba_precond_pcg_iterations.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_uint32,
                                                    C.POINTER(C.c_int), _dp]
+        L.v3dba_refine_consistent_rotations.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, C.POINTER(Options),
+                                                        C.POINTER(Result)]
+        L.v3dba_rotations_create.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, C.POINTER(C.c_void_p)]
+        L.v3dba_rotations_destroy.argtypes = [C.c_void_p]
+        L.v3dba_rotations_minimize.argtypes = [C.c_void_p, C.POINTER(Options), C.POINTER(Result)]
+        L.v3dba_rotations_get.argtypes = [C.c_void_p, _dp]
+        L.v3dba_rotations_set.argtypes = [C.c_void_p, _dp]
+        L.v3dba_rotations_reset.argtypes = [C.c_void_p]
+        L.v3dba_rotations_cost.argtypes = [C.c_void_p, _dp]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -299,6 +310,81 @@ def dense_cholesky_solve(S, rhs):
     check(_lib().v3dba_dense_cholesky_solve(S.shape[0], _d(S), _d(rhs), _d(x), C.byref(fail)),
           "v3dba_dense_cholesky_solve")
     return x, bool(fail.value)
+
+
+def rotation_options(**kw) -> Options:
+    """Reference defaults with SparseRotationOptimizer's maxIterations = 200."""
+    o = default_options(max_iterations=200)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def refine_consistent_rotations(relative_rotations, view_pairs, rotations, options: Options | None = None, **kw):
+    """V3D::refineConsistentRotations through the C-ABI: returns (refined rotations (n, 3, 3),
+    Result).  ``rotations`` is not modified."""
+    rel = _f64(relative_rotations).reshape(-1, 9)
+    pairs = np.ascontiguousarray(view_pairs, dtype=np.int32).reshape(-1, 2)
+    R = np.array(rotations, dtype=np.float64, copy=True).reshape(-1, 3, 3)
+    o = options if options is not None else rotation_options(**kw)
+    r = Result()
+    check(_lib().v3dba_refine_consistent_rotations(R.shape[0], pairs.shape[0], _d(rel), pairs.ctypes.data_as(_ip),
+                                                   _d(R), C.byref(o), C.byref(r)), "v3dba_refine_consistent_rotations")
+    return R, r
+
+
+class Rotations:
+    """A rotation-averaging problem resident on the GPU (wraps v3dba_rotations_*)."""
+
+    def __init__(self, relative_rotations, view_pairs, rotations):
+        self._rel = _f64(relative_rotations).reshape(-1, 9)
+        self._pairs = np.ascontiguousarray(view_pairs, dtype=np.int32).reshape(-1, 2)
+        R0 = _f64(rotations).reshape(-1, 9)
+        self.n_views, self.n_pairs = R0.shape[0], self._pairs.shape[0]
+        h = C.c_void_p()
+        check(_lib().v3dba_rotations_create(self.n_views, self.n_pairs, _d(self._rel), self._pairs.ctypes.data_as(_ip),
+                                            _d(R0), C.byref(h)), "v3dba_rotations_create")
+        self.h = h
+
+    @classmethod
+    def from_graph(cls, graph):
+        return cls(graph.rel, graph.pairs, graph.R0)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            _lib().v3dba_rotations_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def minimize(self, options: Options | None = None, **kw) -> Result:
+        o = options if options is not None else rotation_options(**kw)
+        if options is not None:
+            for k, v in kw.items():
+                setattr(o, k, v)
+        r = Result()
+        check(_lib().v3dba_rotations_minimize(self.h, C.byref(o), C.byref(r)), "v3dba_rotations_minimize")
+        return r
+
+    def get(self):
+        R = np.zeros((self.n_views, 3, 3))
+        check(_lib().v3dba_rotations_get(self.h, _d(R)), "v3dba_rotations_get")
+        return R
+
+    def set(self, rotations):
+        check(_lib().v3dba_rotations_set(self.h, _d(_f64(rotations))), "v3dba_rotations_set")
+
+    def reset(self):
+        check(_lib().v3dba_rotations_reset(self.h), "v3dba_rotations_reset")
+
+    def cost(self) -> float:
+        c = C.c_double()
+        check(_lib().v3dba_rotations_cost(self.h, C.byref(c)), "v3dba_rotations_cost")
+        return c.value
 
 
 class Batch:

@@ -454,4 +454,28 @@ int build_structure_device(const v3dba_problem* p, const DevAlloc& alloc, cudaSt
   return V3DBA_OK;
 }
 
+int group_by_key_device(const int* keys, int n, int nv, int* perm, int* ptr, cudaStream_t st) {
+  if (n < 0 || nv < 0) return V3DBA_ERR_INVALID_ARGUMENT;
+  Scratch sc;
+  sc.st = st;
+  int rc;
+  uint32_t *ka, *kb;
+  int *va, *vb;
+  if ((rc = sc.get(&ka, n)) || (rc = sc.get(&kb, n)) || (rc = sc.get(&va, n)) || (rc = sc.get(&vb, n))) return rc;
+  const int g = cdiv(std::max(n, 1), 256);
+  if (n > 0) {
+    k_int_to_key<<<g, 256, 0, st>>>(keys, ka, n);
+    V3DBA_LAUNCH_CHECK();
+    k_iota<<<g, 256, 0, st>>>(va, n);
+    V3DBA_LAUNCH_CHECK();
+  }
+  uint32_t* k = ka;
+  int* v = va;
+  if ((rc = radix_sort(sc, &k, &v, kb, vb, n, bits_for((uint64_t)std::max(nv - 1, 0)), st))) return rc;
+  if (n > 0) V3DBA_CUDA_TRY(cudaMemcpyAsync(perm, v, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+  k_key_bounds<<<cdiv((long)n + 1, 256), 256, 0, st>>>(k, n, nv, ptr);
+  V3DBA_LAUNCH_CHECK();
+  return V3DBA_OK;
+}
+
 }  // namespace v3dba

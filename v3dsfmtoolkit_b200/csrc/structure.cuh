@@ -34,4 +34,9 @@ struct DeviceStructure {
 // Builds the structure of `p` (validated indices) on the device, on stream `st`.
 int build_structure_device(const v3dba_problem* p, const DevAlloc& alloc, cudaStream_t st, DeviceStructure& S);
 
+// Stable grouping of n items by device int keys in [0, nv): perm[t] is the t-th item in key
+// order (input order among equal keys), items ptr[v] .. ptr[v+1]-1 of perm have key v.  perm
+// ([n]) and ptr ([nv+1]) are caller-owned device buffers; the scratch is stream-ordered.
+int group_by_key_device(const int* keys, int n, int nv, int* perm, int* ptr, cudaStream_t st);
+
 }  // namespace v3dba

@@ -12,6 +12,7 @@ Workloads:
                                50,000 points, tracks of 3-12 consecutive views, 2% outliers
   * :func:`triplet_batch`   -- thousands of independent 3-camera problems of uneven size
   * :func:`cluster_scene`   -- 2,000 cameras in 20 groups, 1M points, ~6M observations
+  * :func:`rotation_graph`  -- view graphs for rotation averaging (refineConsistentRotations)
 """
 from __future__ import annotations
 
@@ -383,3 +384,63 @@ def varying_scene(n_cams=12, n_points=800, seed=0, mode=FULL_BUNDLE_RADIAL_TANGE
     dist = np.zeros((N, 4))
     return Scene(MODEL_VARYING, mode, 1.0, K, sc.R, sc.T, sc.X, sc.meas, sc.view, sc.point, dist,
                  name=f"varying{N}x{sc.n_points}")
+
+
+@dataclasses.dataclass
+class RotationGraph:
+    """Input of refineConsistentRotations: relative rotations R_ij ~ R_j R_i^T of view pairs
+    (i, j) and initial absolute rotations.  ``rel`` (n_pairs, 3, 3), ``pairs`` (n_pairs, 2) int32,
+    ``R0`` (n_views, 3, 3), ``R_true`` (n_views, 3, 3) the noise-free rotations."""
+    rel: np.ndarray
+    pairs: np.ndarray
+    R0: np.ndarray
+    R_true: np.ndarray
+    name: str = "rotations"
+
+    @property
+    def n_views(self) -> int:
+        return int(self.R0.shape[0])
+
+    @property
+    def n_pairs(self) -> int:
+        return int(self.pairs.shape[0])
+
+
+def rotation_graph(n_views=2000, n_pairs=40000, window=5, noise_deg=1.0, init_deg=5.0, outlier_frac=0.0,
+                   seed=0) -> RotationGraph:
+    """A view graph as an SfM pipeline produces it: every view paired with its ``window`` next
+    views along the capture order, the remaining pairs drawn uniformly among all views (loop
+    closures), in random order.  Relative rotations carry ``noise_deg`` of rotation noise (a
+    fraction ``outlier_frac`` of them are random rotations); the initial rotations are the true
+    ones perturbed by ``init_deg``."""
+    rng = np.random.default_rng(seed)
+    ax = random_unit(rng, n_views)
+    R_true = rodrigues(ax * rng.uniform(0.0, math.pi, size=(n_views, 1)))
+    seq = [(i, i + d) for d in range(1, window + 1) for i in range(n_views - d)]
+    have = set(seq)
+    pairs = list(seq[:n_pairs])
+    while len(pairs) < n_pairs and len(have) < n_views * (n_views - 1) // 2:
+        i, j = (int(v) for v in rng.integers(0, n_views, size=2))
+        if i == j:
+            continue
+        i, j = min(i, j), max(i, j)
+        if (i, j) in have:
+            continue
+        have.add((i, j))
+        pairs.append((i, j))
+    pairs = np.array(pairs, dtype=np.int32).reshape(-1, 2)
+    pairs = pairs[rng.permutation(len(pairs))]
+    flip = rng.random(len(pairs)) < 0.5     # either orientation of a pair
+    pairs[flip] = pairs[flip][:, ::-1]
+    i, j = pairs[:, 0], pairs[:, 1]
+    rel = R_true[j] @ np.transpose(R_true[i], (0, 2, 1))
+    noise = rodrigues(rng.normal(scale=math.radians(noise_deg), size=(len(pairs), 3)))
+    rel = noise @ rel
+    n_out = int(round(outlier_frac * len(pairs)))
+    if n_out:
+        sel = rng.choice(len(pairs), size=n_out, replace=False)
+        rel[sel] = rodrigues(random_unit(rng, n_out) * rng.uniform(0.0, math.pi, size=(n_out, 1)))
+    R0 = R_true @ rodrigues(rng.normal(scale=math.radians(init_deg), size=(n_views, 3)))
+    return RotationGraph(np.ascontiguousarray(rel), np.ascontiguousarray(pairs), np.ascontiguousarray(R0),
+                         R_true, name=f"rotations{n_views}x{len(pairs)}")
+
