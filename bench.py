@@ -670,6 +670,7 @@ def run_rotations(args, rank, world, local_rank):
     dist = distributed.init("nccl")
     g = rotation_workload()
     h = capi.Rotations.from_graph(g)
+    group = h.autotune()
     flush = torch.empty(int(256 * 2 ** 20), dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
         h.reset()
@@ -728,6 +729,7 @@ def run_rotations(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": "rotations10000", "n_views": g.n_views, "n_pairs": g.n_pairs,
                    "lm_iterations_per_step": last.iterations, "status": last.status, "final_cost": last.cost,
+                   "lanes_per_view": group,
                    "l2": "flushed (256 MiB write) before every step; the graph (15 MB) stays L2-resident inside a step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "gpu_launches": int(launches), "clocks": clk,

@@ -384,6 +384,11 @@ int v3dba_rotations_get(v3dba_rotations h, double* rotations);
 int v3dba_rotations_set(v3dba_rotations h, const double* rotations);
 int v3dba_rotations_reset(v3dba_rotations h);
 int v3dba_rotations_cost(v3dba_rotations h, double* cost);
+/* Lanes per view (4, 8, 16 or 32) of the linearisation sweep: create picks one from the graph's
+ * mean measurements per view; autotune times the sweep with each and keeps the fastest (the
+ * rotations are not changed); set_group fixes it.  Results do not depend on it beyond rounding. */
+int v3dba_rotations_set_group(v3dba_rotations h, int group);
+int v3dba_rotations_autotune(v3dba_rotations h, int* group);
 
 /* Kernel launches issued by this library in the calling process so far. */
 uint64_t v3dba_launch_count(void);

@@ -95,3 +95,26 @@ def test_empty_problems():
     R0 = scenes.rotation_graph(n_views=5, n_pairs=4, seed=2).R0
     R, r = capi.refine_consistent_rotations(np.zeros((0, 3, 3)), np.zeros((0, 2), np.int32), R0)
     assert r.status == capi.STATUS_CONVERGED and np.array_equal(R, R0)
+
+
+def test_group_sizes_agree_and_autotune_picks_one():
+    graph = scenes.rotation_graph(n_views=800, n_pairs=12000, seed=12)
+    h = capi.Rotations.from_graph(graph)
+    out = []
+    for G in (4, 8, 16, 32):
+        h.set_group(G)
+        h.reset()
+        r = h.minimize()
+        out.append((r, h.get()))
+    r0, R0 = out[0]
+    for r, R in out[1:]:
+        assert r.status == r0.status
+        assert abs(r.cost - r0.cost) <= 1e-9 * r0.cost
+        assert np.abs(R - R0).max() < 1e-8
+    h.reset()
+    c = h.cost()
+    assert h.autotune() in (4, 8, 16, 32)
+    assert h.cost() == pytest.approx(c, rel=1e-12)
+    with pytest.raises(capi.V3dbaError):
+        h.set_group(3)
+

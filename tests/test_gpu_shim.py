@@ -11,12 +11,13 @@ import numpy as np
 import pytest
 
 from v3dsfmtoolkit_b200 import capi
-from tests.helpers import golden_names, load_golden, param_rel
+from tests.helpers import golden_names, load_golden, load_rotation_golden, param_rel, rotation_golden_names
 
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DEMO = os.path.join(ROOT, "tests", "shim", "_build", "shim_demo")
+ROT_DEMO = os.path.join(ROOT, "tests", "shim", "_build", "rotations_demo")
 
 
 def _write_scene(path, sc, max_iterations, precision, nv):
@@ -65,3 +66,25 @@ def test_dropin_header_matches_reference(name):
     assert param_rel((K, R, T, X), (g["K"], g["R"], g["T"], g["X"])) < 1e-5
     if sc.dist is not None:
         assert param_rel((dist,), (g["dist"],)) < 1e-4 or np.abs(dist - g["dist"]).max() < 1e-9
+
+
+@pytest.mark.skipif(not os.path.exists(ROT_DEMO), reason="rotation demo not built (needs the reference headers at build time)")
+@pytest.mark.parametrize("name", rotation_golden_names())
+def test_rotation_header_matches_reference(name):
+    """V3D::B200::refineConsistentRotations called on the reference's own container types gives
+    the reference's refined rotations (golden fixtures)."""
+    graph, g = load_rotation_golden(name)
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "graph.bin"), os.path.join(d, "out.bin")
+        with open(sp, "wb") as f:
+            f.write(struct.pack("<2i", graph.n_views, graph.n_pairs))
+            f.write(np.ascontiguousarray(graph.rel, dtype=np.float64).tobytes())
+            f.write(np.ascontiguousarray(graph.pairs, dtype=np.int32).tobytes())
+            f.write(np.ascontiguousarray(graph.R0, dtype=np.float64).tobytes())
+        r = subprocess.run([ROT_DEMO, sp, op], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        b = open(op, "rb").read()
+    assert struct.unpack_from("<i", b, 0)[0] == capi.OK
+    R = np.frombuffer(b, dtype=np.float64, offset=4).reshape(-1, 3, 3)
+    assert np.abs(R - g["R"]).max() < 1e-5
+

@@ -41,7 +41,8 @@ EXPORTS = (
     "v3dba_precond_set_features", "v3dba_precond_loss_grad", "v3dba_precond_coefficients", "v3dba_precond_train",
     "v3dba_precond_pcg_iterations", "v3dba_structure", "v3dba_refine_consistent_rotations",
     "v3dba_rotations_create", "v3dba_rotations_destroy", "v3dba_rotations_minimize", "v3dba_rotations_get",
-    "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost",
+    "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost", "v3dba_rotations_set_group",
+    "v3dba_rotations_autotune",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -143,6 +144,8 @@ def _lib():
         L.v3dba_rotations_set.argtypes = [C.c_void_p, _dp]
         L.v3dba_rotations_reset.argtypes = [C.c_void_p]
         L.v3dba_rotations_cost.argtypes = [C.c_void_p, _dp]
+        L.v3dba_rotations_set_group.argtypes = [C.c_void_p, C.c_int]
+        L.v3dba_rotations_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -385,6 +388,14 @@ class Rotations:
         c = C.c_double()
         check(_lib().v3dba_rotations_cost(self.h, C.byref(c)), "v3dba_rotations_cost")
         return c.value
+
+    def set_group(self, group: int):
+        check(_lib().v3dba_rotations_set_group(self.h, group), "v3dba_rotations_set_group")
+
+    def autotune(self) -> int:
+        g = C.c_int()
+        check(_lib().v3dba_rotations_autotune(self.h, C.byref(g)), "v3dba_rotations_autotune")
+        return g.value
 
 
 class Batch:

@@ -12,6 +12,13 @@ namespace v3dba {
 // Counts every kernel launch issued by this library (reported by v3dba_launch_count()).
 void note_launches(uint64_t n);
 
+// True when no value is Inf or NaN (host; branch-free so the scan vectorises).
+bool all_finite(const double* p, size_t n);
+
+// Raises the release threshold of the current device's stream-ordered pool once, so memory
+// freed by one handle is kept for the next (handles are created and destroyed in loops).
+int ensure_pool();
+
 #define V3DBA_CUDA_TRY(expr)                                                        \
   do {                                                                              \
     cudaError_t _e = (expr);                                                        \

@@ -67,52 +67,72 @@ __device__ __forceinline__ void load9(const double* __restrict__ p, double (&m)[
   for (int t = 0; t < 9; ++t) m[t] = p[t];
 }
 
-// Normal block, gradient and squared residual of one view, reduced over its warp (every lane
-// ends with the totals).
-__device__ __forceinline__ void linearize_view(const RotArgs& a, const double* __restrict__ R, int v, int lane,
-                                               double (&u)[6], double (&g)[3], double& err) {
+// Contributions of one measurement to its view's normal block u (00 01 02 11 12 22), gradient
+// J^T(-e) and squared residual, accumulated into acc = {u[6], g[3], err}.
+__device__ __forceinline__ void accumulate_measurement(const RotArgs& a, const double* __restrict__ R, int k,
+                                                       double (&acc)[10]) {
+  const bool second = k >= a.P;
+  const int q = second ? k - a.P : k;
+  const int i = __ldg(a.pairs + 2 * q), j = __ldg(a.pairs + 2 * q + 1);
+  double Ri[9];
+  load9(R + 9 * (size_t)i, Ri);
+  const double* __restrict__ Rj = R + 9 * (size_t)j;
+  const double* __restrict__ Rij = a.rel + 9 * (size_t)q;
 #pragma unroll
-  for (int t = 0; t < 6; ++t) u[t] = 0.0;
-  g[0] = g[1] = g[2] = 0.0;
-  err = 0.0;
-  const int end = a.vptr[v + 1];
-  for (int t = a.vptr[v] + lane; t < end; t += kWarp) {
-    const int k = a.vlist[t];
-    const bool second = k >= a.P;
-    const int q = second ? k - a.P : k;
-    const int i = __ldg(a.pairs + 2 * q), j = __ldg(a.pairs + 2 * q + 1);
-    double Ri[9], Rj[9], Rij[9];
-    load9(R + 9 * (size_t)i, Ri);
-    load9(R + 9 * (size_t)j, Rj);
+  for (int r = 0; r < 3; ++r) {
+    // one row of R_ij and R_j at a time keeps the live registers down
+    const double m0 = __ldg(Rij + 3 * r), m1 = __ldg(Rij + 3 * r + 1), m2 = __ldg(Rij + 3 * r + 2);
+    double p[3], e[3], A[3];
 #pragma unroll
-    for (int s = 0; s < 9; ++s) Rij[s] = __ldg(a.rel + 9 * (size_t)q + s);
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      double p[3], e[3], A[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        p[c] = Rij[3 * r] * Ri[c] + Rij[3 * r + 1] * Ri[3 + c] + Rij[3 * r + 2] * Ri[6 + c];
-        e[c] = Rj[3 * r + c] - p[c];
-        A[c] = second ? Rj[3 * r + c] : -p[c];
-        err += e[c] * e[c];
-      }
-      // rows 3r..3r+2 of the 9x3 Jacobian: [0 -A2 A1], [A2 0 -A0], [-A1 A0 0]
-      u[0] += A[1] * A[1] + A[2] * A[2];
-      u[1] -= A[0] * A[1];
-      u[2] -= A[0] * A[2];
-      u[3] += A[0] * A[0] + A[2] * A[2];
-      u[4] -= A[1] * A[2];
-      u[5] += A[0] * A[0] + A[1] * A[1];
-      g[0] -= A[2] * e[1] - A[1] * e[2];
-      g[1] -= A[0] * e[2] - A[2] * e[0];
-      g[2] -= A[1] * e[0] - A[0] * e[1];
+    for (int c = 0; c < 3; ++c) {
+      const double rj = Rj[3 * r + c];
+      p[c] = m0 * Ri[c] + m1 * Ri[3 + c] + m2 * Ri[6 + c];
+      e[c] = rj - p[c];
+      A[c] = second ? rj : -p[c];
+      acc[9] += e[c] * e[c];
     }
+    // rows 3r..3r+2 of the 9x3 Jacobian: [0 -A2 A1], [A2 0 -A0], [-A1 A0 0]
+    acc[0] += A[1] * A[1] + A[2] * A[2];
+    acc[1] -= A[0] * A[1];
+    acc[2] -= A[0] * A[2];
+    acc[3] += A[0] * A[0] + A[2] * A[2];
+    acc[4] -= A[1] * A[2];
+    acc[5] += A[0] * A[0] + A[1] * A[1];
+    acc[6] -= A[2] * e[1] - A[1] * e[2];
+    acc[7] -= A[0] * e[2] - A[2] * e[0];
+    acc[8] -= A[1] * e[0] - A[0] * e[1];
+  }
+}
+
+// Sum of acc over a group of G lanes (aligned, G a power of two <= 32).  The first step is
+// transposed: the lower half of the group keeps values 0-4, the upper half 5-9, so one shuffle
+// per value pair; the halves then finish with butterflies.  Afterwards lane 0 of the group holds
+// the totals of values 0-4 and lane G/2 those of values 5-9 (each in the same slots of acc).
+template <int G>
+__device__ __forceinline__ void group_sum(double (&acc)[10], int lane) {
+  if (G == 1) return;
+  const bool upper = (lane & (G / 2)) != 0;
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    const double send = upper ? acc[t] : acc[5 + t];
+    const double got = __shfl_xor_sync(0xffffffffu, send, G / 2);
+    if (upper)
+      acc[5 + t] += got;
+    else
+      acc[t] += got;
   }
 #pragma unroll
-  for (int t = 0; t < 6; ++t) u[t] = warp_sum(u[t]);
+  for (int o = G / 4; o > 0; o >>= 1) {
 #pragma unroll
-  for (int t = 0; t < 3; ++t) g[t] = warp_sum(g[t]);
-  err = warp_sum(err);
+    for (int t = 0; t < 5; ++t) {
+      const double mine = upper ? acc[5 + t] : acc[t];
+      const double got = __shfl_xor_sync(0xffffffffu, mine, o);
+      if (upper)
+        acc[5 + t] = mine + got;
+      else
+        acc[t] = mine + got;
+    }
+  }
 }
 
 // Grid-wide fold of NV values (the first NS summed, the rest max-reduced): per-block partials,
@@ -153,23 +173,42 @@ __device__ __forceinline__ void grid_fold(double (&v)[NV], double* part, int& pa
 }
 
 // Linearises every view at rotations R into U/g; returns {err, max |g|, max diag U} folded.
+// A group of G lanes owns a view and strides over its measurement list.
+template <int G>
 __device__ __forceinline__ void linearize_all(const RotArgs& a, const double* R, double* U, double* g, double (&out)[3],
                                               int& parity, cg::grid_group& grid) {
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int sub = lane & (G - 1);
+  const int group = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int ngroups = (gridDim.x * blockDim.x) / G;
   double err = 0.0, gmax = 0.0, dmax = -1e300;
-  for (int v = warp; v < a.N; v += nwarps) {
-    double u[6], gv[3], e;
-    linearize_view(a, R, v, lane, u, gv, e);
-    if (lane == 0) {
+  // every lane of a warp runs the same number of rounds (shuffles need the full warp)
+  const int rounds = (a.N + ngroups - 1) / ngroups;
+  for (int r = 0; r < rounds; ++r) {
+    const int v = group + r * ngroups;
+    double acc[10];
 #pragma unroll
-      for (int t = 0; t < 6; ++t) U[6 * (size_t)v + t] = u[t];
+    for (int t = 0; t < 10; ++t) acc[t] = 0.0;
+    if (v < a.N) {
+      const int end = a.vptr[v + 1];
+#pragma unroll 2
+      for (int t = a.vptr[v] + sub; t < end; t += G) accumulate_measurement(a, R, a.vlist[t], acc);
+    }
+    group_sum<G>(acc, lane);
+    if (v < a.N) {
+      if (sub == 0) {
 #pragma unroll
-      for (int t = 0; t < 3; ++t) g[3 * (size_t)v + t] = gv[t];
-      err += e;
-      gmax = fmax(gmax, fmax(fabs(gv[0]), fmax(fabs(gv[1]), fabs(gv[2]))));
-      dmax = fmax(dmax, fmax(u[0], fmax(u[3], u[5])));
+        for (int t = 0; t < 5; ++t) U[6 * (size_t)v + t] = acc[t];
+        dmax = fmax(dmax, fmax(acc[0], acc[3]));
+      }
+      if (sub == (G > 1 ? G / 2 : 0)) {
+        U[6 * (size_t)v + 5] = acc[5];
+#pragma unroll
+        for (int t = 0; t < 3; ++t) g[3 * (size_t)v + t] = acc[6 + t];
+        err += acc[9];
+        gmax = fmax(gmax, fmax(fabs(acc[6]), fmax(fabs(acc[7]), fabs(acc[8]))));
+        dmax = fmax(dmax, acc[5]);
+      }
     }
   }
   out[0] = err;
@@ -239,12 +278,13 @@ __device__ __forceinline__ void rotate_right(const double* __restrict__ R, const
       Rn[3 * r + col] = Rv[3 * r] * M[col] + Rv[3 * r + 1] * M[3 + col] + Rv[3 * r + 2] * M[6 + col];
 }
 
-__global__ void __launch_bounds__(kRotThreads) k_rot_lm(RotArgs a) {
+template <int G>
+__global__ void __launch_bounds__(kRotThreads, 2) k_rot_lm(RotArgs a) {
   cg::grid_group grid = cg::this_grid();
   int parity = 0;
   int cur = a.cur, lb = 0;   // rotations / normal-block buffers of the current linearisation
   double lin[3];
-  linearize_all(a, a.R[cur], a.U[lb], a.g[lb], lin, parity, grid);
+  linearize_all<G>(a, a.R[cur], a.U[lb], a.g[lb], lin, parity, grid);
   double err = lin[0], gmax = lin[1];
   const double err0 = err;
   double err_relin = err0;   // err at the last relinearisation (the reported cost)
@@ -295,7 +335,7 @@ __global__ void __launch_bounds__(kRotThreads) k_rot_lm(RotArgs a) {
       }
       // (2) trial cost, relinearised at the trial rotations into the spare block buffers
       double tr[3];
-      linearize_all(a, a.R[cur ^ 1], a.U[lb ^ 1], a.g[lb ^ 1], tr, parity, grid);
+      linearize_all<G>(a, a.R[cur ^ 1], a.U[lb ^ 1], a.g[lb ^ 1], tr, parity, grid);
       const double rho = (err - tr[0]) / (lambda * s[0] + s[1]);
       if (rho > 0.0) {
         accept = true;
@@ -348,13 +388,42 @@ __global__ void k_rot_keys(const int* __restrict__ pairs, int P, int* __restrict
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
+using RotKernel = void (*)(RotArgs);
+
+RotKernel rot_kernel(int G) {
+  switch (G) {
+    case 4: return k_rot_lm<4>;
+    case 8: return k_rot_lm<8>;
+    case 16: return k_rot_lm<16>;
+    default: return k_rot_lm<32>;
+  }
+}
+
+// Lanes per view: the group size that minimises (views per group) x (measurement rounds per
+// view + reduction steps) for the grid's lane count and the mean measurements per view.
+int pick_group(long n_views, long n_meas, long lanes) {
+  int best = 32;
+  double best_cost = 1e300;
+  const double mean = n_views > 0 ? (double)n_meas / (double)n_views : 0.0;
+  for (int G = 4; G <= 32; G *= 2) {
+    const long groups = std::max(1L, lanes / G);
+    const double seq = std::ceil((double)n_views / (double)groups);
+    const double cost = seq * (std::ceil(mean / G) + 0.5 * std::log2((double)G));
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = G;
+    }
+  }
+  return best;
+}
+
 }  // namespace
 }  // namespace v3dba
 
 using namespace v3dba;
 
 struct v3dba_rotations_s {
-  int N = 0, P = 0, grid = 1, cur = 0;
+  int N = 0, P = 0, full_grid = 1, cur = 0, G = 32;
   double nu = 2.0;
   cudaStream_t st = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -369,12 +438,6 @@ struct v3dba_rotations_s {
 
 namespace {
 
-bool finite_all(const double* p, size_t n) {
-  for (size_t t = 0; t < n; ++t)
-    if (!std::isfinite(p[t])) return false;
-  return true;
-}
-
 void release(v3dba_rotations h) {
   if (!h) return;
   if (h->arena) cudaFreeAsync(h->arena, h->st);
@@ -384,6 +447,11 @@ void release(v3dba_rotations h) {
   if (h->e1) cudaEventDestroy(h->e1);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
+}
+
+int grid_for(v3dba_rotations h, int G) {
+  const long want = std::max(1L, ((long)h->N * G + kRotThreads - 1) / kRotThreads);
+  return (int)std::max(1L, std::min((long)h->full_grid, want));
 }
 
 int run(v3dba_rotations h, const v3dba_options* o, int max_iter, RotState* out, float* ms) {
@@ -420,7 +488,8 @@ int run(v3dba_rotations h, const v3dba_options* o, int max_iter, RotState* out, 
   a.stop_cost = o->stop_cost;
   void* args[] = {&a};
   V3DBA_CUDA_TRY(cudaEventRecord(h->e0, h->st));
-  V3DBA_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_rot_lm, h->grid, kRotThreads, args, 0, h->st));
+  V3DBA_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)rot_kernel(h->G), grid_for(h, h->G), kRotThreads, args, 0,
+                                             h->st));
   note_launches(1);
   V3DBA_CUDA_TRY(cudaEventRecord(h->e1, h->st));
   V3DBA_CUDA_TRY(cudaMemcpyAsync(out, h->state, sizeof(RotState), cudaMemcpyDeviceToHost, h->st));
@@ -443,7 +512,7 @@ int v3dba_rotations_create(int n_views, int n_pairs, const double* relative_rota
   if ((long)n_pairs * 2 > 0x7fffffffL || (long)n_views * 9 > 0x7fffffffL) return V3DBA_ERR_UNSUPPORTED;
   for (long t = 0; t < 2L * n_pairs; ++t)
     if (view_pairs[t] < 0 || view_pairs[t] >= n_views) return V3DBA_ERR_INVALID_INPUT;
-  if (!finite_all(relative_rotations, 9 * (size_t)n_pairs) || !finite_all(rotations, 9 * (size_t)n_views))
+  if (!all_finite(relative_rotations, 9 * (size_t)n_pairs) || !all_finite(rotations, 9 * (size_t)n_views))
     return V3DBA_ERR_INVALID_INPUT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -471,15 +540,18 @@ int v3dba_rotations_create(int n_views, int n_pairs, const double* relative_rota
       return _e == cudaErrorMemoryAllocation ? V3DBA_ERR_OUT_OF_MEMORY : V3DBA_ERR_CUDA;               \
     }                                                                                                  \
   } while (0)
+  TRY(ensure_pool());
   CTRY(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
   CTRY(cudaEventCreate(&h->e0));
   CTRY(cudaEventCreate(&h->e1));
   int dev = 0, sms = 148, per_sm = 1;
   CTRY(cudaGetDevice(&dev));
   CTRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  CTRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rot_lm, kRotThreads, 0));
-  const int want = std::max(1, (n_views + kRotWarps - 1) / kRotWarps);
-  h->grid = std::max(1, std::min(sms * std::max(per_sm, 1), want));
+  // occupancy of the instantiations is the same (one register budget); pick the group size for
+  // the full grid, then trim the grid to what the views need
+  CTRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rot_lm<32>, kRotThreads, 0));
+  h->full_grid = sms * std::max(per_sm, 1);
+  h->G = pick_group(n_views, 2L * n_pairs, (long)h->full_grid * kRotThreads);
   const size_t N = n_views, P = n_pairs;
   // one arena for every buffer
   size_t off = 0;
@@ -490,7 +562,7 @@ int v3dba_rotations_create(int n_views, int n_pairs, const double* relative_rota
   };
   const size_t o_rel = take(72 * P), o_R0 = take(72 * N), o_Ra = take(72 * N), o_Rb = take(72 * N);
   const size_t o_Ua = take(48 * N), o_Ub = take(48 * N), o_ga = take(24 * N), o_gb = take(24 * N);
-  const size_t o_part = take(sizeof(double) * 2 * kRotPart * (size_t)h->grid);
+  const size_t o_part = take(sizeof(double) * 2 * kRotPart * (size_t)h->full_grid);
   const size_t o_pairs = take(8 * P), o_vptr = take(4 * (N + 1)), o_vlist = take(8 * P), o_keys = take(8 * P);
   const size_t o_state = take(sizeof(RotState));
   CTRY(cudaMallocAsync(reinterpret_cast<void**>(&h->arena), off, h->st));
@@ -591,7 +663,7 @@ int v3dba_rotations_get(v3dba_rotations h, double* rotations) {
 
 int v3dba_rotations_set(v3dba_rotations h, const double* rotations) {
   if (!h || (h->N > 0 && !rotations)) return V3DBA_ERR_INVALID_ARGUMENT;
-  if (!finite_all(rotations, 9 * (size_t)h->N)) return V3DBA_ERR_INVALID_INPUT;
+  if (!all_finite(rotations, 9 * (size_t)h->N)) return V3DBA_ERR_INVALID_INPUT;
   h->nu = 2.0;
   if (h->N == 0) return V3DBA_OK;
   V3DBA_CUDA_TRY(cudaMemcpyAsync(h->R[h->cur], rotations, 72 * (size_t)h->N, cudaMemcpyHostToDevice, h->st));
@@ -606,6 +678,40 @@ int v3dba_rotations_reset(v3dba_rotations h) {
   if (h->N == 0) return V3DBA_OK;
   V3DBA_CUDA_TRY(cudaMemcpyAsync(h->R[0], h->R0, 72 * (size_t)h->N, cudaMemcpyDeviceToDevice, h->st));
   V3DBA_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return V3DBA_OK;
+}
+
+int v3dba_rotations_set_group(v3dba_rotations h, int group) {
+  if (!h || (group != 4 && group != 8 && group != 16 && group != 32)) return V3DBA_ERR_INVALID_ARGUMENT;
+  h->G = group;
+  return V3DBA_OK;
+}
+
+int v3dba_rotations_autotune(v3dba_rotations h, int* group) {
+  if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (h->N > 0) {
+    v3dba_options o;
+    v3dba_default_options(&o);
+    int best = h->G;
+    float best_ms = 1e30f;
+    for (int G = 4; G <= 32; G *= 2) {
+      h->G = G;
+      float t_min = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {   // zero iterations: one linearisation sweep, rotations untouched
+        RotState s;
+        float ms = 0.f;
+        const int rc = run(h, &o, 0, &s, &ms);
+        if (rc) return rc;
+        t_min = std::min(t_min, ms);
+      }
+      if (t_min < best_ms) {
+        best_ms = t_min;
+        best = G;
+      }
+    }
+    h->G = best;
+  }
+  if (group) *group = h->G;
   return V3DBA_OK;
 }
 

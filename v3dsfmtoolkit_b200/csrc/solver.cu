@@ -74,28 +74,6 @@ int dims_of(int model, int mode, int* dA, int* dC) {
   return V3DBA_OK;
 }
 
-bool all_finite(const double* p, size_t n) {
-  for (size_t i = 0; i < n; ++i)
-    if (!std::isfinite(p[i])) return false;
-  return true;
-}
-
-// Handle buffers come from the device's stream-ordered pool, which keeps freed memory for the
-// next handle (release threshold raised once per device): creating and destroying handles in a
-// loop then neither maps nor unmaps device memory, and destroy does not stall on cudaFree.
-int ensure_pool() {
-  static std::atomic<uint64_t> done_mask{0};
-  int dev = 0;
-  V3DBA_CUDA_TRY(cudaGetDevice(&dev));
-  const uint64_t bit = 1ull << (dev & 63);
-  if (done_mask.load() & bit) return V3DBA_OK;
-  cudaMemPool_t pool;
-  V3DBA_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
-  uint64_t thr = UINT64_MAX;
-  V3DBA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-  done_mask.fetch_or(bit);
-  return V3DBA_OK;
-}
 
 template <typename T>
 int dalloc(v3dba_handle h, T** p, size_t count) {
