@@ -24,6 +24,11 @@ with the learned preconditioner (factor + gauge coarse space); block-Jacobi and 
 gauge space run beside it, outside the timed region.  One step = minimize() until the cost of 25
 direct-solve (FP64 tile Cholesky) LM iterations is reached (1e-6 relative).
 
+--workload stereo300 measures the rig adjuster (StereoMetricBundleOptimizer): a binocular rig
+(two pinhole cameras, 0.3 baseline, fixed on the rig) at 300 poses along a path, 40,000 points
+seen from up to 6 consecutive poses (~450k observations), 1% outliers, Huber 2 px; one step =
+minimize() until the reference optimizer's own 40-iteration cost (1e-6 relative).
+
 --workload rotations10000 measures rotation averaging (refineConsistentRotations): 10,000 views,
 200,000 view pairs (5 sequential neighbours per view plus random loop closures), 1 deg relative
 rotation noise, 5 deg initial error; one step = one complete LM run (the reference's own stopping
@@ -53,6 +58,12 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "sequence200"
 METRIC = "LM iterations/s to the reference cost (distortion BA, 200 cams / 50k pts / ~375k obs)"
+# bundle-adjustment workloads timed to the reference optimizer's own final cost
+BA_WORKLOADS = {
+    "sequence200": dict(metric=METRIC, model="CommonInternalsMetricBundleOptimizer RADIAL_TANGENTIAL"),
+    "stereo300": dict(metric="LM iterations/s to the reference cost (rig BA, 300 poses x 2 cameras / 39k pts / "
+                             "~450k obs)", model="StereoMetricBundleOptimizer (binocular rig)"),
+}
 UNIT = "LM iterations/s"
 REL_TOL = 1e-6
 
@@ -65,7 +76,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["sequence200", "triplets4096", "cluster2000", "rotations10000"],
+    ap.add_argument("--workload", choices=["sequence200", "stereo300", "triplets4096", "cluster2000", "rotations10000"],
                     default="sequence200")
     ap.add_argument("--profile-stages", type=int, default=0, metavar="R",
                     help="run every stage of one LM iteration R times (mixed precision) and exit; "
@@ -82,13 +93,15 @@ def run_profile_stages(args):
     h.close()
 
 
-def load_reference_target():
-    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_reference.json")))[WORKLOAD]
+def load_reference_target(workload=WORKLOAD):
+    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_reference.json")))[workload]
     return ref
 
 
-def make_scene():
+def make_scene(workload=WORKLOAD):
     from v3dsfmtoolkit_b200 import scenes
+    if workload == "stereo300":
+        return scenes.stereo_rig_scene(n_poses=300, n_points=40000, seed=0, window=6, outlier_frac=0.01)
     return scenes.sequence_scene()
 
 
@@ -99,6 +112,9 @@ def scene_digest(sc):
         h.update(np.ascontiguousarray(a).tobytes())
     if sc.dist is not None:
         h.update(np.ascontiguousarray(sc.dist).tobytes())
+    if getattr(sc, "rig_K", None) is not None:
+        for a in (sc.rig_K, sc.rig_R, sc.rig_T, sc.sub):
+            h.update(np.ascontiguousarray(a).tobytes())
     return h.hexdigest()[:16]
 
 
@@ -181,8 +197,9 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    ref = load_reference_target()
-    sc = make_scene()
+    wl = args.workload
+    ref = load_reference_target(wl)
+    sc = make_scene(wl)
     if scene_digest(sc) != ref["digest"]:
         raise RuntimeError("generated scene differs from the one the reference cost was recorded on")
     target = ref["cost"] * (1.0 + REL_TOL)
@@ -240,7 +257,7 @@ def run_ours(args, rank, world, local_rank):
     traffic = {}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(WORKLOAD, {})
+        traffic = json.load(open(tp)).get(wl, {})
     fp64_peak = capi.fp64_mma_peak_tflops()
     chol_flops = h.cholesky_flops()
     chol_ms = st_ms["cholesky"]
@@ -297,17 +314,17 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(sc, iters_per_sample=10)
+        cpu = cpu_baseline_sample(sc, iters_per_sample=10 if wl == "sequence200" else 4, workload=wl)
         cpu["reference_iterations_to_cost"] = ref["iterations"]
         cpu["time_to_reference_cost_s_est"] = round(ref["iterations"] / cpu["value"], 2)
 
     line = {
-        "metric": METRIC, "value": round(total_it_all / (total_ms_max * 1e-3), 3), "unit": UNIT,
+        "metric": BA_WORKLOADS[wl]["metric"], "value": round(total_it_all / (total_ms_max * 1e-3), 3), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total_ms_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "n_cameras": sc.n_cams, "n_points": sc.n_points,
-                   "n_observations": sc.n_obs, "model": "CommonInternalsMetricBundleOptimizer RADIAL_TANGENTIAL",
+        "config": {"workload": wl, "n_cameras": sc.n_cams, "n_points": sc.n_points,
+                   "n_observations": sc.n_obs, "model": BA_WORKLOADS[wl]["model"],
                    "huber_threshold_px": sc.inlier_threshold, "stop": f"cost <= reference cost * (1 + {REL_TOL})",
                    "reference_cost": ref["cost"], "l2": "flushed (256 MiB write) before every step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -327,7 +344,7 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
-def cpu_baseline_sample(sc, iters_per_sample):
+def cpu_baseline_sample(sc, iters_per_sample, workload=WORKLOAD):
     """The reference optimizer (compiled from its sources) on a bounded sample: one minimize()
     call of `iters_per_sample` LM iterations, including its one-time ordering setup."""
     from oracle.bindings import Reference, reference_available
@@ -340,7 +357,7 @@ def cpu_baseline_sample(sc, iters_per_sample):
     _, info = eng.minimize(sc, max_iterations=iters_per_sample)
     dt = time.perf_counter() - t0
     return {"value": round(info["iterations"] / dt, 4), "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"{WORKLOAD}: one minimize() of {info['iterations']} LM iterations incl. setup, "
+            "sample": f"{workload}: one minimize() of {info['iterations']} LM iterations incl. setup, "
                       f"{dt:.1f} s on 1 host core", "sample_s": round(dt, 3)}
 
 
@@ -390,10 +407,13 @@ def run_reference(args, rank, world):
                                          "minutes on the host; the reference arm is timed on sequence200"}), flush=True)
         return
     from oracle.bindings import Reference, Restatement, reference_available
-    sc = make_scene()
+    wl = args.workload if args.workload in BA_WORKLOADS else WORKLOAD
+    sc = make_scene(wl)
     kind = "reference" if reference_available() else "port"
     eng = Reference() if kind == "reference" else Restatement()
     m = max(2, min(10, 100 // max(args.steps, 1)))
+    if wl == "stereo300":
+        m = 2   # ~1.5 s per iteration on one core
     for _ in range(args.warmup):
         eng.minimize(sc, max_iterations=1)
     t0 = time.perf_counter()
@@ -404,14 +424,14 @@ def run_reference(args, rank, world):
     dt = time.perf_counter() - t0
     v = its / dt
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
+        "impl": "reference", "metric": BA_WORKLOADS[wl]["metric"], "value": round(v, 4), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "n_cameras": sc.n_cams, "n_points": sc.n_points,
+        "config": {"workload": wl, "n_cameras": sc.n_cams, "n_points": sc.n_points,
                    "n_observations": sc.n_obs, "sample": f"{m} LM iterations of minimize() per step"},
         "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": kind,
-                         "sample": f"{args.steps} x minimize() of {m} LM iterations on {WORKLOAD}"},
+                         "sample": f"{args.steps} x minimize() of {m} LM iterations on {wl}"},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

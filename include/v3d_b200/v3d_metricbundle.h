@@ -82,7 +82,7 @@ namespace V3D
             int const N = cams.size(), M = Xs.size(), Kn = measurements.size();
             std::vector<double> Kb, R, T, D;
             pack(Kb, R, T, D);
-            v3dba_problem p;
+            v3dba_problem p = v3dba_problem();
             p.model = model; p.mode = mode;
             p.n_cameras = N; p.n_points = M; p.n_measurements = Kn;
             p.inlier_threshold = inlierThreshold;

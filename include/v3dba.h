@@ -15,6 +15,9 @@
  *   v3dba_set_params /
  *   v3dba_get_params       <- the optimizer's in-place mutation of the caller's cameras, points,
  *                             K and distortion references (v3d_metricbundle.h:94-95, 232-233, 316)
+ *                             StereoMetricBundleOptimizer (V3D/include/Geometry/v3d_stereobundle.h:
+ *                              22-163, V3D/src/Geometry/v3d_stereobundle.cpp:45-67) as
+ *                              V3DBA_MODEL_STEREO
  *   v3dba_refine_consistent_rotations / v3dba_rotations_*
  *                          <- V3D::refineConsistentRotations and its SparseRotationOptimizer
  *                             (V3D/include/Geometry/v3d_mviewutilities.h:359-362,
@@ -59,11 +62,12 @@ enum {
   V3DBA_ERR_NUMERICAL = 8           /* training of the learned preconditioner diverged       */
 };
 
-/* models (the three optimizer classes) */
+/* models (the optimizer classes) */
 enum {
   V3DBA_MODEL_STD = 0,              /* StdMetricBundleOptimizer                             */
   V3DBA_MODEL_COMMON = 1,           /* CommonInternalsMetricBundleOptimizer                 */
-  V3DBA_MODEL_VARYING = 2           /* VaryingInternalsMetricBundleOptimizer                */
+  V3DBA_MODEL_VARYING = 2,          /* VaryingInternalsMetricBundleOptimizer                */
+  V3DBA_MODEL_STEREO = 3            /* StereoMetricBundleOptimizer (rigid multi-camera rigs) */
 };
 
 /* FULL_BUNDLE_* modes (V3D/include/Geometry/v3d_metricbundle.h:140-148) */
@@ -119,6 +123,15 @@ typedef struct v3dba_problem {
   const double* measurements;
   const int32_t* view;
   const int32_t* point;
+  /* V3DBA_MODEL_STEREO only (StereoMetricBundleOptimizer, V3D/include/Geometry/
+   * v3d_stereobundle.h:22-163): R / T are the poses of the n_cameras rig positions, K and dist
+   * are unused (may be NULL); measurement k is seen by camera subcamera[k] of the rig, a fixed
+   * pinhole camera K_l (R_l (R_i X + T_i) + T_l).  Other models ignore these fields. */
+  int n_rig_cameras;
+  const double* rig_K;              /* n_rig_cameras*9                                      */
+  const double* rig_R;              /* n_rig_cameras*9                                      */
+  const double* rig_T;              /* n_rig_cameras*3                                      */
+  const int32_t* subcamera;         /* n_measurements                                       */
 } v3dba_problem;
 
 typedef struct v3dba_options {

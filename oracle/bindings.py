@@ -70,15 +70,43 @@ class Reference:
         L.v3dref_linearize.argtypes = [C.c_int] * 5 + [C.c_double] + [_dp] * 5 + [_dp, _ip, _ip] + [_dp] * 5
         L.v3dref_cost.restype = C.c_double
         L.v3dref_cost.argtypes = [C.c_int] * 5 + [C.c_double] + [_dp] * 5 + [_dp, _ip, _ip]
+        L.v3dref_minimize_stereo.restype = C.c_int
+        L.v3dref_minimize_stereo.argtypes = [C.c_int] * 4 + [C.c_double] + [_dp] * 4 + [_ip] * 3 + [_dp] * 3 + \
+            [C.c_int, C.c_int, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp, _ip, C.c_int, _ip, _ip]
+        L.v3dref_linearize_stereo.restype = C.c_int
+        L.v3dref_linearize_stereo.argtypes = [C.c_int] * 4 + [C.c_double] + [_dp] * 4 + [_ip] * 3 + [_dp] * 7
         L.v3dref_refine_rotations.restype = C.c_int
         L.v3dref_refine_rotations.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, _dp, C.c_int, _ip]
 
     def _head(self, sc):
         return (sc.model, sc.mode, sc.n_cams, sc.n_points, sc.n_obs, float(sc.inlier_threshold))
 
+    def _stereo_args(self, sc):
+        return (_f64(sc.meas), _i32(sc.view), _i32(sc.point), _i32(sc.sub), _f64(sc.rig_K), _f64(sc.rig_R),
+                _f64(sc.rig_T))
+
+    def _minimize_stereo(self, scene, tau, max_iterations, nonvarying, trace_cap):
+        K, R, T, dist, X = _scene_arrays(scene)
+        m, v, p, s, rk, rr, rt = self._stereo_args(scene)
+        st, it, lam = C.c_int(), C.c_int(), C.c_double()
+        tc, tl, ti = np.zeros(trace_cap), np.zeros(trace_cap), np.zeros(trace_cap, dtype=np.int32)
+        tlen, nrej = C.c_int(), C.c_int()
+        self.lib.v3dref_minimize_stereo(scene.n_cams, scene.n_points, scene.n_obs, scene.n_rig,
+                                        float(scene.inlier_threshold), _d(R), _d(T), _d(X), _d(m), _i(v), _i(p),
+                                        _i(s), _d(rk), _d(rr), _d(rt), nonvarying[0], nonvarying[1], tau,
+                                        max_iterations, C.byref(st), C.byref(it), C.byref(lam), _d(tc), _d(tl),
+                                        _i(ti), trace_cap, C.byref(tlen), C.byref(nrej))
+        n = min(tlen.value, trace_cap)
+        info = dict(status=st.value, iterations=it.value, lambda_=lam.value,
+                    trace_cost=tc[:n].copy(), trace_lambda=tl[:n].copy(), trace_iter=ti[:n].copy(),
+                    n_relinearizations=tlen.value, n_rejected=nrej.value)
+        return (K, R, T, dist, X), info
+
     def minimize(self, scene, tau=1e-3, max_iterations=50, nonvarying=(0, 0, 0), verbosity=0,
                  trace_cap=256):
         """Runs minimize() on a copy of ``scene``'s parameters; returns (params, info)."""
+        if scene.model == 3:
+            return self._minimize_stereo(scene, tau, max_iterations, nonvarying, trace_cap)
         K, R, T, dist, X = _scene_arrays(scene)
         meas, view, point = _f64(scene.meas), _i32(scene.view), _i32(scene.point)
         st, it, lam = C.c_int(), C.c_int(), C.c_double()
@@ -100,6 +128,13 @@ class Reference:
         dA, dC = scene.dims
         K, R, T, dist, X = params if params is not None else _scene_arrays(scene)
         n = scene.n_obs
+        if scene.model == 3:
+            m, v, p, s, rk, rr, rt = self._stereo_args(scene)
+            e, w, A, B = np.zeros((n, 2)), np.zeros(n), np.zeros((n, 2, 6)), np.zeros((n, 2, 3))
+            self.lib.v3dref_linearize_stereo(scene.n_cams, scene.n_points, n, scene.n_rig, float(scene.inlier_threshold),
+                                             _d(_f64(R)), _d(_f64(T)), _d(_f64(X)), _d(m), _i(v), _i(p), _i(s),
+                                             _d(rk), _d(rr), _d(rt), _d(e), _d(w), _d(A), _d(B))
+            return e, w, A, B, np.zeros((n, 2, 0))
         e, w = np.zeros((n, 2)), np.zeros(n)
         A, B, Cm = np.zeros((n, 2, dA)), np.zeros((n, 2, 3)), np.zeros((n, 2, max(dC, 1)))
         rc = self.lib.v3dref_linearize(*self._head(scene), _d(_f64(K)), _d(_f64(R)), _d(_f64(T)),
@@ -112,6 +147,9 @@ class Reference:
 
     def cost(self, scene, params=None):
         K, R, T, dist, X = params if params is not None else _scene_arrays(scene)
+        if scene.model == 3:
+            e, w, _, _, _ = self.linearize(scene, (K, R, T, dist, X))
+            return float(np.sum(w * w * np.sum(e * e, axis=1)))
         return self.lib.v3dref_cost(*self._head(scene), _d(_f64(K)), _d(_f64(R)), _d(_f64(T)),
                                     _d(_f64(dist)), _d(_f64(X)), _d(_f64(scene.meas)),
                                     _i(_i32(scene.view)), _i(_i32(scene.point)))
@@ -130,7 +168,8 @@ class Reference:
 class _OrcProblem(C.Structure):
     _fields_ = [("model", C.c_int), ("mode", C.c_int), ("n_cams", C.c_int), ("n_points", C.c_int),
                 ("n_obs", C.c_int), ("inlier_threshold", C.c_double), ("nnA", C.c_int),
-                ("nnB", C.c_int), ("nnC", C.c_int), ("meas", _dp), ("view", _ip), ("point", _ip)]
+                ("nnB", C.c_int), ("nnC", C.c_int), ("meas", _dp), ("view", _ip), ("point", _ip),
+                ("n_rig", C.c_int), ("rig_K", _dp), ("rig_R", _dp), ("rig_T", _dp), ("sub", _ip)]
 
 
 class _OrcParams(C.Structure):
@@ -181,6 +220,11 @@ class Restatement:
         keep = (_f64(scene.meas), _i32(scene.view), _i32(scene.point))
         p = _OrcProblem(scene.model, scene.mode, scene.n_cams, scene.n_points, scene.n_obs,
                         float(scene.inlier_threshold), *nonvarying, _d(keep[0]), _i(keep[1]), _i(keep[2]))
+        if getattr(scene, "rig_K", None) is not None:
+            rig = (_f64(scene.rig_K), _f64(scene.rig_R), _f64(scene.rig_T), _i32(scene.sub))
+            keep = keep + rig
+            p.n_rig = scene.n_rig
+            p.rig_K, p.rig_R, p.rig_T, p.sub = _d(rig[0]), _d(rig[1]), _d(rig[2]), _i(rig[3])
         return p, keep
 
     @staticmethod
@@ -191,7 +235,7 @@ class Restatement:
     @staticmethod
     def cached_ar(scene):
         K = scene.K if scene.K.ndim == 2 else scene.K[0]
-        return float(K[1, 1] / K[0, 0])
+        return float(K[1, 1] / K[0, 0]) if K[0, 0] != 0 else 1.0
 
     def param_length(self, scene):
         p, keep = self._problem(scene)

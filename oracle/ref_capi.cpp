@@ -9,7 +9,8 @@
 //   * V3D::VaryingInternalsMetricBundleOptimizer(V3D/include/Geometry/v3d_metricbundle.h:242-320)
 // all running V3D::SparseLevenbergOptimizer::minimize (V3D/src/Math/v3d_optimization.cpp:719-1250),
 // and the rotation averaging V3D::refineConsistentRotations (V3D/src/Geometry/
-// v3d_mviewutilities.cpp:470-613), which runs the same minimize() on SparseRotationOptimizer.
+// v3d_mviewutilities.cpp:470-613), which runs the same minimize() on SparseRotationOptimizer,
+// and V3D::StereoMetricBundleOptimizer (V3D/include/Geometry/v3d_stereobundle.h:22-163).
 //
 // Parameter layout (row-major, doubles), shared with the product C-ABI:
 //   K    : model 0/2 -> nCams*9 per-camera intrinsics; model 1 -> 9 (the shared K)
@@ -19,6 +20,7 @@
 
 #include "Geometry/v3d_metricbundle.h"
 #include "Geometry/v3d_mviewutilities.h"
+#include "Geometry/v3d_stereobundle.h"
 
 #include <cmath>
 #include <cstring>
@@ -346,4 +348,103 @@ int v3dref_refine_rotations(int nViews, int nPairs, double const* relR, int cons
    return 0;
 }
 
+// StereoMetricBundleOptimizer: nPoses rig poses (R 9, T 3 each; updated in place), nPoints
+// points (updated in place), nRig fixed rig cameras (K 9, R 9, T 3), measurements with view,
+// point and rig camera indices.  Same outputs as v3dref_minimize.
+int v3dref_minimize_stereo(int nPoses, int nPoints, int nObs, int nRig, double inlierThreshold,
+                           double* R, double* T, double* X, double const* meas, int const* view,
+                           int const* point, int const* sub, double const* rigK, double const* rigR,
+                           double const* rigT, int nnA, int nnB, double tau, int maxIterations,
+                           int* status, int* iterations, double* lambda,
+                           double* traceCost, double* traceLambda, int* traceIter, int traceCap,
+                           int* traceLen, int* nRejected)
+{
+   std::vector<Matrix3x3d> rotations(nPoses);
+   std::vector<Vector3d> translations(nPoses), Xs(nPoints);
+   std::vector<CameraMatrix> rig(nRig);
+   std::vector<Vector2d> ms(nObs);
+   for (int i = 0; i < nPoses; ++i)
+   {
+      loadMat3(R + 9 * i, rotations[i]);
+      translations[i] = Vector3d(T[3 * i], T[3 * i + 1], T[3 * i + 2]);
+   }
+   for (int j = 0; j < nPoints; ++j) Xs[j] = Vector3d(X[3 * j], X[3 * j + 1], X[3 * j + 2]);
+   for (int l = 0; l < nRig; ++l)
+   {
+      Matrix3x3d Kl, Rl;
+      loadMat3(rigK + 9 * l, Kl);
+      loadMat3(rigR + 9 * l, Rl);
+      rig[l] = CameraMatrix(Kl, Rl, Vector3d(rigT[3 * l], rigT[3 * l + 1], rigT[3 * l + 2]));
+   }
+   for (int k = 0; k < nObs; ++k) { ms[k][0] = meas[2 * k]; ms[k][1] = meas[2 * k + 1]; }
+   std::vector<int> vv(view, view + nObs), pp(point, point + nObs), ss(sub, sub + nObs);
+
+   Trace tr = { traceCost, traceLambda, traceIter, traceCap, 0, 0 };
+   V3D::optimizerVerbosenessLevel = 0;
+   Traced<StereoMetricBundleOptimizer> opt(&tr, inlierThreshold, rotations, translations, rig, Xs, ms, vv, pp, ss);
+   runMinimize(opt, nnA, nnB, 0, tau, maxIterations, status, iterations, lambda);
+
+   for (int i = 0; i < nPoses; ++i)
+   {
+      storeMat3(rotations[i], R + 9 * i);
+      T[3 * i] = translations[i][0]; T[3 * i + 1] = translations[i][1]; T[3 * i + 2] = translations[i][2];
+   }
+   for (int j = 0; j < nPoints; ++j) { X[3 * j] = Xs[j][0]; X[3 * j + 1] = Xs[j][1]; X[3 * j + 2] = Xs[j][2]; }
+   if (traceLen) *traceLen = tr.len;
+   if (nRejected) *nRejected = tr.nRejected;
+   return 0;
+}
+
+// Residuals, Huber weights and raw Jacobians (A 2x6, B 2x3 per observation) of the stereo model
+// from the reference's evalResidual / fillWeights / fillJacobians.  Any output may be NULL.
+int v3dref_linearize_stereo(int nPoses, int nPoints, int nObs, int nRig, double inlierThreshold,
+                            double const* R, double const* T, double const* X, double const* meas,
+                            int const* view, int const* point, int const* sub, double const* rigK,
+                            double const* rigR, double const* rigT, double* e, double* w, double* A, double* B)
+{
+   std::vector<Matrix3x3d> rotations(nPoses);
+   std::vector<Vector3d> translations(nPoses), Xs(nPoints);
+   std::vector<CameraMatrix> rig(nRig);
+   std::vector<Vector2d> ms(nObs);
+   for (int i = 0; i < nPoses; ++i)
+   {
+      loadMat3(R + 9 * i, rotations[i]);
+      translations[i] = Vector3d(T[3 * i], T[3 * i + 1], T[3 * i + 2]);
+   }
+   for (int j = 0; j < nPoints; ++j) Xs[j] = Vector3d(X[3 * j], X[3 * j + 1], X[3 * j + 2]);
+   for (int l = 0; l < nRig; ++l)
+   {
+      Matrix3x3d Kl, Rl;
+      loadMat3(rigK + 9 * l, Kl);
+      loadMat3(rigR + 9 * l, Rl);
+      rig[l] = CameraMatrix(Kl, Rl, Vector3d(rigT[3 * l], rigT[3 * l + 1], rigT[3 * l + 2]));
+   }
+   for (int k = 0; k < nObs; ++k) { ms[k][0] = meas[2 * k]; ms[k][1] = meas[2 * k + 1]; }
+   std::vector<int> vv(view, view + nObs), pp(point, point + nObs), ss(sub, sub + nObs);
+   StereoMetricBundleOptimizer opt(inlierThreshold, rotations, translations, rig, Xs, ms, vv, pp, ss);
+
+   VectorArray<double> res(nObs, 2);
+   Vector<double> weights(nObs);
+   opt.evalResidual(res);
+   opt.fillWeights(res, weights);
+   Matrix<double> Ak(2, 6), Bk(2, 3), Ck(2, 1);
+   for (int k = 0; k < nObs; ++k)
+   {
+      if (e) { e[2 * k] = res[k][0]; e[2 * k + 1] = res[k][1]; }
+      if (w) w[k] = weights[k];
+      if (A || B)
+      {
+         makeZeroMatrix(Ak); makeZeroMatrix(Bk);
+         opt.fillJacobians(Ak, Bk, Ck, view[k], point[k], k);
+         for (int r = 0; r < 2; ++r)
+         {
+            if (A) for (int c = 0; c < 6; ++c) A[(2 * k + r) * 6 + c] = Ak[r][c];
+            if (B) for (int c = 0; c < 3; ++c) B[(2 * k + r) * 3 + c] = Bk[r][c];
+         }
+      }
+   }
+   return 0;
+}
+
 } // extern "C"
+

@@ -25,6 +25,7 @@ static int intrinsic_dim(int mode)
 
 int orc_dims(int model, int mode, int* dA, int* dC)
 {
+  if (model == ORC_MODEL_STEREO) { *dA = 6; *dC = 0; return 0; }
   if (model < ORC_MODEL_STD || model > ORC_MODEL_VARYING) return -1;
   if (model != ORC_MODEL_STD && (mode < NO_ROT || mode > RADIAL_TAN)) return -1;
   *dA = 6 + (model == ORC_MODEL_VARYING ? intrinsic_dim(mode) : 0);
@@ -123,10 +124,22 @@ static const double* cam_dist(const orc_problem* p, const orc_params* x, int i)
  *   STD     : CameraMatrix::projectPoint, v3d_cameramatrix.h:184-190 (full K incl. skew, row 2)
  *   COMMON  : CommonInternals...::projectPoint, v3d_metricbundle.h:185-196 (shared K)
  *   VARYING : CameraMatrix::projectPoint(distortion, X), v3d_cameramatrix.h:192-205 */
-static void project(const orc_problem* p, const orc_params* x, int i, int j, double* q)
+static void project(const orc_problem* p, const orc_params* x, int i, int j, int k, double* q)
 {
   double XX[3];
   to_camera(x, i, j, XX);
+  if (p->model == ORC_MODEL_STEREO) {
+    /* StereoMetricBundleOptimizer::evalResidual, v3d_stereobundle.h:66-80: rig space, then the
+     * rig camera's projectPoint (v3d_cameramatrix.h:184-190) */
+    int l = p->sub[k];
+    double Y[3] = { XX[0], XX[1], XX[2] }, h[3];
+    rot_apply(p->rig_R + 9 * l, Y, XX);
+    for (int r = 0; r < 3; ++r) XX[r] += p->rig_T[3 * l + r];
+    rot_apply(p->rig_K + 9 * l, XX, h);
+    q[0] = h[0] / h[2];
+    q[1] = h[1] / h[2];
+    return;
+  }
   const double* K = cam_K(p, x, i);
   if (p->model == ORC_MODEL_STD) {
     double h[3];
@@ -144,12 +157,41 @@ static void project(const orc_problem* p, const orc_params* x, int i, int j, dou
 /* Jacobians of observation k (raw, unweighted), v3d_metricbundle.cpp:52-178, 216-296.
  * A: 2 x dA, B: 2 x 3, C: 2 x dC, row-major. */
 static void jacobians(const orc_problem* p, const orc_params* x, double cached_ar, int dA, int dC,
-                      int i, int j, double* A, double* B, double* C)
+                      int i, int j, int k, double* A, double* B, double* C)
 {
   const double* R = x->R + 9 * i;
   const double* T = x->T + 3 * i;
   double XX[3];
   to_camera(x, i, j, XX);
+
+  if (p->model == ORC_MODEL_STEREO) {
+    /* poseDerivatives + StereoMetricBundleOptimizer::fillJacobians, v3d_stereobundle.cpp:11-67:
+     * dY/d(T, omega) = [ I | -[R X]_x ], then through the rig camera's rotation R_l; f and the
+     * aspect ratio of K_l (skew and principal point ignored). */
+    int l = p->sub[k];
+    const double* Rl = p->rig_R + 9 * l;
+    const double* Kl = p->rig_K + 9 * l;
+    double RX[3] = { XX[0] - T[0], XX[1] - T[1], XX[2] - T[2] };
+    double dY[18];
+    memset(dY, 0, sizeof(dY));
+    dY[0 * 6 + 0] = dY[1 * 6 + 1] = dY[2 * 6 + 2] = 1.0;
+    dY[0 * 6 + 3] = 0.0;    dY[0 * 6 + 4] = RX[2];  dY[0 * 6 + 5] = -RX[1];
+    dY[1 * 6 + 3] = -RX[2]; dY[1 * 6 + 4] = 0.0;    dY[1 * 6 + 5] = RX[0];
+    dY[2 * 6 + 3] = RX[1];  dY[2 * 6 + 4] = -RX[0]; dY[2 * 6 + 5] = 0.0;
+    double Xl[3], d_dRT[18], d_dX[9], dp[6];
+    rot_apply(Rl, XX, Xl);
+    for (int r = 0; r < 3; ++r) Xl[r] += p->rig_T[3 * l + r];
+    matmul(Rl, dY, d_dRT, 3, 3, 6);
+    matmul(Rl, R, d_dX, 3, 3, 3);
+    double f = Kl[0], ar = Kl[4] / Kl[0];
+    double bx = f / (Xl[2] * Xl[2]), by = ar * bx;
+    dp[0] = bx * Xl[2]; dp[1] = 0.0;        dp[2] = -bx * Xl[0];
+    dp[3] = 0.0;        dp[4] = by * Xl[2]; dp[5] = -by * Xl[1];
+    matmul(dp, d_dRT, A, 2, 3, 6);
+    matmul(dp, d_dX, B, 2, 3, 3);
+    (void)cached_ar; (void)dA; (void)dC; (void)C;
+    return;
+  }
 
   /* poseDerivatives, v3d_metricbundle.cpp:52-71: d XX / d(T, omega) = [ I | -[XX - T]_x ],
    * d XX / d X = R. */
@@ -248,14 +290,14 @@ int orc_linearize(const orc_problem* p, const orc_params* x, double cached_ar,
   for (int k = 0; k < p->n_obs; ++k) {
     int i = p->view[k], j = p->point[k];
     double q[2], ek[2];
-    project(p, x, i, j, q);
+    project(p, x, i, j, k, q);
     ek[0] = q[0] - p->meas[2 * k];
     ek[1] = q[1] - p->meas[2 * k + 1];
     if (e) { e[2 * k] = ek[0]; e[2 * k + 1] = ek[1]; }
     if (w) w[k] = huber_weight(p->inlier_threshold, ek);
     if (A || B || C) {
       memset(a, 0, sizeof(a)); memset(c, 0, sizeof(c));
-      jacobians(p, x, cached_ar, dA, dC, i, j, a, b, c);
+      jacobians(p, x, cached_ar, dA, dC, i, j, k, a, b, c);
       if (A) memcpy(A + (size_t)k * 2 * dA, a, sizeof(double) * 2 * dA);
       if (B) memcpy(B + (size_t)k * 6, b, sizeof(double) * 6);
       if (C && dC) memcpy(C + (size_t)k * 2 * dC, c, sizeof(double) * 2 * dC);
@@ -270,7 +312,7 @@ double orc_cost(const orc_problem* p, const orc_params* x, double cached_ar, con
   double err = 0.0;
   for (int k = 0; k < p->n_obs; ++k) {
     double q[2], ek[2];
-    project(p, x, p->view[k], p->point[k], q);
+    project(p, x, p->view[k], p->point[k], k, q);
     ek[0] = q[0] - p->meas[2 * k];
     ek[1] = q[1] - p->meas[2 * k + 1];
     double wk = w ? w[k] : huber_weight(p->inlier_threshold, ek);
@@ -302,7 +344,7 @@ double orc_normal_blocks(const orc_problem* p, const orc_params* x, double cache
   for (int k = 0; k < p->n_obs; ++k) {
     int i = p->view[k], j = p->point[k];
     double q[2], ek[2];
-    project(p, x, i, j, q);
+    project(p, x, i, j, k, q);
     ek[0] = q[0] - p->meas[2 * k];
     ek[1] = q[1] - p->meas[2 * k + 1];
     double wk = huber_weight(p->inlier_threshold, ek);
@@ -314,7 +356,7 @@ double orc_normal_blocks(const orc_problem* p, const orc_params* x, double cache
     memset(a, 0, sizeof(a)); memset(b, 0, sizeof(b)); memset(c, 0, sizeof(c));
     /* An observation whose camera and point are both fixed still constrains the globals
      * (the reference skips it and leaves stale Jacobians, quirk Q6). */
-    jacobians(p, x, cached_ar, dA, dC, i, j, a, b, c);
+    jacobians(p, x, cached_ar, dA, dC, i, j, k, a, b, c);
     if (fixA) memset(a, 0, sizeof(a));
     if (fixB) memset(b, 0, sizeof(b));
     for (int l = 0; l < p->nnC && l < dC; ++l) c[l] = c[dC + l] = 0.0;
@@ -591,9 +633,9 @@ void orc_apply_update(const orc_problem* p, orc_params* x, double cached_ar,
 static void copy_params(const orc_problem* p, const orc_params* s, orc_params* d)
 {
   int N = p->n_cams, M = p->n_points;
-  int nK = p->model == ORC_MODEL_COMMON ? 9 : 9 * N;
+  int nK = p->model == ORC_MODEL_STEREO ? 0 : (p->model == ORC_MODEL_COMMON ? 9 : 9 * N);
   int nD = p->model == ORC_MODEL_COMMON ? 4 : (p->model == ORC_MODEL_VARYING ? 4 * N : 0);
-  memcpy(d->K, s->K, sizeof(double) * nK);
+  if (nK) memcpy(d->K, s->K, sizeof(double) * nK);
   memcpy(d->R, s->R, sizeof(double) * 9 * N);
   memcpy(d->T, s->T, sizeof(double) * 3 * N);
   if (nD) memcpy(d->dist, s->dist, sizeof(double) * nD);
@@ -622,7 +664,7 @@ int orc_minimize(const orc_problem* p, orc_params* x, orc_options* opt, orc_resu
   double *gb = malloc(sizeof(double) * 3 * M + 8), *gc = malloc(sizeof(double) * 8);
   double *S = malloc(sizeof(double) * (size_t)n * n + 8), *rhs = malloc(sizeof(double) * n + 8);
   double *Vinv = malloc(sizeof(double) * 9 * M + 8), *db = malloc(sizeof(double) * 3 * M + 8);
-  int nK = p->model == ORC_MODEL_COMMON ? 9 : 9 * N;
+  int nK = p->model == ORC_MODEL_STEREO ? 0 : (p->model == ORC_MODEL_COMMON ? 9 : 9 * N);
   int nD = p->model == ORC_MODEL_COMMON ? 4 : (p->model == ORC_MODEL_VARYING ? 4 * N : 0);
   orc_params saved = { malloc(sizeof(double) * nK), malloc(sizeof(double) * 9 * N + 8),
                        malloc(sizeof(double) * 3 * N + 8), malloc(sizeof(double) * (nD ? nD : 1)),

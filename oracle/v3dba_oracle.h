@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-enum { ORC_MODEL_STD = 0, ORC_MODEL_COMMON = 1, ORC_MODEL_VARYING = 2 };
+enum { ORC_MODEL_STD = 0, ORC_MODEL_COMMON = 1, ORC_MODEL_VARYING = 2, ORC_MODEL_STEREO = 3 };
 enum { ORC_TIMEOUT = 0, ORC_SMALL_UPDATE = 1, ORC_CONVERGED = 2 };
 
 typedef struct {
@@ -30,6 +30,13 @@ typedef struct {
   const double* meas;              /* n_obs*2                                            */
   const int* view;                 /* n_obs                                              */
   const int* point;                /* n_obs                                              */
+  /* ORC_MODEL_STEREO (StereoMetricBundleOptimizer, V3D/include/Geometry/v3d_stereobundle.h:
+   * 22-163): R/T are rig poses, K/dist unused; observation k is seen by rig camera sub[k]. */
+  int n_rig;
+  const double* rig_K;             /* n_rig*9                                            */
+  const double* rig_R;             /* n_rig*9                                            */
+  const double* rig_T;             /* n_rig*3                                            */
+  const int* sub;                  /* n_obs                                              */
 } orc_problem;
 
 typedef struct {                   /* row-major, in/out                                   */

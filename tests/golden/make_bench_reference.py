@@ -24,6 +24,7 @@ from v3dsfmtoolkit_b200 import scenes  # noqa: E402
 WORKLOADS = {
     "circle20": (lambda: scenes.circle_scene(), 100),
     "sequence200": (lambda: scenes.sequence_scene(), 100),
+    "stereo300": (lambda: scenes.stereo_rig_scene(n_poses=300, n_points=40000, seed=0, window=6, outlier_frac=0.01), 40),
 }
 
 
@@ -33,6 +34,9 @@ def scene_digest(sc):
         h.update(np.ascontiguousarray(a).tobytes())
     if sc.dist is not None:
         h.update(np.ascontiguousarray(sc.dist).tobytes())
+    if getattr(sc, "rig_K", None) is not None:
+        for a in (sc.rig_K, sc.rig_R, sc.rig_T, sc.sub):
+            h.update(np.ascontiguousarray(a).tobytes())
     return h.hexdigest()[:16]
 
 

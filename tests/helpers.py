@@ -18,6 +18,8 @@ def load_golden(name):
     sc = scenes.Scene(int(g["model"]), int(g["mode"]), float(g["inlier_threshold"]), g["K0"].copy(),
                       g["R0"].copy(), g["T0"].copy(), g["X0"].copy(), g["meas"].copy(), g["view"].copy(),
                       g["point"].copy(), g["dist0"].copy() if g["dist0"].size else None, name=name)
+    if "rig_K" in g.files:
+        sc.rig_K, sc.rig_R, sc.rig_T, sc.sub = g["rig_K"].copy(), g["rig_R"].copy(), g["rig_T"].copy(), g["sub"].copy()
     return sc, g
 
 

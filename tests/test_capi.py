@@ -40,8 +40,9 @@ def test_dims_and_defaults():
     o = capi.default_options()
     assert o.tau == 1e-3 and o.max_iterations == 50
     assert o.gradient_threshold == 1e-10 and o.update_threshold == 1e-10
+    assert capi.dims(capi.MODEL_STEREO, 0) == (6, 0)
     with pytest.raises(capi.V3dbaError):
-        capi.dims(3, 0)
+        capi.dims(4, 0)
     with pytest.raises(capi.V3dbaError):
         capi.dims(1, 5)
 

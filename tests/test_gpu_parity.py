@@ -30,7 +30,7 @@ def test_linearization_matches_reference(name):
         assert rel(lin["C"][:n], g["C"]) < 1e-12
 
 
-@pytest.mark.parametrize("name", ["std_circle", "common_rt", "varying_rt", "std_fixed"])
+@pytest.mark.parametrize("name", ["std_circle", "common_rt", "varying_rt", "std_fixed", "stereo_rig", "stereo_fixed"])
 def test_gradient_matches_oracle(orc, name):
     sc, g = load_golden(name)
     nv = tuple(int(v) for v in g["nonvarying"])
@@ -44,7 +44,8 @@ def test_gradient_matches_oracle(orc, name):
         assert rel(lin["gc"], bl["gc"]) < 1e-11
 
 
-@pytest.mark.parametrize("name", ["std_circle", "std_fixed", "common_rt", "common_focal", "varying_rt", "varying_pp"])
+@pytest.mark.parametrize("name", ["std_circle", "std_fixed", "common_rt", "common_focal", "varying_rt", "varying_pp",
+                                  "stereo_rig", "stereo_fixed"])
 @pytest.mark.parametrize("precision,tol", [(capi.PRECISION_FP64, 1e-10), (capi.PRECISION_MIXED, 2e-5)])
 def test_reduced_system_matches_oracle(orc, name, precision, tol):
     sc, g = load_golden(name)
@@ -122,7 +123,7 @@ def test_minimize_mixed_reaches_reference_cost(name):
     assert h.cost() <= target or (r.status != capi.STATUS_TIMEOUT and abs(h.cost() - float(g["cost"])) <= 1e-6 * float(g["cost"]))
 
 
-@pytest.mark.parametrize("name", ["std_circle"])
+@pytest.mark.parametrize("name", ["std_circle", "stereo_rig"])
 def test_minimize_mixed_converged_case_matches_reference(name):
     """On a case the reference drives to SMALL_UPDATE, mixed precision ends with the same status,
     the same cost (1e-6) and the same parameters (1e-5)."""

@@ -18,6 +18,7 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DEMO = os.path.join(ROOT, "tests", "shim", "_build", "shim_demo")
 ROT_DEMO = os.path.join(ROOT, "tests", "shim", "_build", "rotations_demo")
+STEREO_DEMO = os.path.join(ROOT, "tests", "shim", "_build", "stereo_demo")
 
 
 def _write_scene(path, sc, max_iterations, precision, nv):
@@ -51,7 +52,7 @@ def _read_out(path, sc):
 
 
 @pytest.mark.skipif(not os.path.exists(DEMO), reason="shim demo not built (needs the reference headers at build time)")
-@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("name", [n for n in golden_names() if not n.startswith("stereo")])
 def test_dropin_header_matches_reference(name):
     sc, g = load_golden(name)
     nv = tuple(int(v) for v in g["nonvarying"])
@@ -87,4 +88,32 @@ def test_rotation_header_matches_reference(name):
     assert struct.unpack_from("<i", b, 0)[0] == capi.OK
     R = np.frombuffer(b, dtype=np.float64, offset=4).reshape(-1, 3, 3)
     assert np.abs(R - g["R"]).max() < 1e-5
+
+
+@pytest.mark.skipif(not os.path.exists(STEREO_DEMO), reason="stereo demo not built (needs the reference headers at build time)")
+@pytest.mark.parametrize("name", [n for n in golden_names() if n.startswith("stereo")])
+def test_stereo_header_matches_reference(name):
+    """include/v3d_b200/v3d_stereobundle.h driven the way the reference's rig adjuster is
+    constructed and minimised gives the reference's status, iterations and parameters."""
+    sc, g = load_golden(name)
+    nv = tuple(int(v) for v in g["nonvarying"])
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "scene.bin"), os.path.join(d, "out.bin")
+        with open(sp, "wb") as f:
+            f.write(struct.pack("<8i", sc.n_cams, sc.n_points, sc.n_obs, sc.n_rig, int(g["max_iterations"]),
+                                capi.PRECISION_FP64, nv[0], nv[1]))
+            f.write(struct.pack("<d", sc.inlier_threshold))
+            for a in (sc.R, sc.T, sc.X, sc.meas, sc.rig_K, sc.rig_R, sc.rig_T):
+                f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+            for a in (sc.view, sc.point, sc.sub):
+                f.write(np.ascontiguousarray(a, dtype=np.int32).tobytes())
+        r = subprocess.run([STEREO_DEMO, sp, op], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        b = open(op, "rb").read()
+    status, iters = struct.unpack_from("<2i", b, 0)
+    N, M = sc.n_cams, sc.n_points
+    vals = np.frombuffer(b, dtype=np.float64, offset=8)
+    R, T, X = vals[:9 * N].reshape(N, 3, 3), vals[9 * N:12 * N].reshape(N, 3), vals[12 * N:].reshape(M, 3)
+    assert status == int(g["status"]) and iters == int(g["iterations"])
+    assert param_rel((R, T, X), (g["R"], g["T"], g["X"])) < 1e-5
 

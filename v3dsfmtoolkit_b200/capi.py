@@ -17,6 +17,7 @@ OK = 0
 (ERR_INVALID_ARGUMENT, ERR_INVALID_INPUT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NO_DEVICE, ERR_UNSUPPORTED, ERR_TIMEOUT,
  ERR_NUMERICAL) = range(1, 9)
 STATUS_TIMEOUT, STATUS_SMALL_UPDATE, STATUS_CONVERGED = 0, 1, 2
+MODEL_STD, MODEL_COMMON, MODEL_VARYING, MODEL_STEREO = 0, 1, 2, 3
 PRECISION_MIXED, PRECISION_FP64 = 0, 1
 SOLVER_AUTO, SOLVER_CHOLESKY, SOLVER_PCG = 0, 1, 2
 PRECOND_BLOCK_JACOBI, PRECOND_LEARNED, PRECOND_GAUGE = 0, 1, 2
@@ -52,7 +53,8 @@ STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "poin
 class Problem(C.Structure):
     _fields_ = [("model", C.c_int), ("mode", C.c_int), ("n_cameras", C.c_int), ("n_points", C.c_int),
                 ("n_measurements", C.c_int), ("inlier_threshold", C.c_double), ("K", _dp), ("R", _dp),
-                ("T", _dp), ("dist", _dp), ("X", _dp), ("measurements", _dp), ("view", _ip), ("point", _ip)]
+                ("T", _dp), ("dist", _dp), ("X", _dp), ("measurements", _dp), ("view", _ip), ("point", _ip),
+                ("n_rig_cameras", C.c_int), ("rig_K", _dp), ("rig_R", _dp), ("rig_T", _dp), ("subcamera", _ip)]
 
 
 class Options(C.Structure):
@@ -199,7 +201,8 @@ def launch_count() -> int:
 class Handle:
     """One problem resident on the GPU (wraps v3dba_create / v3dba_destroy)."""
 
-    def __init__(self, model, mode, inlier_threshold, K, R, T, dist, X, measurements, view, point):
+    def __init__(self, model, mode, inlier_threshold, K, R, T, dist, X, measurements, view, point,
+                 rig_K=None, rig_R=None, rig_T=None, subcamera=None):
         L = _lib()
         self._keep = [_f64(K), _f64(R), _f64(T), _f64(dist if dist is not None else np.zeros(4)), _f64(X),
                       _f64(measurements), np.ascontiguousarray(view, dtype=np.int32),
@@ -210,6 +213,12 @@ class Handle:
         self.shapes = (K_.shape, R_.shape, T_.shape, d_.shape, X_.shape)
         prob = Problem(self.model, self.mode, self.n_cams, self.n_points, self.n_obs, float(inlier_threshold),
                        _d(K_), _d(R_), _d(T_), _d(d_), _d(X_), _d(m_), v_.ctypes.data_as(_ip), p_.ctypes.data_as(_ip))
+        if rig_K is not None:
+            rig = [_f64(rig_K), _f64(rig_R), _f64(rig_T), np.ascontiguousarray(subcamera, dtype=np.int32)]
+            self._keep += rig
+            prob.n_rig_cameras = rig[0].size // 9
+            prob.rig_K, prob.rig_R, prob.rig_T = _d(rig[0]), _d(rig[1]), _d(rig[2])
+            prob.subcamera = rig[3].ctypes.data_as(_ip)
         h = C.c_void_p()
         check(L.v3dba_create(C.byref(prob), C.byref(h)), "v3dba_create")
         self.h = h
@@ -217,7 +226,9 @@ class Handle:
 
     @classmethod
     def from_scene(cls, sc):
-        return cls(sc.model, sc.mode, sc.inlier_threshold, sc.K, sc.R, sc.T, sc.dist, sc.X, sc.meas, sc.view, sc.point)
+        return cls(sc.model, sc.mode, sc.inlier_threshold, sc.K, sc.R, sc.T, sc.dist, sc.X, sc.meas, sc.view, sc.point,
+                   getattr(sc, "rig_K", None), getattr(sc, "rig_R", None), getattr(sc, "rig_T", None),
+                   getattr(sc, "sub", None))
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -23,6 +23,7 @@ __global__ void __launch_bounds__(128) k_raw_linearize(DevState s, double* e, do
   const int i = s.o_cam[k], j = s.o_pt[k], o = s.o_orig[k];
   Cam cam;
   load_cam<MODEL>(cam, s.cur.R, s.cur.T, s.cur.K, s.cur.dist, i);
+  if (MODEL == kModelStereo) load_rig(cam, s.rig, s.o_sub[k]);
   const double X[3] = {s.cur.X[3 * j], s.cur.X[3 * j + 1], s.cur.X[3 * j + 2]};
   double ee[2], a[2][DA], b[2][3], c[2][DCc];
   linearize_obs<MODEL, DA, DC>(cam, X, s.o_meas[2 * k], s.o_meas[2 * k + 1], D.mode, D.cached_ar, ee, a, b, c);
@@ -40,6 +41,7 @@ int launch_raw_linearize(DevState& s, double* e, double* w, double* A, double* B
   const Dims& D = s.d;
 #define RL(M_, A_, C_) k_raw_linearize<M_, A_, C_><<<g, 128, 0, st>>>(s, e, w, A, B, C)
   if (D.model == kModelStd) RL(kModelStd, 6, 0);
+  else if (D.model == kModelStereo) RL(kModelStereo, 6, 0);
   else if (D.model == kModelCommon) {
     switch (D.DC) {
       case 0: RL(kModelCommon, 6, 0); break;

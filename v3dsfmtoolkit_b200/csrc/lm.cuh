@@ -9,6 +9,8 @@
 
 namespace v3dba {
 
+constexpr int kRigStride = 24;   // doubles per rig camera: K 9, R 9, T 3, padding
+
 struct ParamSet {
   double* K = nullptr;     // STD/VARYING: N*9, COMMON: 9
   double* R = nullptr;     // N*9
@@ -39,6 +41,8 @@ struct DevState {
   int* p_ptr = nullptr;     // [M+1] track of point j = [p_ptr[j], p_ptr[j+1])
   int* c_ptr = nullptr;     // [N+1]
   int* c_obs = nullptr;     // [K] permuted observation ids grouped by camera
+  int* o_sub = nullptr;     // [K] rig camera of permuted observation k (STEREO)
+  double* rig = nullptr;    // [n_rig][kRigStride] rig cameras K (9), R (9), T (3) (STEREO)
   int nb = 0;               // camera-pair blocks (i <= l) with at least one shared point
   int* b_i = nullptr;
   int* b_l = nullptr;

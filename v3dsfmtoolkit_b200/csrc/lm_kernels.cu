@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
       const bool fixA = i < D.nnA;
       Cam cam;
       load_cam<MODEL>(cam, s.cur.R, s.cur.T, s.cur.K, s.cur.dist, i);
+      if (MODEL == kModelStereo) load_rig(cam, s.rig, s.o_sub[k]);
       double e[2], A[2][DA], B[2][3], C[2][DCc];
       linearize_obs<MODEL, DA, DC>(cam, X, s.o_meas[2 * k], s.o_meas[2 * k + 1], D.mode, D.cached_ar, e, A, B, C);
       const double w = huber_weight(D.thr, e);
@@ -789,7 +790,7 @@ __global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __res
     for (int t = 0; t < 3; ++t) T[t] = s.cur.T[3 * i + t];
     double K[9];
     double dist[4] = {0, 0, 0, 0};
-    if (MODEL != kModelCommon) {
+    if (MODEL == kModelStd || MODEL == kModelVarying) {   // per-camera K (STEREO has none)
 #pragma unroll
       for (int t = 0; t < 9; ++t) K[t] = s.cur.K[9 * i + t];
     }
@@ -818,7 +819,7 @@ __global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __res
     for (int t = 0; t < 9; ++t) s.trial.R[9 * i + t] = R[t];
 #pragma unroll
     for (int t = 0; t < 3; ++t) s.trial.T[3 * i + t] = T[t];
-    if (MODEL != kModelCommon) {
+    if (MODEL == kModelStd || MODEL == kModelVarying) {
 #pragma unroll
       for (int t = 0; t < 9; ++t) s.trial.K[9 * i + t] = K[t];
     }
@@ -863,6 +864,7 @@ __global__ void __launch_bounds__(256) k_obs_cost(DevState s, ParamSet P, int re
     const int i = s.o_cam[k], j = s.o_pt[k];
     Cam cam;
     load_cam<MODEL>(cam, P.R, P.T, P.K, P.dist, i);
+    if (MODEL == kModelStereo) load_rig(cam, s.rig, s.o_sub[k]);
     const double X[3] = {P.X[3 * j], P.X[3 * j + 1], P.X[3 * j + 2]};
     double XX[3], e[2];
     residual<MODEL>(cam, X, s.o_meas[2 * k], s.o_meas[2 * k + 1], XX, e);
@@ -1034,6 +1036,7 @@ size_t partial_doubles(const DevState& s) {
 template <typename Real>
 const LmOps* ops_for(int model, int DA, int DC) {
   if (model == kModelStd) return DA == 6 && DC == 0 ? Ops<kModelStd, 6, 0, Real>::table() : nullptr;
+  if (model == kModelStereo) return DA == 6 && DC == 0 ? Ops<kModelStereo, 6, 0, Real>::table() : nullptr;
   if (model == kModelCommon) {
     if (DA != 6) return nullptr;
     switch (DC) {

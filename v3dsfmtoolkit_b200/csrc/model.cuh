@@ -8,6 +8,10 @@
 //             v3d_metricbundle.cpp:102-178)
 //   VARYING : VaryingInternalsMetricBundleOptimizer (v3d_metricbundle.h:275-291,
 //             v3d_metricbundle.cpp:216-296)
+//   STEREO  : StereoMetricBundleOptimizer (V3D/include/Geometry/v3d_stereobundle.h:66-80,
+//             V3D/src/Geometry/v3d_stereobundle.cpp:11-67): the rig pose (R, T) moves the point
+//             into rig space, rig camera l (K_l, R_l, T_l) projects it like STD; the Jacobian
+//             is the STD one of camera l composed with R_l (f and aspect ratio of K_l).
 // with the Brown distortion of V3D/include/Geometry/v3d_distortion.h:18-72.
 //
 // The Jacobian is d e / d p for e = proj - m.  Camera columns are (T, omega) first, then for
@@ -21,7 +25,7 @@
 
 namespace v3dba {
 
-enum { kModelStd = 0, kModelCommon = 1, kModelVarying = 2 };
+enum { kModelStd = 0, kModelCommon = 1, kModelVarying = 2, kModelStereo = 3 };
 
 __host__ __device__ constexpr int intrinsic_dim(int mode) {
   return mode == 1 ? 1 : mode == 2 ? 3 : mode == 3 ? 5 : mode == 4 ? 7 : 0;
@@ -30,8 +34,9 @@ __host__ __device__ constexpr int intrinsic_dim(int mode) {
 // Camera parameters gathered for one observation.
 struct Cam {
   double R[9], T[3];
-  double K[9];                      // intrinsics, row-major (STD uses all of K)
+  double K[9];                      // intrinsics, row-major (STD uses all of K; STEREO: K_l)
   double d[4];                      // k1 k2 p1 p2
+  double Rl[9], Tl[3];              // STEREO: pose of the rig camera on the rig
 };
 
 template <int MODEL>
@@ -42,10 +47,12 @@ __device__ __forceinline__ void load_cam(Cam& c, const double* __restrict__ R, c
   for (int t = 0; t < 9; ++t) c.R[t] = __ldg(R + 9 * i + t);
 #pragma unroll
   for (int t = 0; t < 3; ++t) c.T[t] = __ldg(T + 3 * i + t);
-  const double* k = (MODEL == kModelCommon) ? K : K + 9 * i;
+  if (MODEL != kModelStereo) {   // STEREO takes K from the rig camera (load_rig)
+    const double* k = (MODEL == kModelCommon) ? K : K + 9 * i;
 #pragma unroll
-  for (int t = 0; t < 9; ++t) c.K[t] = __ldg(k + t);
-  if (MODEL != kModelStd) {
+    for (int t = 0; t < 9; ++t) c.K[t] = __ldg(k + t);
+  }
+  if (MODEL == kModelCommon || MODEL == kModelVarying) {
     const double* dd = (MODEL == kModelCommon) ? dist : dist + 4 * i;
 #pragma unroll
     for (int t = 0; t < 4; ++t) c.d[t] = __ldg(dd + t);
@@ -54,13 +61,29 @@ __device__ __forceinline__ void load_cam(Cam& c, const double* __restrict__ R, c
   }
 }
 
+// Rig camera l of a STEREO observation: K_l, R_l, T_l from rig[l * 24 ...] (K 9, R 9, T 3).
+__device__ __forceinline__ void load_rig(Cam& c, const double* __restrict__ rig, int l) {
+  const double* r = rig + 24 * (size_t)l;
+#pragma unroll
+  for (int t = 0; t < 9; ++t) c.K[t] = __ldg(r + t);
+#pragma unroll
+  for (int t = 0; t < 9; ++t) c.Rl[t] = __ldg(r + 9 + t);
+#pragma unroll
+  for (int t = 0; t < 3; ++t) c.Tl[t] = __ldg(r + 18 + t);
+}
+
 // e = proj(X) - m.  Returns the camera-space point in XX.
 template <int MODEL>
 __device__ __forceinline__ void residual(const Cam& c, const double X[3], double mx, double my,
                                          double XX[3], double e[2]) {
 #pragma unroll
   for (int r = 0; r < 3; ++r) XX[r] = c.R[3 * r] * X[0] + c.R[3 * r + 1] * X[1] + c.R[3 * r + 2] * X[2] + c.T[r];
-  if (MODEL == kModelStd) {
+  if (MODEL == kModelStereo) {   // into the rig camera: R_l Y + T_l
+    double Y[3] = {XX[0], XX[1], XX[2]};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) XX[r] = c.Rl[3 * r] * Y[0] + c.Rl[3 * r + 1] * Y[1] + c.Rl[3 * r + 2] * Y[2] + c.Tl[r];
+  }
+  if (MODEL == kModelStd || MODEL == kModelStereo) {
     // K (R X + T) dehomogenised, with the full 3x3 K
     const double h0 = c.K[0] * XX[0] + c.K[1] * XX[1] + c.K[2] * XX[2];
     const double h1 = c.K[3] * XX[0] + c.K[4] * XX[1] + c.K[5] * XX[2];
@@ -87,18 +110,34 @@ __device__ __forceinline__ void linearize_obs(const Cam& c, const double X[3], d
   double XX[3];
   residual<MODEL>(c, X, mx, my, XX, e);
 
-  // d XX / d (T, omega) = [ I | -[R X]_x ],  d XX / d X = R  (R X recovered as XX - T)
-  const double v0 = XX[0] - c.T[0], v1 = XX[1] - c.T[1], v2 = XX[2] - c.T[2];
+  // d XX / d (T, omega) = [ I | -[R X]_x ],  d XX / d X = R  (R X recovered as XX - T); STEREO
+  // composes both with R_l (the pose moves the point in rig space)
+  double v0, v1, v2;
+  if (MODEL == kModelStereo) {
+    v0 = c.R[0] * X[0] + c.R[1] * X[1] + c.R[2] * X[2];
+    v1 = c.R[3] * X[0] + c.R[4] * X[1] + c.R[5] * X[2];
+    v2 = c.R[6] * X[0] + c.R[7] * X[1] + c.R[8] * X[2];
+  } else {
+    v0 = XX[0] - c.T[0]; v1 = XX[1] - c.T[1]; v2 = XX[2] - c.T[2];
+  }
   const double iz = 1.0 / XX[2];
 
-  double P[2][3];  // d proj / d XX
+  double P[2][3];  // d proj / d XX (STEREO: d proj / d Y = d proj / d XX * R_l)
   double fx, fy, ux = 0.0, uy = 0.0, xd = 0.0, yd = 0.0;
-  if (MODEL == kModelStd) {
+  if (MODEL == kModelStd || MODEL == kModelStereo) {
     const double f = c.K[0], ar = c.K[4] / c.K[0];
     const double bx = f / (XX[2] * XX[2]), by = ar * bx;
     P[0][0] = bx * XX[2]; P[0][1] = 0.0;        P[0][2] = -bx * XX[0];
     P[1][0] = 0.0;        P[1][1] = by * XX[2]; P[1][2] = -by * XX[1];
     fx = f; fy = ar * f;
+    if (MODEL == kModelStereo) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const double p0 = P[r][0], p1 = P[r][1], p2 = P[r][2];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) P[r][q] = p0 * c.Rl[q] + p1 * c.Rl[3 + q] + p2 * c.Rl[6 + q];
+      }
+    }
   } else {
     const double f = c.K[0];
     const double ar = (MODEL == kModelCommon) ? cached_ar : c.K[4] / c.K[0];
@@ -120,7 +159,7 @@ __device__ __forceinline__ void linearize_obs(const Cam& c, const double X[3], d
     P[1][0] = a10 * iz; P[1][1] = a11 * iz; P[1][2] = a10 * dx2 + a11 * dy2;
   }
 
-  const bool no_trans = (MODEL != kModelStd) && (mode == -1);
+  const bool no_trans = (MODEL == kModelCommon || MODEL == kModelVarying) && (mode == -1);
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     // translation columns: P * I
@@ -136,7 +175,7 @@ __device__ __forceinline__ void linearize_obs(const Cam& c, const double X[3], d
       B[r][q] = P[r][0] * c.R[q] + P[r][1] * c.R[3 + q] + P[r][2] * c.R[6 + q];
   }
 
-  if (MODEL != kModelStd) {
+  if (MODEL == kModelCommon || MODEL == kModelVarying) {
     const int nint = intrinsic_dim(mode);
     // intrinsic columns [f, cx, cy, k1, k2, p1, p2]
     double G[2][7];

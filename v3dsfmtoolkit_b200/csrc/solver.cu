@@ -64,7 +64,12 @@ struct v3dba_handle_s {
 namespace {
 
 int dims_of(int model, int mode, int* dA, int* dC) {
-  if (model < V3DBA_MODEL_STD || model > V3DBA_MODEL_VARYING) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (model < V3DBA_MODEL_STD || model > V3DBA_MODEL_STEREO) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (model == V3DBA_MODEL_STEREO) {   // rig pose (T, omega); intrinsics fixed on the rig cameras
+    *dA = 6;
+    *dC = 0;
+    return V3DBA_OK;
+  }
   if (model != V3DBA_MODEL_STD &&
       (mode < V3DBA_FULL_BUNDLE_NO_ROTATIONS || mode > V3DBA_FULL_BUNDLE_RADIAL_TANGENTIAL))
     return V3DBA_ERR_INVALID_ARGUMENT;
@@ -103,7 +108,7 @@ int alloc_params(v3dba_handle h, ParamSet& P, int N, int M) {
 
 int copy_params(const ParamSet& dst, const ParamSet& src, const v3dba_handle h, cudaStream_t st) {
   const Dims& D = h->s.d;
-  V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.K, src.K, sizeof(double) * h->nK, cudaMemcpyDeviceToDevice, st));
+  if (h->nK) V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.K, src.K, sizeof(double) * h->nK, cudaMemcpyDeviceToDevice, st));
   V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.R, src.R, sizeof(double) * 9 * D.N, cudaMemcpyDeviceToDevice, st));
   V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.T, src.T, sizeof(double) * 3 * D.N, cudaMemcpyDeviceToDevice, st));
   if (h->nD) V3DBA_CUDA_TRY(cudaMemcpyAsync(dst.dist, src.dist, sizeof(double) * h->nD, cudaMemcpyDeviceToDevice, st));
@@ -115,7 +120,7 @@ int upload_params(v3dba_handle h, const ParamSet& P, const double* K, const doub
                   const double* dist, const double* X) {
   const Dims& D = h->s.d;
   cudaStream_t st = h->stream;
-  V3DBA_CUDA_TRY(cudaMemcpyAsync(P.K, K, sizeof(double) * h->nK, cudaMemcpyHostToDevice, st));
+  if (h->nK) V3DBA_CUDA_TRY(cudaMemcpyAsync(P.K, K, sizeof(double) * h->nK, cudaMemcpyHostToDevice, st));
   V3DBA_CUDA_TRY(cudaMemcpyAsync(P.R, R, sizeof(double) * 9 * D.N, cudaMemcpyHostToDevice, st));
   V3DBA_CUDA_TRY(cudaMemcpyAsync(P.T, T, sizeof(double) * 3 * D.N, cudaMemcpyHostToDevice, st));
   if (h->nD) V3DBA_CUDA_TRY(cudaMemcpyAsync(P.dist, dist, sizeof(double) * h->nD, cudaMemcpyHostToDevice, st));
@@ -224,6 +229,12 @@ struct CreateTrace {
   }
 };
 
+// o_sub[k] = subcamera of the caller's observation o_orig[k] (point-major order)
+__global__ void k_gather_sub(const int* __restrict__ sub, const int* __restrict__ orig, int K, int* __restrict__ out) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k < K) out[k] = sub[orig[k]];
+}
+
 // Work chunks over the camera observation lists and the camera-pair blocks: long lists are cut
 // into chunks of 64 observations / 128 pairs, one warp per chunk.
 struct Chunks {
@@ -303,16 +314,31 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   int rc = dims_of(p->model, p->mode, &dA, &dC);
   if (rc) return rc;
   const int N = p->n_cameras, M = p->n_points, K = p->n_measurements;
+  const bool stereo = p->model == V3DBA_MODEL_STEREO;
   if (N < 0 || M < 0 || K < 0) return V3DBA_ERR_INVALID_ARGUMENT;
-  if ((N > 0 && (!p->R || !p->T || !p->K)) || (M > 0 && !p->X) ||
+  if ((N > 0 && (!p->R || !p->T || (!stereo && !p->K))) || (M > 0 && !p->X) ||
       (K > 0 && (!p->measurements || !p->view || !p->point)))
     return V3DBA_ERR_INVALID_ARGUMENT;
   if (p->model == V3DBA_MODEL_COMMON && !p->K) return V3DBA_ERR_INVALID_ARGUMENT;
-  if (p->model != V3DBA_MODEL_STD && !p->dist) return V3DBA_ERR_INVALID_ARGUMENT;
+  if ((p->model == V3DBA_MODEL_COMMON || p->model == V3DBA_MODEL_VARYING) && !p->dist)
+    return V3DBA_ERR_INVALID_ARGUMENT;
+  const int nrig = stereo ? p->n_rig_cameras : 0;
+  if (stereo) {
+    if (nrig < 0 || (K > 0 && (nrig == 0 || !p->subcamera)) ||
+        (nrig > 0 && (!p->rig_K || !p->rig_R || !p->rig_T)))
+      return V3DBA_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < K; ++k)
+      if (p->subcamera[k] < 0 || p->subcamera[k] >= nrig) return V3DBA_ERR_INVALID_INPUT;
+    if (!all_finite(p->rig_K, (size_t)9 * nrig) || !all_finite(p->rig_R, (size_t)9 * nrig) ||
+        !all_finite(p->rig_T, (size_t)3 * nrig))
+      return V3DBA_ERR_INVALID_INPUT;
+    for (int l = 0; l < nrig; ++l)
+      if (p->rig_K[9 * l] == 0.0) return V3DBA_ERR_INVALID_INPUT;   // f divides the aspect ratio
+  }
   if (!(p->inlier_threshold > 0.0) || !std::isfinite(p->inlier_threshold)) return V3DBA_ERR_INVALID_INPUT;
   for (int k = 0; k < K; ++k)
     if (p->view[k] < 0 || p->view[k] >= N || p->point[k] < 0 || p->point[k] >= M) return V3DBA_ERR_INVALID_INPUT;
-  const size_t nK = (p->model == V3DBA_MODEL_COMMON) ? 9 : (size_t)9 * N;
+  const size_t nK = stereo ? 0 : (p->model == V3DBA_MODEL_COMMON) ? 9 : (size_t)9 * N;
   const size_t nD = (p->model == V3DBA_MODEL_COMMON) ? 4 : (p->model == V3DBA_MODEL_VARYING ? (size_t)4 * N : 0);
   if (!all_finite(p->K, nK) || !all_finite(p->R, (size_t)9 * N) || !all_finite(p->T, (size_t)3 * N) ||
       !all_finite(p->X, (size_t)3 * M) || !all_finite(p->measurements, (size_t)2 * K) ||
@@ -334,7 +360,7 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   DevState& s = h->s;
   Dims& D = s.d;
   D.N = N; D.M = M; D.K = K; D.DA = dA; D.DC = dC;
-  D.model = p->model; D.mode = (p->model == V3DBA_MODEL_STD) ? 0 : p->mode;
+  D.model = p->model; D.mode = (p->model == V3DBA_MODEL_STD || stereo) ? 0 : p->mode;
   D.thr = p->inlier_threshold;
   D.cached_ar = (p->model == V3DBA_MODEL_COMMON) ? p->K[4] / p->K[0] : 1.0;
 
@@ -373,6 +399,25 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   s.b_ptr = ds.b_ptr;
   s.pr_k = ds.pr_k;
   s.pr_m = ds.pr_m;
+  if (stereo) {   // rig cameras, and the rig camera of every point-major observation
+    std::vector<double> rig((size_t)std::max(nrig, 1) * kRigStride, 0.0);
+    for (int l = 0; l < nrig; ++l) {
+      std::memcpy(&rig[(size_t)l * kRigStride], p->rig_K + 9 * l, 9 * sizeof(double));
+      std::memcpy(&rig[(size_t)l * kRigStride + 9], p->rig_R + 9 * l, 9 * sizeof(double));
+      std::memcpy(&rig[(size_t)l * kRigStride + 18], p->rig_T + 3 * l, 3 * sizeof(double));
+    }
+    TRY(upload(h, &s.rig, rig));
+    int* sub_in;
+    TRY(dalloc(h, &sub_in, (size_t)std::max(K, 1)));
+    TRY(dalloc(h, &s.o_sub, (size_t)std::max(K, 1)));
+    if (K > 0) {
+      CTRY(cudaMemcpyAsync(sub_in, p->subcamera, sizeof(int) * K, cudaMemcpyHostToDevice, h->stream));
+      k_gather_sub<<<(K + 255) / 256, 256, 0, h->stream>>>(sub_in, s.o_orig, K, s.o_sub);
+      note_launches(1);
+      CTRY(cudaPeekAtLastError());
+    }
+    CTRY(cudaStreamSynchronize(h->stream));   // `rig` must outlive its copy
+  }
   trace.mark("structure", h->stream);
   Chunks st;
   build_chunks(ds.h_c_ptr, ds.h_b_ptr, N, st);
@@ -478,7 +523,7 @@ int v3dba_set_lambda(v3dba_handle h, double lambda) {
 
 int v3dba_set_params(v3dba_handle h, const double* K, const double* R, const double* T, const double* dist,
                      const double* X) {
-  if (!h || !K || !R || !T || !X || (h->nD && !dist)) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (!h || (h->nK && !K) || !R || !T || !X || (h->nD && !dist)) return V3DBA_ERR_INVALID_ARGUMENT;
   return upload_params(h, h->s.cur, K, R, T, dist, X);
 }
 
@@ -487,7 +532,7 @@ int v3dba_get_params(v3dba_handle h, double* K, double* R, double* T, double* di
   const Dims& D = h->s.d;
   const ParamSet& P = h->s.cur;
   cudaStream_t st = h->stream;
-  if (K) V3DBA_CUDA_TRY(cudaMemcpyAsync(K, P.K, sizeof(double) * h->nK, cudaMemcpyDeviceToHost, st));
+  if (K && h->nK) V3DBA_CUDA_TRY(cudaMemcpyAsync(K, P.K, sizeof(double) * h->nK, cudaMemcpyDeviceToHost, st));
   if (R) V3DBA_CUDA_TRY(cudaMemcpyAsync(R, P.R, sizeof(double) * 9 * D.N, cudaMemcpyDeviceToHost, st));
   if (T) V3DBA_CUDA_TRY(cudaMemcpyAsync(T, P.T, sizeof(double) * 3 * D.N, cudaMemcpyDeviceToHost, st));
   if (dist && h->nD) V3DBA_CUDA_TRY(cudaMemcpyAsync(dist, P.dist, sizeof(double) * h->nD, cudaMemcpyDeviceToHost, st));

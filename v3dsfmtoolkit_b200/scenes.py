@@ -12,6 +12,7 @@ Workloads:
                                50,000 points, tracks of 3-12 consecutive views, 2% outliers
   * :func:`triplet_batch`   -- thousands of independent 3-camera problems of uneven size
   * :func:`cluster_scene`   -- 2,000 cameras in 20 groups, 1M points, ~6M observations
+  * :func:`stereo_rig_scene` -- a binocular rig along a path (StereoMetricBundleOptimizer)
   * :func:`rotation_graph`  -- view graphs for rotation averaging (refineConsistentRotations)
 """
 from __future__ import annotations
@@ -21,7 +22,7 @@ import math
 
 import numpy as np
 
-MODEL_STD, MODEL_COMMON, MODEL_VARYING = 0, 1, 2
+MODEL_STD, MODEL_COMMON, MODEL_VARYING, MODEL_STEREO = 0, 1, 2, 3
 FULL_BUNDLE_NO_ROTATIONS, FULL_BUNDLE_METRIC, FULL_BUNDLE_FOCAL_LENGTH = -1, 0, 1
 FULL_BUNDLE_FOCAL_LENGTH_PP, FULL_BUNDLE_RADIAL, FULL_BUNDLE_RADIAL_TANGENTIAL = 2, 3, 4
 
@@ -44,6 +45,11 @@ class Scene:
     point: np.ndarray      # (K,) int32
     dist: np.ndarray | None = None   # (4,) shared or (N,4)
     name: str = ""
+    # MODEL_STEREO: R / T are rig poses; the L fixed rig cameras and each observation's camera
+    rig_K: np.ndarray | None = None  # (L,3,3)
+    rig_R: np.ndarray | None = None  # (L,3,3)
+    rig_T: np.ndarray | None = None  # (L,3)
+    sub: np.ndarray | None = None    # (K,) int32
 
     @property
     def n_cams(self) -> int:
@@ -68,6 +74,10 @@ class Scene:
             self, K=self.K.copy(), R=self.R.copy(), T=self.T.copy(), X=self.X.copy(),
             meas=self.meas.copy(), view=self.view.copy(), point=self.point.copy(),
             dist=None if self.dist is None else self.dist.copy())
+
+    @property
+    def n_rig(self) -> int:
+        return 0 if self.rig_K is None else int(self.rig_K.shape[0])
 
     def params(self):
         """(K, R, T, dist, X) as contiguous float64 arrays (dist is a 1-element dummy for STD)."""
@@ -443,4 +453,62 @@ def rotation_graph(n_views=2000, n_pairs=40000, window=5, noise_deg=1.0, init_de
     R0 = R_true @ rodrigues(rng.normal(scale=math.radians(init_deg), size=(n_views, 3)))
     return RotationGraph(np.ascontiguousarray(rel), np.ascontiguousarray(pairs), np.ascontiguousarray(R0),
                          R_true, name=f"rotations{n_views}x{len(pairs)}")
+
+
+def stereo_rig_scene(n_poses=30, n_points=3000, baseline=0.3, seed=0, noise_px=0.5, outlier_frac=0.0,
+                     inlier_threshold=2.0, rot_perturb=0.01, trans_perturb=0.02, point_perturb=0.05,
+                     window=4) -> Scene:
+    """Rig BA (StereoMetricBundleOptimizer): a binocular rig (camera 0 at the rig origin, camera 1
+    ``baseline`` to its right and toed in by 2 degrees, slightly different intrinsics, 640x480)
+    moving forward along a gently curving path; points in a corridor ahead; every point is seen
+    from up to ``window`` consecutive rig poses, by each rig camera in which it projects inside
+    the image (N(0, noise_px) pixel noise, ``outlier_frac`` gross outliers).  The poses are
+    perturbed by ``rot_perturb`` rad / N(0, trans_perturb) and the points by N(0, point_perturb);
+    Huber threshold ``inlier_threshold`` px."""
+    rng = np.random.default_rng(seed)
+    rig_K = np.stack([_intrinsics(700.0, 320.0, 240.0), _intrinsics(705.0, 318.0, 242.0)])
+    rig_R = np.stack([np.eye(3), rodrigues(np.array([0.0, math.radians(-2.0), 0.0]))])
+    rig_T = np.stack([np.zeros(3), -rig_R[1] @ np.array([baseline, 0.0, 0.0])])
+    # rig centres along z with a slow sway; the rig looks along +z (world -> rig: Y = R X + T)
+    t = np.arange(n_poses, dtype=np.float64)
+    centers = np.stack([0.5 * np.sin(0.15 * t), 0.1 * np.cos(0.2 * t), 0.8 * t], axis=1)
+    yaw = 0.05 * np.sin(0.1 * t)
+    R = rodrigues(np.stack([np.zeros(n_poses), yaw, np.zeros(n_poses)], axis=1))
+    T = -np.einsum("nij,nj->ni", R, centers)
+    X = np.stack([rng.uniform(-4, 4, n_points), rng.uniform(-3, 3, n_points),
+                  rng.uniform(3.0, 0.8 * n_poses + 12.0, n_points)], axis=1)
+    views, points, subs, meas, keep = [], [], [], [], []
+    for j in range(n_points):
+        first = int(np.clip(np.floor((X[j, 2] - 12.0) / 0.8), 0, n_poses - 1))
+        obs = []
+        for i in range(first, min(n_poses, first + window)):
+            Y = R[i] @ X[j] + T[i]
+            for l in range(2):
+                Z = rig_R[l] @ Y + rig_T[l]
+                if Z[2] <= 0.5:
+                    continue
+                h = rig_K[l] @ Z
+                q = h[:2] / h[2]
+                if 0 <= q[0] < 640 and 0 <= q[1] < 480:
+                    obs.append((i, l, q))
+        if len(obs) < 3:
+            continue
+        for i, l, q in obs:
+            views.append(i)
+            points.append(len(keep))
+            subs.append(l)
+            meas.append(q + rng.normal(scale=noise_px, size=2))
+        keep.append(j)
+    meas = np.asarray(meas, dtype=np.float64)
+    n_out = int(round(outlier_frac * len(meas)))
+    if n_out:
+        sel = rng.choice(len(meas), size=n_out, replace=False)
+        meas[sel] += rng.normal(scale=30.0, size=(n_out, 2))
+    X = X[keep]
+    R0, T0 = _perturb_cameras(rng, R, T, rot_perturb, trans_perturb)
+    X0 = X + rng.normal(scale=point_perturb, size=X.shape)
+    return Scene(MODEL_STEREO, FULL_BUNDLE_METRIC, inlier_threshold, np.zeros((1, 3, 3)), R0, T0, X0, meas,
+                 np.asarray(views, dtype=np.int32), np.asarray(points, dtype=np.int32), None,
+                 name=f"stereo{n_poses}x{len(keep)}", rig_K=rig_K, rig_R=rig_R, rig_T=rig_T,
+                 sub=np.asarray(subs, dtype=np.int32))
 
