@@ -25,6 +25,8 @@
  *   v3dba_minimize_batched <- the sequential loop of independent triplet / submodel adjustments
  *                             (SfM/generate_triples/src/generate_triples.cpp:403-415,
  *                              SfM/generate_submodels_L1/src/generate_submodels_L1.cpp:330-337)
+ *   v3dba_triplet_stage    <- the triplet stage around that adjustment: triangulation, filtering,
+ *                             survival tests, BA (generate_triples.cpp:380-415)
  *
  * Conventions: plain pointers and sizes, row-major doubles, 0-based indices, no exceptions.
  * Every entry point returns an int error code (V3DBA_OK == 0).  The reference's convergence
@@ -237,6 +239,63 @@ int v3dba_dense_cholesky_solve_noalloc(int n, const double* S, const double* rhs
 int v3dba_minimize_batched(const v3dba_problem* problems, int count, const v3dba_options* opts,
                            double* const* K, double* const* R, double* const* T,
                            double* const* dist, double* const* X, v3dba_result* results);
+
+/* ---- Triplet stage (SfM/generate_triples/src/generate_triples.cpp:380-415) ----------------
+ * For every view triplet, as the reference's triplet loop does after connectTracks:
+ *   1. triangulateLinear of every track with the triple cameras (K = I; least squares by
+ *      Householder QR, V3D/include/Geometry/v3d_mviewutilities.h:260-303);
+ *   2. filterTripleModel (generate_triples.cpp:44-81): a measurement survives when
+ *      f_view * |float(project(X)) - pos| < max_reproj_error (f_view the view's average focal
+ *      length), a track when at least 3 of its measurements survive;
+ *   3. rejection when fewer than min_points tracks survive or fewer than min_point_ratio times
+ *      the track count (generate_triples.cpp:393-398);
+ *   4. StdMetricBundleOptimizer on the surviving points and measurements (inlier threshold,
+ *      tau, max_iterations; the reference uses 1.0, 1e-3, 5), cameras and points refined.
+ * All triplets of a call run on the GPU together: one launch triangulates and filters every
+ * track, one assembles the bundle problems, one persistent launch adjusts them. */
+typedef struct v3dba_triplet {
+  double R[27];                     /* the three cameras' rotations (row-major 3x3 each)   */
+  double T[9];                      /* and translations; the intrinsics are the identity   */
+  double focal[3];                  /* calibDb.getAvgFocalLength of the three views (px)   */
+  int n_tracks;
+  const int32_t* track_ptr;         /* [n_tracks+1] measurements of each track             */
+  const int32_t* view;              /* [track_ptr[n_tracks]] triple view 0, 1 or 2         */
+  const float* pos;                 /* [2*track_ptr[n_tracks]] normalised image coordinates */
+} v3dba_triplet;
+
+typedef struct v3dba_triplet_stage_options {
+  double max_reproj_error;          /* MAX_REPROJECTION_ERROR_TRIPLET (pixels), default 1.0 */
+  int min_points;                   /* REQUIRED_TRIPLET_POINTS, default 50                 */
+  double min_point_ratio;           /* MINIMUM_TRIPLET_POINT_RATIO, default 0.5            */
+  double inlier_threshold;          /* of the adjustment, default 1.0                      */
+  double tau;                       /* default 1e-3                                         */
+  int max_iterations;               /* default 5                                            */
+} v3dba_triplet_stage_options;
+
+enum {
+  V3DBA_TRIPLET_ACCEPTED = 0,
+  V3DBA_TRIPLET_TOO_FEW_POINTS = 1, /* fewer than min_points tracks survived the filter    */
+  V3DBA_TRIPLET_POINTS_DROPPED = 2  /* fewer than min_point_ratio of the tracks survived    */
+};
+
+typedef struct v3dba_triplet_result {
+  int verdict;                      /* V3DBA_TRIPLET_*                                      */
+  int n_tracks;                     /* nPointsBefore                                        */
+  int n_points;                     /* tracks that survived the filter                      */
+  int status, iterations;           /* of the adjustment (accepted triplets)                */
+  double cost;                      /* of the adjustment at its last linearisation          */
+  double R[27], T[9];               /* cameras after the adjustment (accepted triplets)     */
+} v3dba_triplet_result;
+
+void v3dba_default_triplet_stage_options(v3dba_triplet_stage_options* opts);
+
+/* results[t] for every triplet; X[t] (3 * n_tracks doubles, may be NULL) receives every
+ * track's point: refined for the surviving tracks of accepted triplets, the linear
+ * triangulation otherwise (NaN when the track's system is rank deficient); kept[t] (one byte
+ * per measurement, may be NULL) is 1 for the measurements that survived the filter.
+ * device_ms (may be NULL) receives the device time of the stage's kernels (CUDA events). */
+int v3dba_triplet_stage(const v3dba_triplet* triplets, int count, const v3dba_triplet_stage_options* opts,
+                        v3dba_triplet_result* results, double* const* X, uint8_t* const* kept, double* device_ms);
 
 /* Stages of one LM iteration (benchmark support; no counterpart in the reference). */
 enum {

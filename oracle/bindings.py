@@ -75,6 +75,10 @@ class Reference:
             [C.c_int, C.c_int, C.c_double, C.c_int, _ip, _ip, _dp, _dp, _dp, _ip, C.c_int, _ip, _ip]
         L.v3dref_linearize_stereo.restype = C.c_int
         L.v3dref_linearize_stereo.argtypes = [C.c_int] * 4 + [C.c_double] + [_dp] * 4 + [_ip] * 3 + [_dp] * 7
+        L.v3dref_triplet_stage.restype = C.c_int
+        L.v3dref_triplet_stage.argtypes = [_dp, _dp, _dp, C.c_int, _ip, _ip, C.POINTER(C.c_float), C.c_double,
+                                           C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                           _ip, _ip, _ip, _ip, _dp, _dp, _dp, _dp, C.POINTER(C.c_ubyte)]
         L.v3dref_refine_rotations.restype = C.c_int
         L.v3dref_refine_rotations.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, _dp, C.c_int, _ip]
 
@@ -154,6 +158,25 @@ class Reference:
                                     _d(_f64(dist)), _d(_f64(X)), _d(_f64(scene.meas)),
                                     _i(_i32(scene.view)), _i(_i32(scene.point)))
 
+
+    def triplet_stage(self, trip, max_reproj_error=1.0, min_points=50, min_point_ratio=0.5, inlier_threshold=1.0,
+                      tau=1e-3, max_iterations=5):
+        """The reference's triplet stage (generate_triples.cpp:380-415) on one TripletTracks."""
+        n = trip.n_tracks
+        nm = int(trip.track_ptr[-1])
+        v, ns, st, it = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        cost = C.c_double()
+        Ro, To, X = np.zeros(27), np.zeros(9), np.zeros(3 * max(n, 1))
+        kept = np.zeros(max(nm, 1), dtype=np.uint8)
+        pos = np.ascontiguousarray(trip.pos, dtype=np.float32)
+        self.lib.v3dref_triplet_stage(_d(_f64(trip.R)), _d(_f64(trip.T)), _d(_f64(trip.focal)), n,
+                                      _i(_i32(trip.track_ptr)), _i(_i32(trip.view)),
+                                      pos.ctypes.data_as(C.POINTER(C.c_float)), max_reproj_error, min_points,
+                                      min_point_ratio, inlier_threshold, tau, max_iterations, C.byref(v),
+                                      C.byref(ns), C.byref(st), C.byref(it), C.byref(cost), _d(Ro), _d(To),
+                                      _d(X), kept.ctypes.data_as(C.POINTER(C.c_ubyte)))
+        return dict(verdict=v.value, n_points=ns.value, status=st.value, iterations=it.value, cost=cost.value,
+                    R=Ro.reshape(3, 3, 3), T=To.reshape(3, 3), X=X[:3 * n].reshape(n, 3), kept=kept[:nm].copy())
 
     def refine_rotations(self, graph, rotations=None, trace_cap=512):
         """V3D::refineConsistentRotations on a copy of the graph's initial rotations; returns

@@ -10,7 +10,9 @@
 // all running V3D::SparseLevenbergOptimizer::minimize (V3D/src/Math/v3d_optimization.cpp:719-1250),
 // and the rotation averaging V3D::refineConsistentRotations (V3D/src/Geometry/
 // v3d_mviewutilities.cpp:470-613), which runs the same minimize() on SparseRotationOptimizer,
-// and V3D::StereoMetricBundleOptimizer (V3D/include/Geometry/v3d_stereobundle.h:22-163).
+// and V3D::StereoMetricBundleOptimizer (V3D/include/Geometry/v3d_stereobundle.h:22-163),
+// and the triplet stage around the triplet adjustment (SfM/generate_triples/src/
+// generate_triples.cpp:380-415).
 //
 // Parameter layout (row-major, doubles), shared with the product C-ABI:
 //   K    : model 0/2 -> nCams*9 per-camera intrinsics; model 1 -> 9 (the shared K)
@@ -442,6 +444,101 @@ int v3dref_linearize_stereo(int nPoses, int nPoints, int nObs, int nRig, double 
             if (B) for (int c = 0; c < 3; ++c) B[(2 * k + r) * 3 + c] = Bk[r][c];
          }
       }
+   }
+   return 0;
+}
+
+// The triplet stage of SfM/generate_triples/src/generate_triples.cpp:380-415 for one triplet,
+// with the reference's own triangulateLinear (V3D/include/Geometry/v3d_mviewutilities.h:296-303),
+// BundlePointStructure (:132-205) and StdMetricBundleOptimizer.  filterTripleModel
+// (generate_triples.cpp:44-81) lives in the application file, which needs the reference's
+// database layer to compile; it is restated here on the reference's own types (Vector2f,
+// norm_L2, CameraMatrix::projectPoint), so its float arithmetic is the reference's.
+// Outputs: verdict (0 accepted, 1 too few points, 2 too many dropped), surviving track count,
+// the adjustment's status / iterations / last relinearisation cost, cameras after it, every
+// track's point (refined for surviving tracks of accepted triplets, else the triangulation) and
+// the filter's decision per measurement.
+int v3dref_triplet_stage(double const* R, double const* T, double const* focal, int nTracks,
+                         int const* trackPtr, int const* view, float const* pos, double maxError,
+                         int minPoints, double minRatio, double inlierThreshold, double tau, int maxIterations,
+                         int* verdict, int* nSurvived, int* status, int* iterations, double* cost,
+                         double* Rout, double* Tout, double* Xout, unsigned char* keptOut)
+{
+   std::vector<CameraMatrix> tripleCams(3);
+   Matrix3x3d I;
+   makeIdentityMatrix(I);
+   for (int i = 0; i < 3; ++i)
+   {
+      Matrix3x3d Ri;
+      loadMat3(R + 9 * i, Ri);
+      tripleCams[i].setIntrinsic(I);
+      tripleCams[i].setRotation(Ri);
+      tripleCams[i].setTranslation(Vector3d(T[3 * i], T[3 * i + 1], T[3 * i + 2]));
+   }
+   std::vector<TriangulatedPoint> tripleModel(nTracks);
+   for (int j = 0; j < nTracks; ++j)
+      for (int m = trackPtr[j]; m < trackPtr[j + 1]; ++m)
+         tripleModel[j].measurements.push_back(
+            PointMeasurement(makeVector2<float>(pos[2 * m], pos[2 * m + 1]), view[m], m));
+
+   int const nPointsBefore = tripleModel.size();
+   for (int j = 0; j < nPointsBefore; ++j)
+      tripleModel[j].pos = triangulateLinear(tripleCams, tripleModel[j].measurements);
+
+   // filterTripleModel, generate_triples.cpp:44-81 (restated; see above)
+   std::vector<int> survivors;
+   for (int j = 0; j < nPointsBefore; ++j)
+   {
+      TriangulatedPoint& X = tripleModel[j];
+      std::vector<PointMeasurement> ms;
+      for (size_t k = 0; k < X.measurements.size(); ++k)
+      {
+         PointMeasurement const& m = X.measurements[k];
+         Vector2d p = tripleCams[m.view].projectPoint(X.pos);
+         Vector2f pp = makeVector2<float>(p[0], p[1]);
+         double const err = focal[m.view] * norm_L2(pp - m.pos);
+         bool const keep = err < maxError;
+         keptOut[m.id] = keep ? 1 : 0;
+         if (keep) ms.push_back(m);
+      }
+      X.measurements = ms;
+      if (X.measurements.size() >= 3) survivors.push_back(j);
+   }
+   for (int j = 0; j < nPointsBefore; ++j)
+      for (int r = 0; r < 3; ++r) Xout[3 * j + r] = tripleModel[j].pos[r];
+   std::vector<TriangulatedPoint> model;
+   for (size_t q = 0; q < survivors.size(); ++q) model.push_back(tripleModel[survivors[q]]);
+
+   *nSurvived = model.size();
+   *verdict = 0;
+   if ((int)model.size() < minPoints) *verdict = 1;
+   else if (double(model.size()) < minRatio * nPointsBefore) *verdict = 2;
+   *status = 0; *iterations = 0; *cost = 0.0;
+   if (*verdict == 0)
+   {
+      BundlePointStructure bundleStruct(model);
+      double tc[1024], tl[1024];
+      int ti[1024];
+      Trace tr = { tc, tl, ti, 1024, 0, 0 };
+      Traced<StdMetricBundleOptimizer> opt(&tr, inlierThreshold, tripleCams, bundleStruct.points3d,
+                                           bundleStruct.measurements, bundleStruct.correspondingView,
+                                           bundleStruct.correspondingPoint);
+      V3D::optimizerVerbosenessLevel = 0;
+      opt.tau = tau;
+      opt.maxIterations = maxIterations;
+      opt.minimize();
+      *status = opt.status;
+      *iterations = opt.currentIteration;
+      *cost = tr.len > 0 ? tc[std::min(tr.len, 1024) - 1] : 0.0;
+      bundleStruct.createPointStructure(model);
+      for (size_t q = 0; q < survivors.size(); ++q)
+         for (int r = 0; r < 3; ++r) Xout[3 * survivors[q] + r] = model[q].pos[r];
+   }
+   for (int i = 0; i < 3; ++i)
+   {
+      storeMat3(tripleCams[i].getRotation(), Rout + 9 * i);
+      Vector3d const& Ti = tripleCams[i].getTranslation();
+      Tout[3 * i] = Ti[0]; Tout[3 * i + 1] = Ti[1]; Tout[3 * i + 2] = Ti[2];
    }
    return 0;
 }

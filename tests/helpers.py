@@ -52,3 +52,22 @@ def load_rotation_golden(name):
     graph = scenes.RotationGraph(g["rel"].copy(), g["pairs"].copy(), g["R0"].copy(), g["R"].copy(), name=name)
     return graph, g
 
+
+def load_triplet_stage_golden():
+    """(list of TripletTracks, list of the reference's per-triplet outputs) of
+    tests/golden/triplets/stage.npz."""
+    g = np.load(os.path.join(GOLDEN, "triplets", "stage.npz"))
+    trips, outs = [], []
+    tp, mo = g["tp_off"], g["m_off"]
+    x0 = 0
+    for i in range(len(g["verdict"])):
+        ptr = g["track_ptr"][tp[i]:tp[i + 1]]
+        n = len(ptr) - 1
+        trips.append(scenes.TripletTracks(g["R"][i], g["T"][i], g["focal"][i], ptr, g["view"][mo[i]:mo[i + 1]],
+                                          g["pos"][mo[i]:mo[i + 1]]))
+        outs.append(dict(verdict=int(g["verdict"][i]), n_points=int(g["n_points"][i]), status=int(g["status"][i]),
+                         iterations=int(g["iterations"][i]), cost=float(g["cost"][i]), R=g["R_out"][i],
+                         T=g["T_out"][i], X=g["X_out"][x0:x0 + n], kept=g["kept"][mo[i]:mo[i + 1]]))
+        x0 += n
+    return trips, outs
+

@@ -43,7 +43,7 @@ EXPORTS = (
     "v3dba_precond_pcg_iterations", "v3dba_structure", "v3dba_refine_consistent_rotations",
     "v3dba_rotations_create", "v3dba_rotations_destroy", "v3dba_rotations_minimize", "v3dba_rotations_get",
     "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost", "v3dba_rotations_set_group",
-    "v3dba_rotations_autotune",
+    "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -72,6 +72,24 @@ class Result(C.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Triplet(C.Structure):
+    _fields_ = [("R", C.c_double * 27), ("T", C.c_double * 9), ("focal", C.c_double * 3), ("n_tracks", C.c_int),
+                ("track_ptr", _ip), ("view", _ip), ("pos", C.POINTER(C.c_float))]
+
+
+class TripletStageOptions(C.Structure):
+    _fields_ = [("max_reproj_error", C.c_double), ("min_points", C.c_int), ("min_point_ratio", C.c_double),
+                ("inlier_threshold", C.c_double), ("tau", C.c_double), ("max_iterations", C.c_int)]
+
+
+class TripletResult(C.Structure):
+    _fields_ = [("verdict", C.c_int), ("n_tracks", C.c_int), ("n_points", C.c_int), ("status", C.c_int),
+                ("iterations", C.c_int), ("cost", C.c_double), ("R", C.c_double * 27), ("T", C.c_double * 9)]
+
+
+TRIPLET_ACCEPTED, TRIPLET_TOO_FEW_POINTS, TRIPLET_POINTS_DROPPED = 0, 1, 2
 
 
 class V3dbaError(RuntimeError):
@@ -148,6 +166,11 @@ def _lib():
         L.v3dba_rotations_cost.argtypes = [C.c_void_p, _dp]
         L.v3dba_rotations_set_group.argtypes = [C.c_void_p, C.c_int]
         L.v3dba_rotations_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+        L.v3dba_default_triplet_stage_options.argtypes = [C.POINTER(TripletStageOptions)]
+        L.v3dba_default_triplet_stage_options.restype = None
+        L.v3dba_triplet_stage.argtypes = [C.POINTER(Triplet), C.c_int, C.POINTER(TripletStageOptions),
+                                          C.POINTER(TripletResult), C.POINTER(_dp), C.POINTER(C.POINTER(C.c_ubyte)),
+                                          _dp]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -324,6 +347,49 @@ def dense_cholesky_solve(S, rhs):
     check(_lib().v3dba_dense_cholesky_solve(S.shape[0], _d(S), _d(rhs), _d(x), C.byref(fail)),
           "v3dba_dense_cholesky_solve")
     return x, bool(fail.value)
+
+
+def triplet_stage(triplets, timing=None, **kw):
+    """The triplet stage (triangulation, filtering, survival tests, adjustment) of every triplet
+    in one call; returns a list of dicts (verdict, n_points, status, iterations, cost, R, T, X,
+    kept) in input order.  Keyword arguments override v3dba_triplet_stage_options; a dict passed
+    as ``timing`` receives the device time of the stage's kernels under "device_ms"."""
+    L = _lib()
+    o = TripletStageOptions()
+    L.v3dba_default_triplet_stage_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    n = len(triplets)
+    arr = (Triplet * n)()
+    keep, Xs, kepts = [], [], []
+    for i, t in enumerate(triplets):
+        tp = np.ascontiguousarray(t.track_ptr, dtype=np.int32)
+        vw = np.ascontiguousarray(t.view, dtype=np.int32)
+        ps = np.ascontiguousarray(t.pos, dtype=np.float32)
+        keep += [tp, vw, ps]
+        a = arr[i]
+        a.R[:] = list(np.ascontiguousarray(t.R, dtype=np.float64).ravel())
+        a.T[:] = list(np.ascontiguousarray(t.T, dtype=np.float64).ravel())
+        a.focal[:] = list(np.asarray(t.focal, dtype=np.float64).ravel())
+        a.n_tracks = t.n_tracks
+        a.track_ptr, a.view = tp.ctypes.data_as(_ip), vw.ctypes.data_as(_ip)
+        a.pos = ps.ctypes.data_as(C.POINTER(C.c_float))
+        Xs.append(np.zeros((max(t.n_tracks, 1), 3)))
+        kepts.append(np.zeros(max(int(tp[-1]), 1), dtype=np.uint8))
+    res = (TripletResult * n)()
+    Xp = (_dp * n)(*[x.ctypes.data_as(_dp) for x in Xs])
+    Kp = (C.POINTER(C.c_ubyte) * n)(*[k.ctypes.data_as(C.POINTER(C.c_ubyte)) for k in kepts])
+    ms = C.c_double()
+    check(L.v3dba_triplet_stage(arr, n, C.byref(o), res, Xp, Kp, C.byref(ms)), "v3dba_triplet_stage")
+    if timing is not None:
+        timing["device_ms"] = ms.value
+    out = []
+    for i, t in enumerate(triplets):
+        r = res[i]
+        out.append(dict(verdict=r.verdict, n_points=r.n_points, status=r.status, iterations=r.iterations,
+                        cost=r.cost, R=np.array(r.R[:]).reshape(3, 3, 3), T=np.array(r.T[:]).reshape(3, 3),
+                        X=Xs[i][:t.n_tracks], kept=kepts[i][:int(t.track_ptr[-1])]))
+    return out
 
 
 def rotation_options(**kw) -> Options:

@@ -836,3 +836,434 @@ int v3dba_minimize_batched(const v3dba_problem* problems, int count, const v3dba
 }
 
 }  // extern "C"
+
+// ---- triplet stage ---------------------------------------------------------------------------
+//
+// The steps either side of the triplet adjustment (SfM/generate_triples/src/generate_triples.cpp:
+// 380-415) for all triplets of a call: k_triplet_prepare (one thread per track) triangulates and
+// filters, k_triplet_assemble (one block per triplet) applies the survival tests and packs the
+// surviving points and measurements point-major into the batch layout, k_batched_lm adjusts every
+// accepted triplet, k_triplet_scatter returns each track's point.
+
+namespace v3dba {
+namespace {
+
+struct StageDev {
+  int n_trk = 0;
+  const int* trk_tri = nullptr;     // [n_trk] triplet of each track
+  const int* tptr = nullptr;        // [n_trk+1] measurements of each track (global)
+  const unsigned char* mview = nullptr;  // [n_meas] triple view
+  const float* mpos = nullptr;      // [2 n_meas]
+  const double* focal = nullptr;    // [3 count]
+  const int* trk_off = nullptr;     // [count] first track of each triplet
+  const int* n_trk_of = nullptr;    // [count]
+  double* Xtri = nullptr;           // [3 n_trk] linear triangulation
+  unsigned char* kept = nullptr;    // [n_meas]
+  int* keptcnt = nullptr;           // [n_trk] surviving measurements of a surviving track, else 0
+  int* slot = nullptr;              // [n_trk] point slot inside its triplet's problem, or -1
+  int* verdict = nullptr;           // [count]
+  int* n_surv = nullptr;            // [count]
+  int* pt_track = nullptr;          // [total point slots]
+  double max_err, min_ratio;
+  int min_points;
+};
+
+// Least squares of the 2K x 3 system A x = b by Householder QR (the algorithm of TNT's QR,
+// V3D/include/Math/v3d_linear_tnt.h:1589-1629 and its solve, :1734-1771): column norms by hypot,
+// reflector sign from the diagonal, R's diagonal kept apart.  Returns false when rank deficient.
+__device__ bool qr_least_squares3(double (*A)[3], double* b, int m, double x[3]) {
+  double rdiag[3];
+  for (int k = 0; k < 3; ++k) {
+    double nrm = 0.0;
+    for (int i = k; i < m; ++i) nrm = hypot(nrm, A[i][k]);
+    if (nrm != 0.0) {
+      if (A[k][k] < 0.0) nrm = -nrm;
+      for (int i = k; i < m; ++i) A[i][k] /= nrm;
+      A[k][k] += 1.0;
+      for (int j = k + 1; j < 3; ++j) {
+        double s = 0.0;
+        for (int i = k; i < m; ++i) s += A[i][k] * A[i][j];
+        s = -s / A[k][k];
+        for (int i = k; i < m; ++i) A[i][j] += s * A[i][k];
+      }
+    }
+    rdiag[k] = -nrm;
+  }
+  if (rdiag[0] == 0.0 || rdiag[1] == 0.0 || rdiag[2] == 0.0) return false;
+  for (int k = 0; k < 3; ++k) {
+    double s = 0.0;
+    for (int i = k; i < m; ++i) s += A[i][k] * b[i];
+    s = -s / A[k][k];
+    for (int i = k; i < m; ++i) b[i] += s * A[i][k];
+  }
+  for (int k = 2; k >= 0; --k) {
+    b[k] /= rdiag[k];
+    for (int i = 0; i < k; ++i) b[i] -= b[k] * A[i][k];
+  }
+  x[0] = b[0];
+  x[1] = b[1];
+  x[2] = b[2];
+  return true;
+}
+
+// One thread per track: triangulateLinear (v3d_mviewutilities.h:260-303) and filterTripleModel
+// (generate_triples.cpp:44-81).  The filter mirrors the reference's arithmetic: the projection
+// rounded to float, the float difference and sum of squares, the float square root, times the
+// view's focal length in double (no fused multiply-adds, so the decision is the host's).
+__global__ void __launch_bounds__(128) k_triplet_prepare(BatchDev b, StageDev s) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= s.n_trk) return;
+  const int t = s.trk_tri[g];
+  const int c0 = b.cam_off[t];
+  const int m0 = s.tptr[g], K = s.tptr[g + 1] - m0;
+  double A[2 * kMaxTrack][3], rhs[2 * kMaxTrack], X[3];
+  for (int q = 0; q < K; ++q) {
+    const int v = s.mview[m0 + q];
+    const double* R = b.R + 9 * (size_t)(c0 + v);
+    const double* T = b.T + 3 * (size_t)(c0 + v);
+    const double x = (double)s.mpos[2 * (m0 + q)], y = (double)s.mpos[2 * (m0 + q) + 1];
+    for (int c = 0; c < 3; ++c) {
+      A[2 * q][c] = __dsub_rn(__dmul_rn(x, R[6 + c]), R[c]);
+      A[2 * q + 1][c] = __dsub_rn(__dmul_rn(y, R[6 + c]), R[3 + c]);
+    }
+    rhs[2 * q] = __dsub_rn(T[0], __dmul_rn(x, T[2]));
+    rhs[2 * q + 1] = __dsub_rn(T[1], __dmul_rn(y, T[2]));
+  }
+  const bool ok = K > 0 && qr_least_squares3(A, rhs, 2 * K, X);
+  if (!ok) X[0] = X[1] = X[2] = nan("");
+  int cnt = 0;
+  for (int q = 0; q < K; ++q) {
+    const int v = s.mview[m0 + q];
+    const double* R = b.R + 9 * (size_t)(c0 + v);
+    const double* T = b.T + 3 * (size_t)(c0 + v);
+    double Y[3];
+    for (int r = 0; r < 3; ++r) {
+      double acc = __dmul_rn(R[3 * r], X[0]);
+      acc = __dadd_rn(acc, __dmul_rn(R[3 * r + 1], X[1]));
+      acc = __dadd_rn(acc, __dmul_rn(R[3 * r + 2], X[2]));
+      Y[r] = __dadd_rn(acc, T[r]);
+    }
+    const float px = (float)__ddiv_rn(Y[0], Y[2]), py = (float)__ddiv_rn(Y[1], Y[2]);
+    const float dx = __fsub_rn(px, s.mpos[2 * (m0 + q)]), dy = __fsub_rn(py, s.mpos[2 * (m0 + q) + 1]);
+    const float n = (float)sqrt((double)__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+    const double err = __dmul_rn(s.focal[3 * t + v], (double)n);
+    const bool keep = err < s.max_err;   // false for NaN
+    s.kept[m0 + q] = keep ? 1 : 0;
+    cnt += keep ? 1 : 0;
+  }
+  s.keptcnt[g] = cnt >= 3 ? cnt : 0;
+  s.Xtri[3 * (size_t)g] = X[0];
+  s.Xtri[3 * (size_t)g + 1] = X[1];
+  s.Xtri[3 * (size_t)g + 2] = X[2];
+}
+
+// Exclusive block-wide scan of one int per thread (256 threads); returns the prefix and the
+// block total in *total.
+__device__ __forceinline__ int block_scan256(int v, int* sm /* [8] */, int* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm[wid] = x;
+  __syncthreads();
+  int base = 0, tot = 0;
+  for (int w = 0; w < 8; ++w) {
+    if (w < wid) base += sm[w];
+    tot += sm[w];
+  }
+  __syncthreads();
+  *total = tot;
+  return base + x - v;
+}
+
+// One block (256 threads) per triplet: survival tests (generate_triples.cpp:393-398) and the
+// bundle problem of the survivors, point-major as BundlePointStructure builds it
+// (v3d_mviewutilities.h:136-158).
+__global__ void __launch_bounds__(256) k_triplet_assemble(BatchDev b, StageDev s) {
+  __shared__ int sm[8];
+  const int t = blockIdx.x;
+  const int g0 = s.trk_off[t], n = s.n_trk_of[t];
+  int surv = 0;
+  for (int base = 0; base < n; base += 256) {
+    const int g = g0 + base + threadIdx.x;
+    int tot;
+    block_scan256((base + (int)threadIdx.x < n && s.keptcnt[g] > 0) ? 1 : 0, sm, &tot);
+    surv += tot;
+  }
+  int verdict = V3DBA_TRIPLET_ACCEPTED;
+  if (surv < s.min_points) verdict = V3DBA_TRIPLET_TOO_FEW_POINTS;
+  else if ((double)surv < s.min_ratio * (double)n) verdict = V3DBA_TRIPLET_POINTS_DROPPED;
+  const int pt0 = b.pt_off[t];
+  const int ob0 = s.tptr[g0];   // the triplet's measurement range bounds its kept measurements
+  if (threadIdx.x == 0) {
+    s.verdict[t] = verdict;
+    s.n_surv[t] = surv;
+    b.n_pts[t] = verdict == V3DBA_TRIPLET_ACCEPTED ? surv : 0;
+    b.ptr[pt0] = ob0;
+  }
+  int q_run = 0, o_run = 0;
+  for (int base = 0; base < n; base += 256) {
+    const int g = g0 + base + threadIdx.x;
+    const bool in = base + (int)threadIdx.x < n;
+    const int kc = in ? s.keptcnt[g] : 0;
+    const bool sv = kc > 0 && verdict == V3DBA_TRIPLET_ACCEPTED;
+    int tq, to;
+    const int q = q_run + block_scan256(sv ? 1 : 0, sm, &tq);
+    const int o = o_run + block_scan256(sv ? kc : 0, sm, &to);
+    if (in) s.slot[g] = sv ? q : -1;
+    if (sv) {
+      const int p = pt0 + q;
+      b.X[3 * (size_t)p] = s.Xtri[3 * (size_t)g];
+      b.X[3 * (size_t)p + 1] = s.Xtri[3 * (size_t)g + 1];
+      b.X[3 * (size_t)p + 2] = s.Xtri[3 * (size_t)g + 2];
+      b.ptr[p + 1] = ob0 + o + kc;
+      s.pt_track[p] = g;
+      int w = ob0 + o;
+      for (int m = s.tptr[g]; m < s.tptr[g + 1]; ++m) {
+        if (!s.kept[m]) continue;
+        b.meas[2 * (size_t)w] = (double)s.mpos[2 * m];
+        b.meas[2 * (size_t)w + 1] = (double)s.mpos[2 * m + 1];
+        b.cam[w] = s.mview[m];
+        ++w;
+      }
+    }
+    q_run += tq;
+    o_run += to;
+  }
+}
+
+// One thread per track: the point after the stage.
+__global__ void __launch_bounds__(256) k_triplet_scatter(BatchDev b, StageDev s, double* __restrict__ Xout) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= s.n_trk) return;
+  const int t = s.trk_tri[g], q = s.slot[g];
+  const double* src = (q >= 0) ? b.X + 3 * (size_t)(b.pt_off[t] + q) : s.Xtri + 3 * (size_t)g;
+  Xout[3 * (size_t)g] = src[0];
+  Xout[3 * (size_t)g + 1] = src[1];
+  Xout[3 * (size_t)g + 2] = src[2];
+}
+
+}  // namespace
+}  // namespace v3dba
+
+extern "C" {
+
+void v3dba_default_triplet_stage_options(v3dba_triplet_stage_options* o) {
+  if (!o) return;
+  o->max_reproj_error = 1.0;
+  o->min_points = 50;
+  o->min_point_ratio = 0.5;
+  o->inlier_threshold = 1.0;
+  o->tau = 1e-3;
+  o->max_iterations = 5;
+}
+
+int v3dba_triplet_stage(const v3dba_triplet* trips, int count, const v3dba_triplet_stage_options* opts,
+                        v3dba_triplet_result* results, double* const* Xout, uint8_t* const* keptout,
+                        double* device_ms) {
+  if (!trips || count <= 0 || !results) return V3DBA_ERR_INVALID_ARGUMENT;
+  v3dba_triplet_stage_options o;
+  v3dba_default_triplet_stage_options(&o);
+  if (opts) o = *opts;
+  if (!(o.inlier_threshold > 0.0) || o.max_iterations < 0 || !(o.tau >= 0.0)) return V3DBA_ERR_INVALID_ARGUMENT;
+  // validation and packing
+  size_t n_trk = 0, n_meas = 0;
+  for (int t = 0; t < count; ++t) {
+    const v3dba_triplet& q = trips[t];
+    if (q.n_tracks < 0 || (q.n_tracks > 0 && (!q.track_ptr || !q.view || !q.pos))) return V3DBA_ERR_INVALID_ARGUMENT;
+    if (!all_finite(q.R, 27) || !all_finite(q.T, 9) || !all_finite(q.focal, 3)) return V3DBA_ERR_INVALID_INPUT;
+    if (q.n_tracks > 0 && q.track_ptr[0] != 0) return V3DBA_ERR_INVALID_INPUT;
+    for (int k = 0; k < q.n_tracks; ++k) {
+      const int len = q.track_ptr[k + 1] - q.track_ptr[k];
+      if (len < 0) return V3DBA_ERR_INVALID_INPUT;
+      if (len > kMaxTrack) return V3DBA_ERR_UNSUPPORTED;
+    }
+    const int nm = q.n_tracks > 0 ? q.track_ptr[q.n_tracks] : 0;
+    for (int m = 0; m < nm; ++m) {
+      if (q.view[m] < 0 || q.view[m] > 2) return V3DBA_ERR_INVALID_INPUT;
+      if (!std::isfinite(q.pos[2 * m]) || !std::isfinite(q.pos[2 * m + 1])) return V3DBA_ERR_INVALID_INPUT;
+    }
+    n_trk += q.n_tracks;
+    n_meas += nm;
+  }
+  if (n_trk > 0x7fffffffull - (size_t)count || n_meas > 0x7fffffffull) return V3DBA_ERR_UNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return V3DBA_ERR_NO_DEVICE; }
+
+  std::vector<double> R(27 * (size_t)count), T(9 * (size_t)count), K(27 * (size_t)count, 0.0), focal(3 * (size_t)count);
+  std::vector<double> thr(count, o.inlier_threshold);
+  std::vector<int> cam_off(count), n_cams(count, 3), pt_off(count), trk_off(count), n_trk_of(count);
+  std::vector<int> trk_tri(n_trk), tptr(n_trk + 1);
+  std::vector<unsigned char> mview(n_meas);
+  std::vector<float> mpos(2 * n_meas);
+  std::vector<int> size(count);
+  size_t g = 0, mm = 0;
+  for (int t = 0; t < count; ++t) {
+    const v3dba_triplet& q = trips[t];
+    std::copy(q.R, q.R + 27, R.begin() + 27 * (size_t)t);
+    std::copy(q.T, q.T + 9, T.begin() + 9 * (size_t)t);
+    for (int c = 0; c < 3; ++c) K[27 * (size_t)t + 9 * c] = K[27 * (size_t)t + 9 * c + 4] = K[27 * (size_t)t + 9 * c + 8] = 1.0;
+    std::copy(q.focal, q.focal + 3, focal.begin() + 3 * (size_t)t);
+    cam_off[t] = 3 * t;
+    trk_off[t] = (int)g;
+    n_trk_of[t] = q.n_tracks;
+    pt_off[t] = (int)g + t;   // one spare point slot per triplet keeps the end pointers apart
+    const int nm = q.n_tracks > 0 ? q.track_ptr[q.n_tracks] : 0;
+    size[t] = nm;
+    for (int k = 0; k < q.n_tracks; ++k) {
+      trk_tri[g + k] = t;
+      tptr[g + k] = (int)mm + q.track_ptr[k];
+    }
+    for (int m = 0; m < nm; ++m) {
+      mview[mm + m] = (unsigned char)q.view[m];
+      mpos[2 * (mm + m)] = q.pos[2 * m];
+      mpos[2 * (mm + m) + 1] = q.pos[2 * m + 1];
+    }
+    g += q.n_tracks;
+    mm += nm;
+  }
+  tptr[n_trk] = (int)mm;
+  const size_t n_slots = n_trk + count;
+
+  v3dba_batch_t h = new (std::nothrow) v3dba_batch_s();
+  if (!h) return V3DBA_ERR_OUT_OF_MEMORY;
+  h->total_cams = 3 * count;
+  h->total_pts = (int)n_slots;
+  h->total_obs = (int)n_meas;
+  h->h_order.resize(count);
+  std::iota(h->h_order.begin(), h->h_order.end(), 0);
+  std::stable_sort(h->h_order.begin(), h->h_order.end(), [&](int a, int c) { return size[a] > size[c]; });
+  int rc;
+#define BTRY(x) do { if ((rc = (x)) != V3DBA_OK) { batch_free(h); return rc; } } while (0)
+#define BCUDA(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { cudaGetLastError(); batch_free(h); \
+    return _e == cudaErrorMemoryAllocation ? V3DBA_ERR_OUT_OF_MEMORY : V3DBA_ERR_CUDA; } } while (0)
+#define BLAUNCH() do { note_launches(1); BCUDA(cudaPeekAtLastError()); } while (0)
+  StageDev s;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    batch_free(h);
+    return V3DBA_ERR_CUDA;
+  }
+  h->d.count = count;
+  int *d_trk_tri, *d_tptr, *d_trk_off, *d_n_trk_of;
+  unsigned char* d_mview;
+  float* d_mpos;
+  double* d_focal;
+  double* d_Xout;
+  BTRY(bupload(h, &h->d.cam_off, cam_off));
+  BTRY(bupload(h, &h->d.n_cams, n_cams));
+  BTRY(bupload(h, &h->d.pt_off, pt_off));
+  BTRY(balloc(h, &h->d.n_pts, count));
+  BTRY(bupload(h, &h->d.order, h->h_order));
+  BTRY(bupload(h, &h->d.thr, thr));
+  BTRY(bupload(h, &h->d.R, R));
+  BTRY(bupload(h, &h->d.T, T));
+  BTRY(bupload(h, &h->d.K, K));
+  BTRY(balloc(h, &h->d.X, 3 * n_slots));
+  BTRY(balloc(h, &h->d.Xt, 3 * n_slots));
+  BTRY(balloc(h, &h->d.ptr, n_slots + 1));
+  BTRY(balloc(h, &h->d.meas, 2 * n_meas));
+  BTRY(balloc(h, &h->d.cam, n_meas));
+  BTRY(balloc(h, &h->d.w, n_meas));
+  BTRY(balloc(h, &h->d.status, count));
+  BTRY(balloc(h, &h->d.iterations, count));
+  BTRY(balloc(h, &h->d.rejected, count));
+  BTRY(balloc(h, &h->d.cost, count));
+  BTRY(balloc(h, &h->d.init_cost, count));
+  BTRY(balloc(h, &h->d.lambda_out, count));
+  BTRY(balloc(h, &h->d.queue, 1));
+  BTRY(bupload(h, &d_trk_tri, trk_tri));
+  BTRY(bupload(h, &d_tptr, tptr));
+  BTRY(bupload(h, &d_trk_off, trk_off));
+  BTRY(bupload(h, &d_n_trk_of, n_trk_of));
+  BTRY(bupload(h, &d_mview, mview));
+  BTRY(bupload(h, &d_mpos, mpos));
+  BTRY(bupload(h, &d_focal, focal));
+  BTRY(balloc(h, &s.Xtri, 3 * std::max<size_t>(n_trk, 1)));
+  BTRY(balloc(h, &s.kept, std::max<size_t>(n_meas, 1)));
+  BTRY(balloc(h, &s.keptcnt, std::max<size_t>(n_trk, 1)));
+  BTRY(balloc(h, &s.slot, std::max<size_t>(n_trk, 1)));
+  BTRY(balloc(h, &s.verdict, count));
+  BTRY(balloc(h, &s.n_surv, count));
+  BTRY(balloc(h, &s.pt_track, n_slots));
+  BTRY(balloc(h, &d_Xout, 3 * std::max<size_t>(n_trk, 1)));
+  s.n_trk = (int)n_trk;
+  s.trk_tri = d_trk_tri;
+  s.tptr = d_tptr;
+  s.mview = d_mview;
+  s.mpos = d_mpos;
+  s.focal = d_focal;
+  s.trk_off = d_trk_off;
+  s.n_trk_of = d_n_trk_of;
+  s.max_err = o.max_reproj_error;
+  s.min_ratio = o.min_point_ratio;
+  s.min_points = o.min_points;
+  BCUDA(cudaEventRecord(h->ev0, h->stream));
+  if (n_trk > 0) {
+    k_triplet_prepare<<<(unsigned)((n_trk + 127) / 128), 128, 0, h->stream>>>(h->d, s);
+    BLAUNCH();
+  }
+  k_triplet_assemble<<<count, 256, 0, h->stream>>>(h->d, s);
+  BLAUNCH();
+  BatchOpts bo;
+  bo.tau = o.tau;
+  bo.grad_thr = 1e-10;
+  bo.upd_thr = 1e-10;
+  bo.max_iter = o.max_iterations;
+  BTRY(launch_range(h, 128, 0, count, bo));
+  if (n_trk > 0) {
+    k_triplet_scatter<<<(unsigned)((n_trk + 255) / 256), 256, 0, h->stream>>>(h->d, s, d_Xout);
+    BLAUNCH();
+  }
+  BCUDA(cudaEventRecord(h->ev1, h->stream));
+  // results
+  std::vector<int> verdict(count), nsurv(count), status(count), iters(count);
+  std::vector<double> cost(count), Ro(27 * (size_t)count), To(9 * (size_t)count), Xo(3 * n_trk);
+  std::vector<unsigned char> kept(n_meas);
+  BCUDA(cudaMemcpyAsync(verdict.data(), s.verdict, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
+  BCUDA(cudaMemcpyAsync(nsurv.data(), s.n_surv, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
+  BCUDA(cudaMemcpyAsync(status.data(), h->d.status, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
+  BCUDA(cudaMemcpyAsync(iters.data(), h->d.iterations, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
+  BCUDA(cudaMemcpyAsync(cost.data(), h->d.cost, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
+  BCUDA(cudaMemcpyAsync(Ro.data(), h->d.R, sizeof(double) * Ro.size(), cudaMemcpyDeviceToHost, h->stream));
+  BCUDA(cudaMemcpyAsync(To.data(), h->d.T, sizeof(double) * To.size(), cudaMemcpyDeviceToHost, h->stream));
+  if (n_trk) BCUDA(cudaMemcpyAsync(Xo.data(), d_Xout, sizeof(double) * Xo.size(), cudaMemcpyDeviceToHost, h->stream));
+  if (n_meas) BCUDA(cudaMemcpyAsync(kept.data(), s.kept, n_meas, cudaMemcpyDeviceToHost, h->stream));
+  BCUDA(cudaStreamSynchronize(h->stream));
+  if (device_ms) {
+    float ms = 0.f;
+    BCUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    *device_ms = ms;
+  }
+  size_t gg = 0, m2 = 0;
+  for (int t = 0; t < count; ++t) {
+    v3dba_triplet_result& r = results[t];
+    r.verdict = verdict[t];
+    r.n_tracks = trips[t].n_tracks;
+    r.n_points = nsurv[t];
+    const bool acc = verdict[t] == V3DBA_TRIPLET_ACCEPTED;
+    r.status = acc ? status[t] : V3DBA_STATUS_TIMEOUT;
+    r.iterations = acc ? iters[t] : 0;
+    r.cost = acc ? cost[t] : 0.0;
+    const double* Rs = acc ? Ro.data() + 27 * (size_t)t : trips[t].R;
+    const double* Ts = acc ? To.data() + 9 * (size_t)t : trips[t].T;
+    std::copy(Rs, Rs + 27, r.R);
+    std::copy(Ts, Ts + 9, r.T);
+    const int nt = trips[t].n_tracks, nm = nt > 0 ? trips[t].track_ptr[nt] : 0;
+    if (Xout && Xout[t]) std::copy(Xo.begin() + 3 * gg, Xo.begin() + 3 * (gg + nt), Xout[t]);
+    if (keptout && keptout[t]) std::copy(kept.begin() + m2, kept.begin() + m2 + nm, keptout[t]);
+    gg += nt;
+    m2 += nm;
+  }
+  batch_free(h);
+#undef BTRY
+#undef BCUDA
+#undef BLAUNCH
+  return V3DBA_OK;
+}
+
+}  // extern "C"

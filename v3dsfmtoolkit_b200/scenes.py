@@ -14,6 +14,8 @@ Workloads:
   * :func:`cluster_scene`   -- 2,000 cameras in 20 groups, 1M points, ~6M observations
   * :func:`stereo_rig_scene` -- a binocular rig along a path (StereoMetricBundleOptimizer)
   * :func:`rotation_graph`  -- view graphs for rotation averaging (refineConsistentRotations)
+  * :func:`triplet_stage_batch` -- triplets with raw tracks for the triplet stage (triangulation,
+                               filtering, adjustment)
 """
 from __future__ import annotations
 
@@ -511,4 +513,67 @@ def stereo_rig_scene(n_poses=30, n_points=3000, baseline=0.3, seed=0, noise_px=0
                  np.asarray(views, dtype=np.int32), np.asarray(points, dtype=np.int32), None,
                  name=f"stereo{n_poses}x{len(keep)}", rig_K=rig_K, rig_R=rig_R, rig_T=rig_T,
                  sub=np.asarray(subs, dtype=np.int32))
+
+
+@dataclasses.dataclass
+class TripletTracks:
+    """One triplet as the triplet stage receives it after connectTracks: the three cameras (K = I,
+    world -> camera R (3,3,3), T (3,3)), each view's average focal length (3,), and the tracks:
+    ``track_ptr`` (n+1,) int32 into ``view`` (int32) / ``pos`` (float32, normalised coordinates)."""
+    R: np.ndarray
+    T: np.ndarray
+    focal: np.ndarray
+    track_ptr: np.ndarray
+    view: np.ndarray
+    pos: np.ndarray
+
+    @property
+    def n_tracks(self) -> int:
+        return int(self.track_ptr.shape[0] - 1)
+
+
+def triplet_stage_batch(n_triplets=4096, min_tracks=30, max_tracks=800, seed=0, noise_px=0.3,
+                        outlier_frac=0.1, two_view_frac=0.05, pose_rot_deg=0.01, pose_trans=0.0005,
+                        bad_frac=0.05, bad_outlier_frac=0.7) -> list[TripletTracks]:
+    """Triplets for the triplet stage: U{min_tracks..max_tracks} tracks each, geometry as in
+    :func:`triplet_batch` but in normalised coordinates (focal lengths U[700, 1200] px per view),
+    N(0, noise_px) pixel noise, a fraction ``outlier_frac`` of measurements replaced by wrong
+    matches 5-40 px away, ``two_view_frac`` of the tracks seen in two views only, and the
+    relative-pose error of the cameras (``pose_rot_deg``, ``pose_trans`` of the baseline).  A
+    fraction ``bad_frac`` of the triplets get ``bad_outlier_frac`` wrong matches (the stage must
+    drop them)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for t in range(n_triplets):
+        m = int(rng.integers(min_tracks, max_tracks + 1))
+        b = rng.uniform(0.5, 2.0)
+        alpha = np.deg2rad(rng.uniform(5.0, 30.0))
+        D = b / (2 * np.sin(alpha / 2))
+        ang = np.array([-alpha, 0.0, alpha])
+        centers = np.stack([D * np.sin(ang), np.zeros(3), D - D * np.cos(ang)], axis=1)
+        target = np.broadcast_to(np.array([0.0, 0.0, D]), (3, 3)).copy()
+        R, T = look_at(centers, target, np.array([0.0, -1.0, 0.0]))
+        focal = rng.uniform(700.0, 1200.0, size=3)
+        X = np.array([0.0, 0.0, D]) + rng.uniform(-0.18 * D, 0.18 * D, size=(m, 3))
+        Y = np.einsum("vij,mj->mvi", R, X) + T[None]
+        q = Y[..., :2] / Y[..., 2:3]                                            # (m,3,2)
+        q = q + rng.normal(size=q.shape) * (noise_px / focal)[None, :, None]
+        frac = bad_outlier_frac if rng.random() < bad_frac else outlier_frac
+        bad = rng.random((m, 3)) < frac
+        disp = rng.uniform(5.0, 40.0, size=(m, 3)) / focal[None, :]
+        phi = rng.uniform(0, 2 * np.pi, size=(m, 3))
+        q[..., 0] += np.where(bad, disp * np.cos(phi), 0.0)
+        q[..., 1] += np.where(bad, disp * np.sin(phi), 0.0)
+        keep = np.ones((m, 3), dtype=bool)
+        two = rng.random(m) < two_view_frac
+        keep[two, rng.integers(0, 3, size=int(two.sum()))] = False
+        counts = keep.sum(axis=1)
+        track_ptr = np.zeros(m + 1, dtype=np.int32)
+        track_ptr[1:] = np.cumsum(counts)
+        view = np.nonzero(keep)[1].astype(np.int32)
+        pos = q[keep].astype(np.float32)
+        R0, T0 = _perturb_cameras(rng, R, T, np.deg2rad(pose_rot_deg), pose_trans * b)
+        out.append(TripletTracks(np.ascontiguousarray(R0), np.ascontiguousarray(T0), focal, track_ptr, view,
+                                 np.ascontiguousarray(pos.reshape(-1, 2))))
+    return out
 
