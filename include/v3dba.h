@@ -297,6 +297,18 @@ void v3dba_default_triplet_stage_options(v3dba_triplet_stage_options* opts);
 int v3dba_triplet_stage(const v3dba_triplet* triplets, int count, const v3dba_triplet_stage_options* opts,
                         v3dba_triplet_result* results, double* const* X, uint8_t* const* kept, double* device_ms);
 
+/* The same on all triplets concatenated: triplet t's cameras at R + 27 t, T + 9 t, focal + 3 t;
+ * its tracks are tracks_of[t] .. tracks_of[t+1]-1 (tracks_of[0] = 0); track g's measurements are
+ * track_ptr[g] .. track_ptr[g+1]-1 of view / pos (track_ptr[0] = 0, one list over all triplets).
+ * Outputs per triplet (verdict, n_points, status, iterations, cost, R_out 27, T_out 9: the
+ * adjustment's for accepted triplets, the inputs' cameras otherwise) and, when not NULL, X_out
+ * (3 per track) and kept (1 byte per measurement) as in v3dba_triplet_stage. */
+int v3dba_triplet_stage_flat(int count, const double* R, const double* T, const double* focal, const int32_t* tracks_of,
+                             const int32_t* track_ptr, const int32_t* view, const float* pos,
+                             const v3dba_triplet_stage_options* opts, int32_t* verdict, int32_t* n_points,
+                             int32_t* status, int32_t* iterations, double* cost, double* R_out, double* T_out,
+                             double* X_out, uint8_t* kept, double* device_ms);
+
 /* Stages of one LM iteration (benchmark support; no counterpart in the reference). */
 enum {
   V3DBA_STAGE_LINEARIZE = 0,        /* residuals, Huber weights, Jacobian blocks, point sums  */

@@ -66,3 +66,20 @@ def test_invalid_triplets_are_rejected():
     pos[0, 0] = np.nan
     with pytest.raises(capi.V3dbaError):
         capi.triplet_stage([scenes.TripletTracks(t.R, t.T, t.focal, t.track_ptr, t.view, pos)])
+
+
+def test_flat_entry_point_matches_the_per_triplet_one():
+    trips = scenes.triplet_stage_batch(n_triplets=40, seed=8, max_tracks=300)
+    per = capi.triplet_stage(trips)
+    flat = capi.triplet_stage_flat(capi.concat_triplets(trips))
+    g = m = 0
+    for i, (t, r) in enumerate(zip(trips, per)):
+        assert flat["verdict"][i] == r["verdict"] and flat["n_points"][i] == r["n_points"]
+        assert np.array_equal(flat["X"][g:g + t.n_tracks], r["X"], equal_nan=True)
+        nm = int(t.track_ptr[-1])
+        assert np.array_equal(flat["kept"][m:m + nm], r["kept"])
+        if r["verdict"] == capi.TRIPLET_ACCEPTED:
+            assert flat["status"][i] == r["status"] and np.array_equal(flat["R"][i], r["R"])
+        g += t.n_tracks
+        m += nm
+

@@ -44,6 +44,7 @@ EXPORTS = (
     "v3dba_rotations_create", "v3dba_rotations_destroy", "v3dba_rotations_minimize", "v3dba_rotations_get",
     "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost", "v3dba_rotations_set_group",
     "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
+    "v3dba_triplet_stage_flat",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -171,6 +172,9 @@ def _lib():
         L.v3dba_triplet_stage.argtypes = [C.POINTER(Triplet), C.c_int, C.POINTER(TripletStageOptions),
                                           C.POINTER(TripletResult), C.POINTER(_dp), C.POINTER(C.POINTER(C.c_ubyte)),
                                           _dp]
+        L.v3dba_triplet_stage_flat.argtypes = [C.c_int, _dp, _dp, _dp, _ip, _ip, _ip, C.POINTER(C.c_float),
+                                               C.POINTER(TripletStageOptions), _ip, _ip, _ip, _ip, _dp, _dp, _dp, _dp,
+                                               C.POINTER(C.c_ubyte), _dp]
         L.v3dba_launch_count.restype = C.c_uint64
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
@@ -389,6 +393,54 @@ def triplet_stage(triplets, timing=None, **kw):
         out.append(dict(verdict=r.verdict, n_points=r.n_points, status=r.status, iterations=r.iterations,
                         cost=r.cost, R=np.array(r.R[:]).reshape(3, 3, 3), T=np.array(r.T[:]).reshape(3, 3),
                         X=Xs[i][:t.n_tracks], kept=kepts[i][:int(t.track_ptr[-1])]))
+    return out
+
+
+def concat_triplets(triplets):
+    """All triplets' inputs as the flat arrays of v3dba_triplet_stage_flat."""
+    n = len(triplets)
+    tracks_of = np.zeros(n + 1, dtype=np.int32)
+    tracks_of[1:] = np.cumsum([t.n_tracks for t in triplets])
+    m_of = np.zeros(n + 1, dtype=np.int64)
+    m_of[1:] = np.cumsum([int(t.track_ptr[-1]) for t in triplets])
+    track_ptr = np.concatenate([t.track_ptr[:-1] + m_of[i] for i, t in enumerate(triplets)] + [[m_of[-1]]])
+    return dict(count=n, R=np.ascontiguousarray(np.stack([t.R for t in triplets]), dtype=np.float64),
+                T=np.ascontiguousarray(np.stack([t.T for t in triplets]), dtype=np.float64),
+                focal=np.ascontiguousarray(np.stack([t.focal for t in triplets]), dtype=np.float64),
+                tracks_of=tracks_of, track_ptr=np.ascontiguousarray(track_ptr, dtype=np.int32),
+                view=np.ascontiguousarray(np.concatenate([t.view for t in triplets]), dtype=np.int32),
+                pos=np.ascontiguousarray(np.concatenate([t.pos for t in triplets]).reshape(-1, 2), dtype=np.float32))
+
+
+def triplet_stage_flat(flat, timing=None, want_points=True, **kw):
+    """v3dba_triplet_stage_flat on the arrays of :func:`concat_triplets`; returns a dict of flat
+    outputs (verdict, n_points, status, iterations, cost, R, T per triplet; X per track and kept
+    per measurement unless want_points is False)."""
+    L = _lib()
+    o = TripletStageOptions()
+    L.v3dba_default_triplet_stage_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    n = flat["count"]
+    n_trk, n_meas = int(flat["tracks_of"][-1]), int(flat["track_ptr"][-1])
+    out = dict(verdict=np.zeros(n, np.int32), n_points=np.zeros(n, np.int32), status=np.zeros(n, np.int32),
+               iterations=np.zeros(n, np.int32), cost=np.zeros(n), R=np.zeros((n, 3, 3, 3)), T=np.zeros((n, 3, 3)))
+    if want_points:
+        out["X"], out["kept"] = np.zeros((max(n_trk, 1), 3)), np.zeros(max(n_meas, 1), np.uint8)
+    ms = C.c_double()
+    ip = lambda a: a.ctypes.data_as(_ip)
+    check(L.v3dba_triplet_stage_flat(n, _d(flat["R"]), _d(flat["T"]), _d(flat["focal"]), ip(flat["tracks_of"]),
+                                     ip(flat["track_ptr"]), ip(flat["view"]),
+                                     flat["pos"].ctypes.data_as(C.POINTER(C.c_float)), C.byref(o),
+                                     ip(out["verdict"]), ip(out["n_points"]), ip(out["status"]), ip(out["iterations"]),
+                                     _d(out["cost"]), _d(out["R"]), _d(out["T"]),
+                                     _d(out["X"]) if want_points else None,
+                                     out["kept"].ctypes.data_as(C.POINTER(C.c_ubyte)) if want_points else None,
+                                     C.byref(ms)), "v3dba_triplet_stage_flat")
+    if want_points:
+        out["X"], out["kept"] = out["X"][:n_trk], out["kept"][:n_meas]
+    if timing is not None:
+        timing["device_ms"] = ms.value
     return out
 
 

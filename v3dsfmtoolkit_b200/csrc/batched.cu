@@ -852,7 +852,7 @@ struct StageDev {
   int n_trk = 0;
   const int* trk_tri = nullptr;     // [n_trk] triplet of each track
   const int* tptr = nullptr;        // [n_trk+1] measurements of each track (global)
-  const unsigned char* mview = nullptr;  // [n_meas] triple view
+  const int* mview = nullptr;       // [n_meas] triple view
   const float* mpos = nullptr;      // [2 n_meas]
   const double* focal = nullptr;    // [3 count]
   const int* trk_off = nullptr;     // [count] first track of each triplet
@@ -1026,7 +1026,7 @@ __global__ void __launch_bounds__(256) k_triplet_assemble(BatchDev b, StageDev s
         if (!s.kept[m]) continue;
         b.meas[2 * (size_t)w] = (double)s.mpos[2 * m];
         b.meas[2 * (size_t)w + 1] = (double)s.mpos[2 * m + 1];
-        b.cam[w] = s.mview[m];
+        b.cam[w] = (unsigned char)s.mview[m];
         ++w;
       }
     }
@@ -1046,102 +1046,64 @@ __global__ void __launch_bounds__(256) k_triplet_scatter(BatchDev b, StageDev s,
   Xout[3 * (size_t)g + 2] = src[2];
 }
 
+// Per-triplet bookkeeping filled on the device: the triplet of every track, the batch layout's
+// camera / point offsets, identity intrinsics and the adjustment's threshold.
+__global__ void __launch_bounds__(256) k_triplet_setup(BatchDev b, int* __restrict__ trk_tri, const int* __restrict__ trk_off,
+                                                       int* __restrict__ n_trk_of, double thr) {
+  const int t = blockIdx.x;
+  const int g0 = trk_off[t], g1 = trk_off[t + 1];
+  for (int g = g0 + threadIdx.x; g < g1; g += blockDim.x) trk_tri[g] = t;
+  if (threadIdx.x < 27) b.K[27 * (size_t)t + threadIdx.x] = (threadIdx.x % 9 == 0 || threadIdx.x % 9 == 4 || threadIdx.x % 9 == 8) ? 1.0 : 0.0;
+  if (threadIdx.x == 0) {
+    b.cam_off[t] = 3 * t;
+    b.n_cams[t] = 3;
+    b.pt_off[t] = g0 + t;   // one spare point slot per triplet keeps the end pointers apart
+    b.thr[t] = thr;
+    n_trk_of[t] = g1 - g0;
+  }
+}
+
 }  // namespace
 }  // namespace v3dba
 
-extern "C" {
+namespace {
 
-void v3dba_default_triplet_stage_options(v3dba_triplet_stage_options* o) {
-  if (!o) return;
-  o->max_reproj_error = 1.0;
-  o->min_points = 50;
-  o->min_point_ratio = 0.5;
-  o->inlier_threshold = 1.0;
-  o->tau = 1e-3;
-  o->max_iterations = 5;
-}
-
-int v3dba_triplet_stage(const v3dba_triplet* trips, int count, const v3dba_triplet_stage_options* opts,
-                        v3dba_triplet_result* results, double* const* Xout, uint8_t* const* keptout,
-                        double* device_ms) {
-  if (!trips || count <= 0 || !results) return V3DBA_ERR_INVALID_ARGUMENT;
-  v3dba_triplet_stage_options o;
-  v3dba_default_triplet_stage_options(&o);
-  if (opts) o = *opts;
-  if (!(o.inlier_threshold > 0.0) || o.max_iterations < 0 || !(o.tau >= 0.0)) return V3DBA_ERR_INVALID_ARGUMENT;
-  // validation and packing
-  size_t n_trk = 0, n_meas = 0;
-  for (int t = 0; t < count; ++t) {
-    const v3dba_triplet& q = trips[t];
-    if (q.n_tracks < 0 || (q.n_tracks > 0 && (!q.track_ptr || !q.view || !q.pos))) return V3DBA_ERR_INVALID_ARGUMENT;
-    if (!all_finite(q.R, 27) || !all_finite(q.T, 9) || !all_finite(q.focal, 3)) return V3DBA_ERR_INVALID_INPUT;
-    if (q.n_tracks > 0 && q.track_ptr[0] != 0) return V3DBA_ERR_INVALID_INPUT;
-    for (int k = 0; k < q.n_tracks; ++k) {
-      const int len = q.track_ptr[k + 1] - q.track_ptr[k];
-      if (len < 0) return V3DBA_ERR_INVALID_INPUT;
-      if (len > kMaxTrack) return V3DBA_ERR_UNSUPPORTED;
-    }
-    const int nm = q.n_tracks > 0 ? q.track_ptr[q.n_tracks] : 0;
-    for (int m = 0; m < nm; ++m) {
-      if (q.view[m] < 0 || q.view[m] > 2) return V3DBA_ERR_INVALID_INPUT;
-      if (!std::isfinite(q.pos[2 * m]) || !std::isfinite(q.pos[2 * m + 1])) return V3DBA_ERR_INVALID_INPUT;
-    }
-    n_trk += q.n_tracks;
-    n_meas += nm;
-  }
+// The stage on flat inputs (all triplets concatenated); outputs flat.  See v3dba_triplet_stage_flat.
+int triplet_stage_core(int count, const double* R, const double* T, const double* focal, const int32_t* tracks_of,
+                       const int32_t* track_ptr, const int32_t* view, const float* pos,
+                       const v3dba_triplet_stage_options& o, int32_t* verdict_out, int32_t* npts_out,
+                       int32_t* status_out, int32_t* iters_out, double* cost_out, double* R_out, double* T_out,
+                       double* X_out, uint8_t* kept_out, double* device_ms) {
+  const size_t n_trk = (size_t)tracks_of[count];
+  const size_t n_meas = n_trk > 0 ? (size_t)track_ptr[n_trk] : 0;
   if (n_trk > 0x7fffffffull - (size_t)count || n_meas > 0x7fffffffull) return V3DBA_ERR_UNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return V3DBA_ERR_NO_DEVICE; }
-
-  std::vector<double> R(27 * (size_t)count), T(9 * (size_t)count), K(27 * (size_t)count, 0.0), focal(3 * (size_t)count);
-  std::vector<double> thr(count, o.inlier_threshold);
-  std::vector<int> cam_off(count), n_cams(count, 3), pt_off(count), trk_off(count), n_trk_of(count);
-  std::vector<int> trk_tri(n_trk), tptr(n_trk + 1);
-  std::vector<unsigned char> mview(n_meas);
-  std::vector<float> mpos(2 * n_meas);
-  std::vector<int> size(count);
-  size_t g = 0, mm = 0;
-  for (int t = 0; t < count; ++t) {
-    const v3dba_triplet& q = trips[t];
-    std::copy(q.R, q.R + 27, R.begin() + 27 * (size_t)t);
-    std::copy(q.T, q.T + 9, T.begin() + 9 * (size_t)t);
-    for (int c = 0; c < 3; ++c) K[27 * (size_t)t + 9 * c] = K[27 * (size_t)t + 9 * c + 4] = K[27 * (size_t)t + 9 * c + 8] = 1.0;
-    std::copy(q.focal, q.focal + 3, focal.begin() + 3 * (size_t)t);
-    cam_off[t] = 3 * t;
-    trk_off[t] = (int)g;
-    n_trk_of[t] = q.n_tracks;
-    pt_off[t] = (int)g + t;   // one spare point slot per triplet keeps the end pointers apart
-    const int nm = q.n_tracks > 0 ? q.track_ptr[q.n_tracks] : 0;
-    size[t] = nm;
-    for (int k = 0; k < q.n_tracks; ++k) {
-      trk_tri[g + k] = t;
-      tptr[g + k] = (int)mm + q.track_ptr[k];
-    }
-    for (int m = 0; m < nm; ++m) {
-      mview[mm + m] = (unsigned char)q.view[m];
-      mpos[2 * (mm + m)] = q.pos[2 * m];
-      mpos[2 * (mm + m) + 1] = q.pos[2 * m + 1];
-    }
-    g += q.n_tracks;
-    mm += nm;
-  }
-  tptr[n_trk] = (int)mm;
+  // longest-processing-time order of the adjustments (by raw measurement count)
+  std::vector<int> size(count), order(count);
+  for (int t = 0; t < count; ++t) size[t] = track_ptr[tracks_of[t + 1]] - track_ptr[tracks_of[t]];
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return size[a] > size[c]; });
   const size_t n_slots = n_trk + count;
 
+  PhaseTrace trace("V3DBA_TRACE_STAGE", "v3dba_triplet_stage");
   v3dba_batch_t h = new (std::nothrow) v3dba_batch_s();
   if (!h) return V3DBA_ERR_OUT_OF_MEMORY;
   h->total_cams = 3 * count;
   h->total_pts = (int)n_slots;
   h->total_obs = (int)n_meas;
-  h->h_order.resize(count);
-  std::iota(h->h_order.begin(), h->h_order.end(), 0);
-  std::stable_sort(h->h_order.begin(), h->h_order.end(), [&](int a, int c) { return size[a] > size[c]; });
   int rc;
-#define BTRY(x) do { if ((rc = (x)) != V3DBA_OK) { batch_free(h); return rc; } } while (0)
-#define BCUDA(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { cudaGetLastError(); batch_free(h); \
+  Arena ar;
+  auto done = [&]() {
+    ar.release(h->stream);
+    batch_free(h);   // synchronises the stream before destroying it
+  };
+#define BTRY(x) do { if ((rc = (x)) != V3DBA_OK) { done(); return rc; } } while (0)
+#define BCUDA(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { cudaGetLastError(); done(); \
     return _e == cudaErrorMemoryAllocation ? V3DBA_ERR_OUT_OF_MEMORY : V3DBA_ERR_CUDA; } } while (0)
 #define BLAUNCH() do { note_launches(1); BCUDA(cudaPeekAtLastError()); } while (0)
-  StageDev s;
+#define BUP(dst, src, n) do { if ((n) > 0) BCUDA(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (n), cudaMemcpyHostToDevice, h->stream)); } while (0)
+#define BDOWN(dst, src, n) do { if ((n) > 0) BCUDA(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (n), cudaMemcpyDeviceToHost, h->stream)); } while (0)
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
     cudaGetLastError();
@@ -1149,52 +1111,64 @@ int v3dba_triplet_stage(const v3dba_triplet* trips, int count, const v3dba_tripl
     return V3DBA_ERR_CUDA;
   }
   h->d.count = count;
-  int *d_trk_tri, *d_tptr, *d_trk_off, *d_n_trk_of;
-  unsigned char* d_mview;
+  StageDev s;
+  int *d_trk_tri, *d_tptr, *d_trk_off, *d_n_trk_of, *d_view;
   float* d_mpos;
   double* d_focal;
   double* d_Xout;
-  BTRY(bupload(h, &h->d.cam_off, cam_off));
-  BTRY(bupload(h, &h->d.n_cams, n_cams));
-  BTRY(bupload(h, &h->d.pt_off, pt_off));
-  BTRY(balloc(h, &h->d.n_pts, count));
-  BTRY(bupload(h, &h->d.order, h->h_order));
-  BTRY(bupload(h, &h->d.thr, thr));
-  BTRY(bupload(h, &h->d.R, R));
-  BTRY(bupload(h, &h->d.T, T));
-  BTRY(bupload(h, &h->d.K, K));
-  BTRY(balloc(h, &h->d.X, 3 * n_slots));
-  BTRY(balloc(h, &h->d.Xt, 3 * n_slots));
-  BTRY(balloc(h, &h->d.ptr, n_slots + 1));
-  BTRY(balloc(h, &h->d.meas, 2 * n_meas));
-  BTRY(balloc(h, &h->d.cam, n_meas));
-  BTRY(balloc(h, &h->d.w, n_meas));
-  BTRY(balloc(h, &h->d.status, count));
-  BTRY(balloc(h, &h->d.iterations, count));
-  BTRY(balloc(h, &h->d.rejected, count));
-  BTRY(balloc(h, &h->d.cost, count));
-  BTRY(balloc(h, &h->d.init_cost, count));
-  BTRY(balloc(h, &h->d.lambda_out, count));
-  BTRY(balloc(h, &h->d.queue, 1));
-  BTRY(bupload(h, &d_trk_tri, trk_tri));
-  BTRY(bupload(h, &d_tptr, tptr));
-  BTRY(bupload(h, &d_trk_off, trk_off));
-  BTRY(bupload(h, &d_n_trk_of, n_trk_of));
-  BTRY(bupload(h, &d_mview, mview));
-  BTRY(bupload(h, &d_mpos, mpos));
-  BTRY(bupload(h, &d_focal, focal));
-  BTRY(balloc(h, &s.Xtri, 3 * std::max<size_t>(n_trk, 1)));
-  BTRY(balloc(h, &s.kept, std::max<size_t>(n_meas, 1)));
-  BTRY(balloc(h, &s.keptcnt, std::max<size_t>(n_trk, 1)));
-  BTRY(balloc(h, &s.slot, std::max<size_t>(n_trk, 1)));
-  BTRY(balloc(h, &s.verdict, count));
-  BTRY(balloc(h, &s.n_surv, count));
-  BTRY(balloc(h, &s.pt_track, n_slots));
-  BTRY(balloc(h, &d_Xout, 3 * std::max<size_t>(n_trk, 1)));
+  ar.add(&h->d.cam_off, count);
+  ar.add(&h->d.n_cams, count);
+  ar.add(&h->d.pt_off, count);
+  ar.add(&h->d.n_pts, count);
+  ar.add(&h->d.order, count);
+  ar.add(&h->d.thr, count);
+  ar.add(&h->d.R, 27 * (size_t)count);
+  ar.add(&h->d.T, 9 * (size_t)count);
+  ar.add(&h->d.K, 27 * (size_t)count);
+  ar.add(&h->d.X, 3 * n_slots);
+  ar.add(&h->d.Xt, 3 * n_slots);
+  ar.add(&h->d.ptr, n_slots + 1);
+  ar.add(&h->d.meas, 2 * n_meas);
+  ar.add(&h->d.cam, n_meas);
+  ar.add(&h->d.w, n_meas);
+  ar.add(&h->d.status, count);
+  ar.add(&h->d.iterations, count);
+  ar.add(&h->d.rejected, count);
+  ar.add(&h->d.cost, count);
+  ar.add(&h->d.init_cost, count);
+  ar.add(&h->d.lambda_out, count);
+  ar.add(&h->d.queue, 1);
+  ar.add(&d_trk_tri, n_trk);
+  ar.add(&d_tptr, n_trk + 1);
+  ar.add(&d_trk_off, (size_t)count + 1);
+  ar.add(&d_n_trk_of, count);
+  ar.add(&d_view, n_meas);
+  ar.add(&d_mpos, 2 * n_meas);
+  ar.add(&d_focal, 3 * (size_t)count);
+  ar.add(&s.Xtri, 3 * n_trk);
+  ar.add(&s.kept, n_meas);
+  ar.add(&s.keptcnt, n_trk);
+  ar.add(&s.slot, n_trk);
+  ar.add(&s.verdict, count);
+  ar.add(&s.n_surv, count);
+  ar.add(&s.pt_track, n_slots);
+  ar.add(&d_Xout, 3 * n_trk);
+  BTRY(ar.commit(h->stream));
+  trace.mark("alloc", h->stream);
+  // inputs: one copy of each caller array
+  BUP(h->d.R, R, 27 * (size_t)count);
+  BUP(h->d.T, T, 9 * (size_t)count);
+  BUP(d_focal, focal, 3 * (size_t)count);
+  BUP(d_trk_off, tracks_of, (size_t)count + 1);
+  BUP(d_tptr, track_ptr, n_trk + 1);
+  BUP(d_view, view, n_meas);
+  BUP(d_mpos, pos, 2 * n_meas);
+  BUP(h->d.order, order.data(), (size_t)count);
+  trace.mark("upload", h->stream);
   s.n_trk = (int)n_trk;
   s.trk_tri = d_trk_tri;
   s.tptr = d_tptr;
-  s.mview = d_mview;
+  s.mview = d_view;
   s.mpos = d_mpos;
   s.focal = d_focal;
   s.trk_off = d_trk_off;
@@ -1203,6 +1177,8 @@ int v3dba_triplet_stage(const v3dba_triplet* trips, int count, const v3dba_tripl
   s.min_ratio = o.min_point_ratio;
   s.min_points = o.min_points;
   BCUDA(cudaEventRecord(h->ev0, h->stream));
+  k_triplet_setup<<<count, 256, 0, h->stream>>>(h->d, d_trk_tri, d_trk_off, d_n_trk_of, o.inlier_threshold);
+  BLAUNCH();
   if (n_trk > 0) {
     k_triplet_prepare<<<(unsigned)((n_trk + 127) / 128), 128, 0, h->stream>>>(h->d, s);
     BLAUNCH();
@@ -1220,31 +1196,148 @@ int v3dba_triplet_stage(const v3dba_triplet* trips, int count, const v3dba_tripl
     BLAUNCH();
   }
   BCUDA(cudaEventRecord(h->ev1, h->stream));
-  // results
-  std::vector<int> verdict(count), nsurv(count), status(count), iters(count);
-  std::vector<double> cost(count), Ro(27 * (size_t)count), To(9 * (size_t)count), Xo(3 * n_trk);
-  std::vector<unsigned char> kept(n_meas);
-  BCUDA(cudaMemcpyAsync(verdict.data(), s.verdict, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
-  BCUDA(cudaMemcpyAsync(nsurv.data(), s.n_surv, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
-  BCUDA(cudaMemcpyAsync(status.data(), h->d.status, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
-  BCUDA(cudaMemcpyAsync(iters.data(), h->d.iterations, sizeof(int) * count, cudaMemcpyDeviceToHost, h->stream));
-  BCUDA(cudaMemcpyAsync(cost.data(), h->d.cost, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
-  BCUDA(cudaMemcpyAsync(Ro.data(), h->d.R, sizeof(double) * Ro.size(), cudaMemcpyDeviceToHost, h->stream));
-  BCUDA(cudaMemcpyAsync(To.data(), h->d.T, sizeof(double) * To.size(), cudaMemcpyDeviceToHost, h->stream));
-  if (n_trk) BCUDA(cudaMemcpyAsync(Xo.data(), d_Xout, sizeof(double) * Xo.size(), cudaMemcpyDeviceToHost, h->stream));
-  if (n_meas) BCUDA(cudaMemcpyAsync(kept.data(), s.kept, n_meas, cudaMemcpyDeviceToHost, h->stream));
+  trace.mark("kernels", h->stream);
+  BDOWN(verdict_out, s.verdict, (size_t)count);
+  BDOWN(npts_out, s.n_surv, (size_t)count);
+  BDOWN(status_out, h->d.status, (size_t)count);
+  BDOWN(iters_out, h->d.iterations, (size_t)count);
+  BDOWN(cost_out, h->d.cost, (size_t)count);
+  BDOWN(R_out, h->d.R, 27 * (size_t)count);
+  BDOWN(T_out, h->d.T, 9 * (size_t)count);
+  if (X_out) BDOWN(X_out, d_Xout, 3 * n_trk);
+  if (kept_out) BDOWN(kept_out, s.kept, n_meas);
   BCUDA(cudaStreamSynchronize(h->stream));
+  trace.mark("download");
   if (device_ms) {
     float ms = 0.f;
     BCUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     *device_ms = ms;
   }
+  done();
+  trace.mark("free");
+#undef BTRY
+#undef BCUDA
+#undef BLAUNCH
+#undef BUP
+#undef BDOWN
+  return V3DBA_OK;
+}
+
+// Shared validation of one triplet's tracks (track_ptr relative to the triplet).
+int check_tracks(int n_tracks, const int32_t* track_ptr, const int32_t* view, const float* pos) {
+  if (n_tracks < 0 || (n_tracks > 0 && (!track_ptr || !view || !pos))) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (n_tracks == 0) return V3DBA_OK;
+  if (track_ptr[0] != 0) return V3DBA_ERR_INVALID_INPUT;
+  for (int k = 0; k < n_tracks; ++k) {
+    const int len = track_ptr[k + 1] - track_ptr[k];
+    if (len < 0) return V3DBA_ERR_INVALID_INPUT;
+    if (len > kMaxTrack) return V3DBA_ERR_UNSUPPORTED;
+  }
+  const int nm = track_ptr[n_tracks];
+  unsigned bad = 0;
+  for (int m = 0; m < nm; ++m) bad |= (unsigned)view[m] > 2u ? 1u : 0u;
+  if (bad) return V3DBA_ERR_INVALID_INPUT;
+  if (!all_finite_f(pos, 2 * (size_t)nm)) return V3DBA_ERR_INVALID_INPUT;
+  return V3DBA_OK;
+}
+
+int stage_options(const v3dba_triplet_stage_options* opts, v3dba_triplet_stage_options* o) {
+  v3dba_default_triplet_stage_options(o);
+  if (opts) *o = *opts;
+  if (!(o->inlier_threshold > 0.0) || o->max_iterations < 0 || !(o->tau >= 0.0)) return V3DBA_ERR_INVALID_ARGUMENT;
+  return V3DBA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void v3dba_default_triplet_stage_options(v3dba_triplet_stage_options* o) {
+  if (!o) return;
+  o->max_reproj_error = 1.0;
+  o->min_points = 50;
+  o->min_point_ratio = 0.5;
+  o->inlier_threshold = 1.0;
+  o->tau = 1e-3;
+  o->max_iterations = 5;
+}
+
+int v3dba_triplet_stage_flat(int count, const double* R, const double* T, const double* focal, const int32_t* tracks_of,
+                             const int32_t* track_ptr, const int32_t* view, const float* pos,
+                             const v3dba_triplet_stage_options* opts, int32_t* verdict, int32_t* n_points,
+                             int32_t* status, int32_t* iterations, double* cost, double* R_out, double* T_out,
+                             double* X_out, uint8_t* kept, double* device_ms) {
+  if (count <= 0 || !R || !T || !focal || !tracks_of || !track_ptr || !verdict || !n_points || !status ||
+      !iterations || !cost || !R_out || !T_out)
+    return V3DBA_ERR_INVALID_ARGUMENT;
+  v3dba_triplet_stage_options o;
+  int rc = stage_options(opts, &o);
+  if (rc) return rc;
+  if (!all_finite(R, 27 * (size_t)count) || !all_finite(T, 9 * (size_t)count) || !all_finite(focal, 3 * (size_t)count))
+    return V3DBA_ERR_INVALID_INPUT;
+  if (tracks_of[0] != 0) return V3DBA_ERR_INVALID_INPUT;
+  for (int t = 0; t < count; ++t)
+    if (tracks_of[t + 1] < tracks_of[t]) return V3DBA_ERR_INVALID_INPUT;
+  const int n_trk = tracks_of[count];
+  if (n_trk > 0 && (!view || !pos)) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (track_ptr[0] != 0) return V3DBA_ERR_INVALID_INPUT;
+  // the global track_ptr is one list: check it in one pass, as one triplet of n_trk tracks
+  if ((rc = check_tracks(n_trk, track_ptr, view, pos))) return rc;
+  return triplet_stage_core(count, R, T, focal, tracks_of, track_ptr, view, pos, o, verdict, n_points, status,
+                            iterations, cost, R_out, T_out, X_out, kept, device_ms);
+}
+
+int v3dba_triplet_stage(const v3dba_triplet* trips, int count, const v3dba_triplet_stage_options* opts,
+                        v3dba_triplet_result* results, double* const* Xout, uint8_t* const* keptout,
+                        double* device_ms) {
+  if (!trips || count <= 0 || !results) return V3DBA_ERR_INVALID_ARGUMENT;
+  v3dba_triplet_stage_options o;
+  int rc = stage_options(opts, &o);
+  if (rc) return rc;
+  size_t n_trk = 0, n_meas = 0;
+  for (int t = 0; t < count; ++t) {
+    const v3dba_triplet& q = trips[t];
+    if ((rc = check_tracks(q.n_tracks, q.track_ptr, q.view, q.pos))) return rc;
+    if (!all_finite(q.R, 27) || !all_finite(q.T, 9) || !all_finite(q.focal, 3)) return V3DBA_ERR_INVALID_INPUT;
+    n_trk += q.n_tracks;
+    n_meas += q.n_tracks > 0 ? q.track_ptr[q.n_tracks] : 0;
+  }
+  if (n_trk > 0x7fffffffull - (size_t)count || n_meas > 0x7fffffffull) return V3DBA_ERR_UNSUPPORTED;
+  // concatenate
+  std::vector<double> R(27 * (size_t)count), T(9 * (size_t)count), focal(3 * (size_t)count);
+  std::vector<int32_t> tracks_of((size_t)count + 1), tptr(n_trk + 1), view(n_meas);
+  std::vector<float> pos(2 * n_meas);
+  size_t g = 0, mm = 0;
+  for (int t = 0; t < count; ++t) {
+    const v3dba_triplet& q = trips[t];
+    std::copy(q.R, q.R + 27, R.begin() + 27 * (size_t)t);
+    std::copy(q.T, q.T + 9, T.begin() + 9 * (size_t)t);
+    std::copy(q.focal, q.focal + 3, focal.begin() + 3 * (size_t)t);
+    tracks_of[t] = (int32_t)g;
+    const int nm = q.n_tracks > 0 ? q.track_ptr[q.n_tracks] : 0;
+    for (int k = 0; k < q.n_tracks; ++k) tptr[g + k] = (int32_t)mm + q.track_ptr[k];
+    if (nm) {
+      std::copy(q.view, q.view + nm, view.begin() + mm);
+      std::copy(q.pos, q.pos + 2 * nm, pos.begin() + 2 * mm);
+    }
+    g += q.n_tracks;
+    mm += nm;
+  }
+  tracks_of[count] = (int32_t)g;
+  tptr[n_trk] = (int32_t)mm;
+  std::vector<int32_t> verdict(count), npts(count), status(count), iters(count);
+  std::vector<double> cost(count), Ro(27 * (size_t)count), To(9 * (size_t)count), Xo(3 * n_trk);
+  std::vector<uint8_t> kept(n_meas);
+  rc = triplet_stage_core(count, R.data(), T.data(), focal.data(), tracks_of.data(), tptr.data(), view.data(),
+                          pos.data(), o, verdict.data(), npts.data(), status.data(), iters.data(), cost.data(),
+                          Ro.data(), To.data(), Xo.data(), kept.data(), device_ms);
+  if (rc) return rc;
   size_t gg = 0, m2 = 0;
   for (int t = 0; t < count; ++t) {
     v3dba_triplet_result& r = results[t];
     r.verdict = verdict[t];
     r.n_tracks = trips[t].n_tracks;
-    r.n_points = nsurv[t];
+    r.n_points = npts[t];
     const bool acc = verdict[t] == V3DBA_TRIPLET_ACCEPTED;
     r.status = acc ? status[t] : V3DBA_STATUS_TIMEOUT;
     r.iterations = acc ? iters[t] : 0;
@@ -1259,10 +1352,6 @@ int v3dba_triplet_stage(const v3dba_triplet* trips, int count, const v3dba_tripl
     gg += nt;
     m2 += nm;
   }
-  batch_free(h);
-#undef BTRY
-#undef BCUDA
-#undef BLAUNCH
   return V3DBA_OK;
 }
 

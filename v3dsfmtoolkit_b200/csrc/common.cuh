@@ -2,8 +2,10 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <vector>
 
 #include "v3dba.h"
 
@@ -14,6 +16,35 @@ void note_launches(uint64_t n);
 
 // True when no value is Inf or NaN (host; branch-free so the scan vectorises).
 bool all_finite(const double* p, size_t n);
+bool all_finite_f(const float* p, size_t n);
+
+// Host phase timings on stderr when the environment variable `env` is set (diagnostics).
+struct PhaseTrace {
+  explicit PhaseTrace(const char* env, const char* label);
+  void mark(const char* phase, cudaStream_t st = nullptr);
+  bool on;
+  const char* label;
+  double t;
+};
+
+// Many device buffers carved from one stream-ordered allocation (one cudaMallocAsync, one
+// cudaFreeAsync): add() records the requests, commit() allocates and assigns the pointers.
+struct Arena {
+  template <typename T>
+  void add(T** p, size_t n) {
+    req_.push_back({reinterpret_cast<void**>(p), (std::max<size_t>(n, 1) * sizeof(T) + 255) & ~(size_t)255});
+  }
+  int commit(cudaStream_t st);
+  void release(cudaStream_t st);
+  char* base = nullptr;
+
+ private:
+  struct Req {
+    void** p;
+    size_t bytes;
+  };
+  std::vector<Req> req_;
+};
 
 // Raises the release threshold of the current device's stream-ordered pool once, so memory
 // freed by one handle is kept for the next (handles are created and destroyed in loops).

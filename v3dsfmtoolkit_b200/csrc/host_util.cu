@@ -1,5 +1,7 @@
 // Host-side helpers shared by the entry points.
 #include <atomic>
+#include <chrono>
+#include <cstdlib>
 #include <cstring>
 
 #include "common.cuh"
@@ -15,6 +17,52 @@ bool all_finite(const double* p, size_t n) {
     bad |= (uint64_t)((b & kExp) == kExp);
   }
   return bad == 0;
+}
+
+bool all_finite_f(const float* p, size_t n) {
+  constexpr uint32_t kExp = 0x7f800000u;
+  uint32_t bad = 0;
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t b;
+    std::memcpy(&b, p + i, sizeof(b));
+    bad |= (uint32_t)((b & kExp) == kExp);
+  }
+  return bad == 0;
+}
+
+static double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+PhaseTrace::PhaseTrace(const char* env, const char* lbl) : on(std::getenv(env) != nullptr), label(lbl), t(now_ms()) {}
+
+void PhaseTrace::mark(const char* phase, cudaStream_t st) {
+  if (!on) return;
+  if (st) cudaStreamSynchronize(st);
+  const double n = now_ms();
+  std::fprintf(stderr, "%s %-12s %8.3f ms\n", label, phase, n - t);
+  t = n;
+}
+
+int Arena::commit(cudaStream_t st) {
+  size_t total = 0;
+  for (const Req& r : req_) total += r.bytes;
+  int rc = ensure_pool();
+  if (rc) return rc;
+  void* q = nullptr;
+  V3DBA_CUDA_TRY(cudaMallocAsync(&q, std::max<size_t>(total, 256), st));
+  base = static_cast<char*>(q);
+  size_t off = 0;
+  for (const Req& r : req_) {
+    *r.p = base + off;
+    off += r.bytes;
+  }
+  return V3DBA_OK;
+}
+
+void Arena::release(cudaStream_t st) {
+  if (base) cudaFreeAsync(base, st);
+  base = nullptr;
 }
 
 int ensure_pool() {

@@ -215,20 +215,6 @@ int use_gnn(v3dba_handle h, bool learned) {
   return V3DBA_OK;
 }
 
-// Phase timings of v3dba_create on stderr when V3DBA_TRACE_CREATE is set (diagnostics).
-struct CreateTrace {
-  bool on = std::getenv("V3DBA_TRACE_CREATE") != nullptr;
-  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
-  void mark(const char* phase, cudaStream_t st = nullptr) {
-    if (!on) return;
-    if (st) cudaStreamSynchronize(st);
-    const auto now = std::chrono::steady_clock::now();
-    std::fprintf(stderr, "v3dba_create %-12s %8.3f ms\n", phase,
-                 std::chrono::duration<double, std::milli>(now - t).count());
-    t = now;
-  }
-};
-
 // o_sub[k] = subcamera of the caller's observation o_orig[k] (point-major order)
 __global__ void k_gather_sub(const int* __restrict__ sub, const int* __restrict__ orig, int K, int* __restrict__ out) {
   const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -308,7 +294,7 @@ uint64_t v3dba_launch_count(void) { return g_launches.load(); }
 
 int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   if (!p || !out) return V3DBA_ERR_INVALID_ARGUMENT;
-  CreateTrace trace;
+  PhaseTrace trace("V3DBA_TRACE_CREATE", "v3dba_create");
   *out = nullptr;
   int dA, dC;
   int rc = dims_of(p->model, p->mode, &dA, &dC);
