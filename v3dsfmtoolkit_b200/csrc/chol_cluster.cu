@@ -6,13 +6,16 @@
 // (barrier.cluster, sub-microsecond) instead of kernel boundaries, which removes the launch and
 // drain latency that dominates small reduced systems (hundreds to a few thousand unknowns).
 //
-// Per tile column k:
-//   A  CTA 0 factors the diagonal tile: 16-column blocking, each 16x16 diagonal block factored
-//      and inverted by one warp in registers (shuffles), panels and trailing blocks updated with
-//      FP64 tensor-core MMAs (DMMA m8n8k4); it also assembles Z = L_kk^-1.
-//   B  panel tiles (and the rhs row): L_rk = A_rk Z^T, one 64x64x64 DMMA GEMM per tile.
-//   C  trailing tiles: A_rc -= L_rk L_ck^T (DMMA).
-// Then the back-substitution L^T x = y (y = the factored rhs row) by CTA 0 with coalesced loads.
+// Per tile column k, CTA 0 owns the chain along the diagonal and keeps it in shared memory:
+//   with Z_k = L_kk^-1 resident it forms the panel tile next to the diagonal,
+//   L_{k+1,k} = A_{k+1,k} Z_k^T, publishes it (split cluster barrier: arrive, keep working), applies
+//   it to the next diagonal tile (fetched meanwhile) and factors that tile: 16-column blocking,
+//   each 16x16 diagonal block factored and inverted by one warp in registers, panels and trailing
+//   blocks updated with FP64 tensor-core MMAs (DMMA m8n8k4), Z_{k+1} assembled;
+//   CTAs 1.. form the other panel tiles (and the rhs row), L_rk = A_rk Z_k^T, one 64x64x64 DMMA
+//   GEMM per tile, then the other trailing tiles, A_rc -= L_rk L_ck^T (DMMA).
+// Then the back-substitution L^T x = y (y = the factored rhs row) by CTA 0, with x kept in
+// shared memory and Z_kk fetched ahead of the dependent sums.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -249,6 +252,11 @@ __device__ __forceinline__ void tile_wait() { asm volatile("cp.async.wait_all;\n
 
 }  // namespace
 
+// Split cluster barrier: arrive (release: this CTA's writes become visible to the cluster) and
+// wait (acquire).  A CTA may do independent work between the two.
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
     k_chol_cluster(double* __restrict__ S, int ld, int nt, int n_pad, const int* __restrict__ pptr,
                    const int* __restrict__ prows, const int* __restrict__ uptr, const int* __restrict__ ur,
@@ -259,17 +267,36 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
   extern __shared__ double sm[];
   double* T0 = sm;
   double* T1 = sm + TB * LDT;
+  double* T2 = sm + 2 * TB * LDT;   // rank 0 only: the next diagonal tile
   const size_t lds = (size_t)ld;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
 
-  // CTA 0 factors a diagonal tile and publishes Z = L_kk^-1 for the panel phase.
-  auto factor_diag = [&](int k) {
-    const size_t k0 = (size_t)k * TB;
+  // global tile at (r0, c0) = acc (op 0) or -= acc (op 1); optionally also into the shared tile
+  // Csm (col-major LDT)
+  auto store_acc = [&](const double (&acc)[2][2][2][2], size_t r0, size_t c0, int op, double* Csm) {
+    const int bi = w >> 1;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int bj = 2 * (w & 1) + h;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int col = 16 * bj + 8 * b + 2 * q + i, row = 16 * bi + 8 * a + g;
+            double* gp = S + (c0 + col) * lds + r0 + row;
+            if (op == 0) *gp = acc[h][a][b][i];
+            else *gp -= acc[h][a][b][i];
+            if (Csm) Csm[col * LDT + row] = acc[h][a][b][i];
+          }
+    }
+  };
+  // rank 0: factor the diagonal tile held in T2; Z = L^-1 into T1 (kept for the next panel) and to
+  // global (for the other CTAs' panels and the back-substitution)
+  auto factor_resident = [&](int k) {
     __syncthreads();
-    load_tile(T0, S, lds, k0, k0);
-    tile_wait();
-    __syncthreads();
-    const bool ok = cta_factor_tile(T0, T1);
+    const bool ok = cta_factor_tile(T2, T1);
     if (!ok && tid == 0) atomicExch(fail, 1);
     double* Z = ldiag + (size_t)k * TB * TB;
     for (int e = tid; e < TB * TB; e += blockDim.x) Z[e] = T1[(e >> 6) * LDT + (e & 63)];
@@ -284,20 +311,8 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
     __syncthreads();
     double acc[2][2][2][2];
     cta_gemm_abt(acc, T0, c0 != r0 ? T1 : T0);
-    const int bi = w >> 1;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int bj = 2 * (w & 1) + h;
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-          for (int i = 0; i < 2; ++i)
-            S[(c0 + 16 * bj + 8 * b + 2 * q + i) * lds + r0 + 16 * bi + 8 * a + g] -= acc[h][a][b][i];
-    }
+    store_acc(acc, r0, c0, 1, nullptr);
   };
-
   // optional phase timestamps (ns): trace[(2 k + phase) * kCluster + rank]
   auto stamp = [&](int slot) {
     if (trace != nullptr && tid == 0) {
@@ -306,16 +321,65 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
       trace[(size_t)slot * kCluster + rank] = t;
     }
   };
-  if (rank == 0) factor_diag(0);
+  if (rank == 0) {
+    load_tile(T2, S, lds, 0, 0);
+    tile_wait();
+    factor_resident(0);
+  }
   __threadfence();
   cl.sync();
+  // Per tile step k: CTA 0 owns the chain along the diagonal (panel L_{k+1,k} with Z_k resident,
+  // the update of the next diagonal tile in shared memory, its factor); CTAs 1.. form the other
+  // panel tiles and apply the other trailing updates.  CTA 0 publishes L_{k+1,k} with a split
+  // barrier and factors while the others work.
   for (int k = 0; k < nt; ++k) {
     const size_t k0 = (size_t)k * TB;
+    const int p0 = pptr[k], np = pptr[k + 1] - p0;
+    const bool has_next = k + 1 < nt;
+    const bool diag_panel = has_next && np > 0 && prows[p0] == k + 1;   // rows are listed ascending
     stamp(2 * k);
-    // B: panel tiles L_rk = A_rk Z^T (the rhs row included)
-    {
-      const int p0 = pptr[k], np = pptr[k + 1] - p0;
-      if (rank < np) {
+    if (rank == 0) {
+      if (has_next) {
+        __syncthreads();
+        load_tile(T2, S, lds, k0 + TB, k0 + TB);   // the next diagonal tile, fetched meanwhile
+        if (diag_panel) {
+          load_tile(T0, S, lds, k0 + TB, k0);
+          tile_wait();
+          __syncthreads();
+          double acc[2][2][2][2];
+          cta_gemm_abt(acc, T0, T1);              // L_{k+1,k} = A_{k+1,k} Z_k^T
+          __syncthreads();                        // T0 is overwritten with L_{k+1,k}
+          store_acc(acc, k0 + TB, k0, 0, T0);
+        }
+      }
+      __threadfence();
+      cluster_arrive();                           // L_{k+1,k} is published
+      if (has_next) {
+        tile_wait();
+        __syncthreads();
+        if (diag_panel) {                         // A_{k+1,k+1} -= L_{k+1,k} L_{k+1,k}^T in place
+          double acc[2][2][2][2];
+          cta_gemm_abt(acc, T0, T0);
+          const int bi = w >> 1;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int bj = 2 * (w & 1) + h;
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+              for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+                  T2[(16 * bj + 8 * b + 2 * q + i) * LDT + 16 * bi + 8 * a + g] -= acc[h][a][b][i];
+          }
+        }
+        factor_resident(k + 1);
+      }
+      cluster_wait();
+    } else {
+      // B: the other panel tiles L_rk = A_rk Z^T (the rhs row included)
+      const int first = diag_panel ? 1 : 0;
+      if (np - first > 0) {
         const double* Z = ldiag + (size_t)k * TB * TB;
         __syncthreads();
         for (int e = tid; e < TB * TB / 2; e += blockDim.x) {
@@ -325,7 +389,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
         }
         asm volatile("cp.async.commit_group;\n" ::);
       }
-      for (int t = rank; t < np; t += kCluster) {
+      for (int t = first + rank - 1; t < np; t += kCluster - 1) {
         const size_t r0 = (size_t)prows[p0 + t] * TB;
         __syncthreads();
         load_tile(T0, S, lds, r0, k0);
@@ -333,53 +397,44 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
         __syncthreads();
         double acc[2][2][2][2];
         cta_gemm_abt(acc, T0, T1);
-        const int bi = w >> 1;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int bj = 2 * (w & 1) + h;
-#pragma unroll
-          for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b)
-#pragma unroll
-              for (int i = 0; i < 2; ++i)
-                S[(k0 + 16 * bj + 8 * b + 2 * q + i) * lds + r0 + 16 * bi + 8 * a + g] = acc[h][a][b][i];
-        }
+        store_acc(acc, r0, k0, 0, nullptr);
       }
       __threadfence();
-    }
-    cl.sync();
-    stamp(2 * k + 1);
-    // C: trailing tiles.  Lookahead: CTA 0 applies the update of the next diagonal tile and
-    // factors it at once; CTAs 1.. take the other trailing tiles.
-    {
+      cluster_arrive();
+      cluster_wait();
+      stamp(2 * k + 1);
+      // C: trailing tiles other than the next diagonal one (CTA 0's)
       const int u0 = uptr[k], nu = uptr[k + 1] - u0;
-      if (rank == 0) {
-        if (k + 1 < nt) {
-          for (int t = 0; t < nu; ++t)
-            if (ur[u0 + t] == k + 1 && uc[u0 + t] == k + 1) { update_tile(k, k + 1, k + 1); break; }
-          factor_diag(k + 1);
-        }
-      } else {
-        int slot = 0;
-        for (int t = 0; t < nu; ++t) {
-          if (ur[u0 + t] == k + 1 && uc[u0 + t] == k + 1) continue;
-          if (slot++ % (kCluster - 1) != rank - 1) continue;
-          update_tile(k, ur[u0 + t], uc[u0 + t]);
-        }
+      int slot = 0;
+      for (int t = 0; t < nu; ++t) {
+        if (ur[u0 + t] == k + 1 && uc[u0 + t] == k + 1) continue;
+        if (slot++ % (kCluster - 1) != rank - 1) continue;
+        update_tile(k, ur[u0 + t], uc[u0 + t]);
       }
-      __threadfence();
     }
+    __threadfence();
     cl.sync();
   }
 
   stamp(2 * nt);
-  // back-substitution L^T x = y on CTA 0:  x_k = Z_kk^T (y_k - sum_{r > k} L_rk^T x_r)
+  // back-substitution L^T x = y on CTA 0:  x_k = Z_kk^T (y_k - sum_{r > k} L_rk^T x_r).  The
+  // solution stays in shared memory (T1/T2 are free by now) when it fits, and Z_kk is fetched
+  // into registers before the dependent sums so that its latency overlaps them.
   if (rank != 0) return;
   double* v = T0;             // 64 entries
   double* part = T0 + 64;     // 8 warps x 64
+  const bool xs_ok = n_pad <= 2 * TB * LDT;
+  double* xs = xs_ok ? T1 : x;
   for (int k = nt - 1; k >= 0; --k) {
     const size_t k0 = (size_t)k * TB;
+    const double* Z = ldiag + (size_t)k * TB * TB;
+    double z0[8], z1[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double* zc = Z + (size_t)(8 * w + c) * TB;
+      z0[c] = zc[lane];
+      z1[c] = zc[32 + lane];
+    }
     // warp w handles columns 8w..8w+7 of tile column k; lanes run over rows (coalesced)
     double sums[8];
 #pragma unroll
@@ -388,7 +443,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
       const int r = prows[p];
       if (r >= nt) continue;
       const size_t r0 = (size_t)r * TB;
-      const double x0 = x[r0 + lane], x1 = x[r0 + 32 + lane];
+      const double x0 = xs[r0 + lane], x1 = xs[r0 + 32 + lane];
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         const double* col = S + (k0 + 8 * w + c) * lds + r0;
@@ -401,20 +456,20 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
       if (lane == 0) v[8 * w + c] = S[(k0 + 8 * w + c) * lds + n_pad] - s;
     }
     __syncthreads();
-    // x_k[col] = sum_m Z[m][col] v[m]  (Z col-major 64x64 in ldiag)
-    const double* Z = ldiag + (size_t)k * TB * TB;
+    // x_k[col] = sum_m Z[m][col] v[m]  (Z col-major 64x64)
+    const double v0 = v[lane], v1 = v[32 + lane];
     double zs[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const double* zc = Z + (size_t)(8 * w + c) * TB;
-      zs[c] = warp_sum(zc[lane] * v[lane] + zc[32 + lane] * v[32 + lane]);
-    }
+    for (int c = 0; c < 8; ++c) zs[c] = warp_sum(z0[c] * v0 + z1[c] * v1);
     if (lane == 0) {
 #pragma unroll
       for (int c = 0; c < 8; ++c) part[8 * w + c] = zs[c];
     }
     __syncthreads();
-    if (tid < TB) x[k0 + tid] = part[tid];
+    if (tid < TB) {
+      xs[k0 + tid] = part[tid];
+      if (xs_ok) x[k0 + tid] = part[tid];
+    }
     __syncthreads();
     __threadfence_block();
   }
@@ -425,7 +480,7 @@ int chol_cluster_setup() {
   static bool done = false;
   if (done) return V3DBA_OK;
   V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * TB * LDT * sizeof(double))));
+                                      (int)(3 * TB * LDT * sizeof(double))));
   done = true;
   return V3DBA_OK;
 }
@@ -434,7 +489,7 @@ int chol_cluster_solve(const TileChol& tc, double* S, double* x, int* d_fail, cu
                        unsigned long long* trace) {
   int rc = chol_cluster_setup();
   if (rc) return rc;
-  const size_t smem = 2 * TB * LDT * sizeof(double);
+  const size_t smem = 3 * TB * LDT * sizeof(double);
   k_chol_cluster<<<kCluster, 256, smem, st>>>(S, tc.ld, tc.nt, tc.n_pad, tc.d_panel_ptr, tc.d_panel_rows,
                                               tc.d_upd_ptr, tc.d_upd_r, tc.d_upd_c, tc.d_ldiag, x, d_fail, trace);
   V3DBA_LAUNCH_CHECK();
