@@ -44,7 +44,7 @@ EXPORTS = (
     "v3dba_rotations_create", "v3dba_rotations_destroy", "v3dba_rotations_minimize", "v3dba_rotations_get",
     "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost", "v3dba_rotations_set_group",
     "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
-    "v3dba_triplet_stage_flat",
+    "v3dba_triplet_stage_flat", "v3dba_cholesky_schedule", "v3dba_tile_schedule",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -137,6 +137,9 @@ def _lib():
         L.v3dba_batch_get_all_params.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.v3dba_measure_fp64_mma_peak.argtypes = [_dp]
         L.v3dba_cholesky_flops.argtypes = [C.c_void_p, _dp]
+        L.v3dba_cholesky_schedule.argtypes = [C.c_void_p, _ip, _ip, _ip]
+        L.v3dba_tile_schedule.argtypes = [C.c_int, C.POINTER(C.c_uint8), _ip, _ip, _ip, _dp, _ip, C.c_int, _ip,
+                                          _ip]
         L.v3dba_structure.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int)] + [_ip] * 8
         _fp = C.POINTER(C.c_float)
         L.v3dba_precond_model_size.argtypes = []
@@ -195,6 +198,10 @@ def check(rc, what=""):
 
 def _d(a):
     return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
 
 
 def _f64(a):
@@ -336,11 +343,44 @@ class Handle:
         check(_lib().v3dba_cholesky_flops(self.h, C.byref(f)), "v3dba_cholesky_flops")
         return f.value
 
+    def cholesky_schedule(self):
+        """("levels" | "steps", number of levels, number of tile columns) of the dense solve."""
+        sch, nl, nt = C.c_int32(), C.c_int32(), C.c_int32()
+        check(_lib().v3dba_cholesky_schedule(self.h, C.byref(sch), C.byref(nl), C.byref(nt)),
+              "v3dba_cholesky_schedule")
+        return ("levels" if sch.value else "steps"), nl.value, nt.value
+
     def reduced_system(self, lam, precision=PRECISION_FP64):
         n = self.n_cams * self.dA + self.dC
         S, rhs = np.zeros((n, n)), np.zeros(n)
         check(_lib().v3dba_reduced_system(self.h, precision, float(lam), _d(S), _d(rhs)), "v3dba_reduced_system")
         return S, rhs
+
+
+LEVEL_PLAN_FIELDS = ("p1ptr", "p1", "p2ptr", "p2", "task_r", "task_c", "task_mode", "task_cptr", "ck", "perm",
+                     "bptr", "brow")
+
+
+def tile_schedule(pattern):
+    """The level schedule of the tile Cholesky for a lower-triangle tile pattern (nt x nt bool):
+    dict(order, n_levels, uses_levels, est_levels_us, est_steps_us, plan={field: int array})."""
+    pat = np.ascontiguousarray(np.asarray(pattern, dtype=bool).astype(np.uint8))
+    nt = pat.shape[0]
+    L = _lib()
+    order = np.zeros(nt, np.int32)
+    nl, use, plen = C.c_int32(), C.c_int32(), C.c_int32()
+    est = np.zeros(2)
+    offs = np.zeros(len(LEVEL_PLAN_FIELDS), np.int32)
+    u8 = pat.ctypes.data_as(C.POINTER(C.c_uint8))
+    check(L.v3dba_tile_schedule(nt, u8, _i(order), C.byref(nl), C.byref(use), _d(est), None, 0, C.byref(plen),
+                                _i(offs)), "v3dba_tile_schedule")
+    buf = np.zeros(max(plen.value, 1), np.int32)
+    check(L.v3dba_tile_schedule(nt, u8, _i(order), C.byref(nl), C.byref(use), _d(est), _i(buf), len(buf),
+                                C.byref(plen), _i(offs)), "v3dba_tile_schedule")
+    bounds = list(offs) + [plen.value]
+    plan = {f: buf[bounds[i]:bounds[i + 1]].copy() for i, f in enumerate(LEVEL_PLAN_FIELDS)} if plen.value else {}
+    return dict(order=order, n_levels=nl.value, uses_levels=bool(use.value), est_levels_us=float(est[0]),
+                est_steps_us=float(est[1]), plan=plan)
 
 
 def dense_cholesky_solve(S, rhs):

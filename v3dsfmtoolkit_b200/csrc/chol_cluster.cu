@@ -78,68 +78,63 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
   return y;
 }
 
+// 1/x for a positive pivot: the hardware approximation (rcp.approx.ftz.f64) refined by two
+// Newton-Raphson steps for the reciprocal, y <- y + y (1 - x y), each of which roughly doubles
+// the number of correct bits (two dependent FMAs per step).
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  return y;
+}
+
 // One warp: Cholesky of the 16x16 block D (lower, col-major ld LDT) in place and its inverse
 // into Z (16x16, col-major, zero upper part).  Returns false on a non-positive pivot.
-// Lane c (< 16) owns column c in registers.  At pivot j lane j scales its column by one
-// reciprocal square root and stores it to D; after a warp barrier every lane reads that column
-// back with broadcast vector loads and applies its rank-1 update.  The inverse is then formed
-// column by column (lane c computes Z[:, c]) from broadcast reads of L.
-__device__ bool warp_chol_inv16(double* D, double* Z) {
+// Gaussian elimination in registers, both halves of the warp running the same instructions:
+// lane c < 16 holds column c of the symmetric trailing matrix (both triangles), lane 16 + c
+// column c of W, which starts as the identity and receives the same row operations.  At pivot j
+// the pivot column (lane j) is broadcast with shuffles and every lane applies
+// v[r] -= A[r][j] (v[j] / A[j][j]) for r > j (lanes c <= j of the first half are done).  Then
+// A = U D U^T with U unit lower (column c of U D is lane c's column at its pivot), W = U^-1, and
+// L = U D^1/2, L^-1 = D^-1/2 W.  Only a reciprocal of the pivot is on the chain from one pivot
+// to the next; the square roots are taken once at the end.
+__device__ __noinline__ bool warp_chol_inv16(double* D, double* Z) {
   const int lane = threadIdx.x & 31;
-  const int c = lane;                 // owned column (lanes >= 16 own none)
-  __shared__ double inv_diag[8][16];  // per-warp reciprocal diagonal of L
-  double* invd = inv_diag[threadIdx.x >> 5];
-  double a[16];
+  const int c = lane & 15;
+  const bool a_half = lane < 16;
+  double v[16];
 #pragma unroll
-  for (int r = 0; r < 16; ++r) a[r] = (c < 16 && r >= c) ? D[c * LDT + r] : 0.0;
+  for (int r = 0; r < 16; ++r)
+    v[r] = a_half ? (r >= c ? D[c * LDT + r] : D[r * LDT + c]) : (r == c ? 1.0 : 0.0);
+  __shared__ double rs_all[8][16];   // per warp: 1/sqrt of the pivots
+  double* rs = rs_all[threadIdx.x >> 5];
   bool ok = true;
+  double piv = 1.0;   // this lane's column's pivot
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    if (c == j) {
-      const double d = a[j];
-      const double rs = d > 0.0 ? rsqrt_nr(d) : 1.0;
-      if (!(d > 0.0)) ok = false;
-      invd[j] = rs;
-      a[j] = d * rs;
+    const double d = __shfl_sync(FULL, v[j], j);
+    if (!(d > 0.0)) ok = false;
+    if (c == j) piv = d;
+    const double m = v[j] * rcp_nr(d > 0.0 ? d : 1.0);
+    const bool upd = !a_half || c > j;
 #pragma unroll
-      for (int r = j + 1; r < 16; ++r) a[r] *= rs;
-      double2* col = reinterpret_cast<double2*>(D + j * LDT);
-#pragma unroll
-      for (int r = 0; r < 16; r += 2) col[r / 2] = make_double2(r >= j ? a[r] : 0.0, r + 1 >= j ? a[r + 1] : 0.0);
+    for (int r = j + 1; r < 16; ++r) {
+      const double col = __shfl_sync(FULL, v[r], j);
+      if (upd) v[r] = fma(-col, m, v[r]);
     }
-    __syncwarp();
-    if (c > j && c < 16) {
-      const double2* col = reinterpret_cast<const double2*>(D + j * LDT);
-      double l[16];
-#pragma unroll
-      for (int r = 0; r < 16; r += 2) {
-        const double2 v = col[r / 2];
-        l[r] = v.x;
-        l[r + 1] = v.y;
-      }
-      const double m = D[j * LDT + c];
-#pragma unroll
-      for (int r = j + 1; r < 16; ++r)
-        if (r >= c) a[r] -= l[r] * m;
-    }
-    __syncwarp();
   }
-  ok = __all_sync(FULL, ok);
-  // Z[:, c]: z[rr] = (delta_{rr,c} - sum_{t<rr} L[rr][t] z[t]) / L[rr][rr]
-  if (c < 16) {
-    double z[16];
+  const double sc = rsqrt_nr(piv > 0.0 ? piv : 1.0);
+  if (a_half) rs[c] = sc;
+  __syncwarp();
+  if (a_half) {
 #pragma unroll
-    for (int rr = 0; rr < 16; ++rr) {
-      double s0 = (rr == c) ? 1.0 : 0.0, s1 = 0.0;
+    for (int r = 0; r < 16; ++r) D[c * LDT + r] = r >= c ? v[r] * sc : 0.0;
+  } else {
 #pragma unroll
-      for (int t = 0; t < rr; t += 2) {
-        s0 -= D[t * LDT + rr] * z[t];
-        if (t + 1 < rr) s1 -= D[(t + 1) * LDT + rr] * z[t + 1];
-      }
-      z[rr] = (rr >= c) ? (s0 + s1) * invd[rr] : 0.0;
-    }
-#pragma unroll
-    for (int rr = 0; rr < 16; ++rr) Z[c * LDT + rr] = z[rr];
+    for (int r = 0; r < 16; ++r) Z[c * LDT + r] = r >= c ? v[r] * rs[r] : 0.0;
   }
   __syncwarp();
   return ok;
@@ -160,63 +155,77 @@ __device__ __forceinline__ void acc_store(const double (&acc)[2][2][2], double* 
 }
 
 // CTA (256 threads): factor the 64x64 tile A (shared, col-major LDT, lower triangle valid) in
-// place and write Z = L^-1 (full 64x64, zero upper part) into Zs.  Blocked by 16 columns: each
-// 16x16 diagonal block is factored and inverted by one warp (warp_chol_inv16); the panel blocks
-// (L_ip = A_ip Z_pp^T), the trailing blocks (A_ij -= L_ip L_jp^T) and the off-diagonal blocks of
-// Z (Z_ij = -Z_ii sum_t L_it Z_tj, by distance i - j) are 16x16 DMMA products.  Returns false
-// on a non-positive pivot.
+// place and write Z = L^-1 (full 64x64, zero upper part) into Zs.  Blocked by 16 columns with
+// lookahead: warp 0 carries the chain of diagonal blocks (update of the next diagonal block by
+// the panel just formed, then its factor and inverse, warp_chol_inv16) while warps 1..7 apply the
+// other trailing updates (A_ij -= L_ip L_jp^T) and form block row p of Z
+// (Z_pj = -Z_pp sum_{t=j}^{p-1} L_pt Z_tj); the panel blocks L_ip = A_ip Z_pp^T are formed by
+// the first warps between.  All products are 16x16 DMMA tiles.  Returns false on a non-positive
+// pivot.  (The upper blocks of Zs are zeroed before the first block is factored, not beside it:
+// on B200 the first block factor ran an order of magnitude slower with the zeroing stores of the
+// other warps alongside.)
 __device__ bool cta_factor_tile(double* A, double* Zs) {
   const int tid = threadIdx.x, w = tid >> 5;
   __shared__ int s_ok;
   if (tid == 0) s_ok = 1;
-  for (int e = tid; e < TB * TB; e += blockDim.x) Zs[(e >> 6) * LDT + (e & 63)] = 0.0;
+  for (int e = tid; e < 6 * 256; e += blockDim.x) {   // the strictly upper blocks (bi < bj)
+    const int b = e >> 8, q = e & 255;
+    const int bi = b < 3 ? 0 : b < 5 ? 1 : 2;
+    const int bj = b < 3 ? 1 + b : b < 5 ? b - 1 : 3;
+    Zs[(16 * bj + (q >> 4)) * LDT + 16 * bi + (q & 15)] = 0.0;
+  }
+  __syncthreads();
+  if (w == 0 && !warp_chol_inv16(A, Zs) && (tid & 31) == 0) s_ok = 0;
   __syncthreads();
   for (int p = 0; p < 4; ++p) {
-    double* App = A + 16 * p * LDT + 16 * p;
+    if (p < 3) {
+      if (w < 3 - p) {   // panel blocks L_ip = A_ip Z_pp^T
+        const int i = p + 1 + w;
+        double acc[2][2][2];
+        acc_zero(acc);
+        warp_mma16(acc, A + 16 * p * LDT + 16 * i, 1, LDT, Zs + 16 * p * LDT + 16 * p, LDT, 1, 16);
+        __syncwarp();
+        acc_store(acc, A + 16 * p * LDT + 16 * i, LDT, 1.0, 0.0);
+      }
+      __syncthreads();
+    }
     if (w == 0) {
-      const bool ok = warp_chol_inv16(App, Zs + 16 * p * LDT + 16 * p);
-      if ((threadIdx.x & 31) == 0 && !ok) s_ok = 0;
-    }
-    __syncthreads();
-    if (w < 3 - p) {
-      const int i = p + 1 + w;
-      double acc[2][2][2];
-      acc_zero(acc);
-      const double* Aip = A + 16 * p * LDT + 16 * i;
-      const double* Zpp = Zs + 16 * p * LDT + 16 * p;
-      warp_mma16(acc, Aip, 1, LDT, Zpp, LDT, 1, 16);   // A_ip Z_pp^T
-      __syncwarp();
-      acc_store(acc, A + 16 * p * LDT + 16 * i, LDT, 1.0, 0.0);
-    }
-    __syncthreads();
-    {
+      if (p < 3) {   // the next diagonal block: A_qq -= L_qp L_qp^T, then its factor and inverse
+        const int q1 = p + 1;
+        double acc[2][2][2];
+        acc_zero(acc);
+        warp_mma16(acc, A + 16 * p * LDT + 16 * q1, 1, LDT, A + 16 * p * LDT + 16 * q1, LDT, 1, 16);
+        acc_store(acc, A + 16 * q1 * LDT + 16 * q1, LDT, -1.0, 1.0);
+        __syncwarp();
+        if (!warp_chol_inv16(A + 16 * q1 * LDT + 16 * q1, Zs + 16 * q1 * LDT + 16 * q1) && (tid & 31) == 0)
+          s_ok = 0;
+      }
+    } else {
       int task = 0;
       for (int i = p + 1; i < 4; ++i)
-        for (int j = p + 1; j <= i; ++j, ++task) {
-          if (task % 8 != w) continue;
+        for (int j = p + 1; j <= i; ++j) {
+          if (i == p + 1 && j == p + 1) continue;
+          if (task++ % 7 != w - 1) continue;
           double acc[2][2][2];
           acc_zero(acc);
           warp_mma16(acc, A + 16 * p * LDT + 16 * i, 1, LDT, A + 16 * p * LDT + 16 * j, LDT, 1, 16);
           acc_store(acc, A + 16 * j * LDT + 16 * i, LDT, -1.0, 1.0);
         }
-    }
-    __syncthreads();
-  }
-  for (int d = 1; d < 4; ++d) {
-    if (w < 4 - d) {
-      const int j = w, i = w + d;
-      double acc[2][2][2];
-      acc_zero(acc);
-      for (int t = j; t < i; ++t)
-        warp_mma16(acc, A + 16 * t * LDT + 16 * i, 1, LDT, Zs + 16 * j * LDT + 16 * t, 1, LDT, 16);
-      double* Wij = Zs + 16 * j * LDT + 16 * i;   // still zero: use it as scratch for W
-      acc_store(acc, Wij, LDT, 1.0, 0.0);
-      __syncwarp();
-      double acc2[2][2][2];
-      acc_zero(acc2);
-      warp_mma16(acc2, Zs + 16 * i * LDT + 16 * i, 1, LDT, Wij, 1, LDT, 16);
-      __syncwarp();
-      acc_store(acc2, Wij, LDT, -1.0, 0.0);
+      for (int j = 0; j < p; ++j) {
+        if (task++ % 7 != w - 1) continue;
+        double acc[2][2][2];
+        acc_zero(acc);
+        for (int t = j; t < p; ++t)
+          warp_mma16(acc, A + 16 * t * LDT + 16 * p, 1, LDT, Zs + 16 * j * LDT + 16 * t, 1, LDT, 16);
+        double* Wpj = Zs + 16 * j * LDT + 16 * p;   // the block itself holds W = sum L Z meanwhile
+        acc_store(acc, Wpj, LDT, 1.0, 0.0);
+        __syncwarp();
+        double acc2[2][2][2];
+        acc_zero(acc2);
+        warp_mma16(acc2, Zs + 16 * p * LDT + 16 * p, 1, LDT, Wpj, 1, LDT, 16);
+        __syncwarp();
+        acc_store(acc2, Wpj, LDT, -1.0, 0.0);
+      }
     }
     __syncthreads();
   }
@@ -234,6 +243,20 @@ __device__ __forceinline__ void cta_gemm_abt(double (&acc)[2][2][2][2], const do
     acc_zero(acc[h]);
     // A(m,t) = A[t*LDT + 16 bi + m]; B(t,n) = B(n,t) = B[t*LDT + 16 bj + n]
     warp_mma16(acc[h], A + 16 * bi, 1, LDT, B + 16 * bj, LDT, 1, TB);
+  }
+}
+
+// CTA: acc += A B^T for shared tiles A, B (col-major LDT), with the same fragment ownership as
+// cta_gemm_abt; A is read transposed (A(m,t) = A[m*LDT + t]) when a_t.
+__device__ __forceinline__ void cta_gemm_abt_acc(double (&acc)[2][2][2][2], const double* A, bool a_t,
+                                                 const double* B) {
+  const int w = threadIdx.x >> 5;
+  const int bi = w >> 1;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int bj = 2 * (w & 1) + h;
+    if (a_t) warp_mma16(acc[h], A + 16 * bi * LDT, LDT, 1, B + 16 * bj, LDT, 1, TB);
+    else warp_mma16(acc[h], A + 16 * bi, 1, LDT, B + 16 * bj, LDT, 1, TB);
   }
 }
 
@@ -476,10 +499,236 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
   stamp(2 * nt + 1);
 }
 
+// Pointers into the packed level plan (TileChol::h_lv on the device).
+struct LevelPlanPtrs {
+  const int *p1ptr, *p1, *p2ptr, *p2, *tr, *tc, *tmode, *tcptr, *ck, *perm, *bptr, *brow;
+  int n_levels;
+};
+
+// Level-scheduled tile Cholesky + solve in one launch of an 8-CTA cluster, under the tile order
+// and schedule of tile_levels_plan.  Logical tile (r, c) lives at physical tile (perm r, perm c)
+// of S; its input, when the assembled tile is the mirrored (perm c, perm r), is read transposed.
+// Per level (columns that are independent of each other):
+//   phase 1: the columns of the previous level update every tile they reach,
+//            A_rc -= sum_k L_rk L_ck^T (one task per target tile, k in a fixed order), and the
+//            diagonal tiles of this level, their last updates in, are factored and inverted in
+//            shared memory (Z_j = L_jj^-1 to ldiag);
+//   phase 2: L_rj = A_rj Z_j^T for the off-diagonal tiles of this level's columns (the rhs row
+//            included);
+// the tasks of a phase are spread over the CTAs by the host, one cluster barrier after each
+// phase.  Every tile is written by one CTA per phase and its updates are summed in a fixed
+// order, so the result does not depend on timing.  Then the back-substitution, as in
+// k_chol_cluster.
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
+    k_chol_levels(double* __restrict__ S, int ld, int nt, int n_pad, LevelPlanPtrs P,
+                  double* __restrict__ ldiag, double* __restrict__ x, int* __restrict__ fail,
+                  unsigned long long* __restrict__ trace) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  extern __shared__ double sm[];
+  double* T0 = sm;
+  double* T1 = sm + TB * LDT;
+  double* T2 = sm + 2 * TB * LDT;
+  const size_t lds = (size_t)ld;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
+  auto stamp = [&](int slot) {
+    if (trace != nullptr && tid == 0) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      trace[(size_t)slot * kCluster + rank] = t;
+    }
+  };
+  // rhs row of tile column j (at physical column pc0): b_j -= sum_k L_jk y_k (phase 1) and
+  // y_j = Z_j b_j (phase 2); thread (group, col) sums every fourth t, groups combined in a fixed
+  // order through shared memory
+  double* red = T0;
+  auto rhs_update = [&](size_t pc0, int t) {
+    const int col = tid & 63, grp = tid >> 6;
+    double acc = 0.0;
+    for (int u = P.tcptr[t]; u < P.tcptr[t + 1]; ++u) {
+      const size_t pk0 = (size_t)P.perm[P.ck[u]] * TB;
+      for (int s = grp; s < TB; s += 4) acc += S[(pk0 + s) * lds + n_pad] * S[(pk0 + s) * lds + pc0 + col];
+    }
+    red[grp * TB + col] = acc;
+    __syncthreads();
+    if (tid < TB) {
+      double* b = S + (pc0 + tid) * lds + n_pad;
+      *b = *b - (((red[tid] + red[TB + tid]) + red[2 * TB + tid]) + red[3 * TB + tid]);
+    }
+  };
+  auto rhs_solve = [&](size_t pc0, int j) {
+    const int col = tid & 63, grp = tid >> 6;
+    const double* Z = ldiag + (size_t)j * TB * TB;
+    double acc = 0.0;
+    for (int s = grp; s < TB; s += 4) acc += S[(pc0 + s) * lds + n_pad] * Z[s * TB + col];
+    red[grp * TB + col] = acc;
+    __syncthreads();
+    if (tid < TB) S[(pc0 + tid) * lds + n_pad] = ((red[tid] + red[TB + tid]) + red[2 * TB + tid]) + red[3 * TB + tid];
+  };
+  // fragment element (h, a, b, i) of this thread: tile row and column
+  auto frag_row = [&](int a) { return 16 * (w >> 1) + 8 * a + g; };
+  auto frag_col = [&](int h, int b, int i) { return 16 * (2 * (w & 1) + h) + 8 * b + 2 * q + i; };
+
+  for (int lv = 0; lv < P.n_levels; ++lv) {
+    stamp(2 * lv);
+    for (int e = P.p1ptr[lv * kCluster + rank]; e < P.p1ptr[lv * kCluster + rank + 1]; ++e) {
+      const int t = P.p1[e];
+      const int r = P.tr[t], j = P.tc[t], mode = P.tmode[t] & 3;
+      const size_t pr0 = (size_t)P.perm[r] * TB, pc0 = (size_t)P.perm[j] * TB;
+      const bool diag = r == j, factor = (P.tmode[t] & kLvFactor) != 0;
+      __syncthreads();
+      if (r == nt) {   // the rhs row: only row 0 of its tiles is nonzero, so each update is a GEMV
+        rhs_update(pc0, t);
+        continue;
+      }
+      if (mode == 1) load_tile(T2, S, lds, pr0, pc0);
+      else if (mode == 2) load_tile(T2, S, lds, pc0, pr0);
+      double acc[2][2][2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) acc_zero(acc[h]);
+      for (int u = P.tcptr[t]; u < P.tcptr[t + 1]; ++u) {
+        const size_t pk0 = (size_t)P.perm[P.ck[u]] * TB;
+        load_tile(T0, S, lds, pr0, pk0);                 // L_rk
+        if (!diag) load_tile(T1, S, lds, pc0, pk0);      // L_jk
+        tile_wait();
+        __syncthreads();
+        cta_gemm_abt_acc(acc, T0, false, diag ? T0 : T1);
+        __syncthreads();
+      }
+      tile_wait();
+      __syncthreads();
+      if (factor) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+              for (int i = 0; i < 2; ++i) T2[frag_col(h, b, i) * LDT + frag_row(a)] -= acc[h][a][b][i];
+        __syncthreads();
+        const bool ok = cta_factor_tile(T2, T1);
+        if (!ok && tid == 0) atomicExch(fail, 1);
+        double* Z = ldiag + (size_t)j * TB * TB;
+        for (int f = tid; f < TB * TB; f += blockDim.x) Z[f] = T1[(f >> 6) * LDT + (f & 63)];
+      } else {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+              for (int i = 0; i < 2; ++i) {
+                const int row = frag_row(a), col = frag_col(h, b, i);
+                const double in = mode == 1 ? T2[col * LDT + row] : mode == 2 ? T2[row * LDT + col] : 0.0;
+                S[(pc0 + col) * lds + pr0 + row] = in - acc[h][a][b][i];
+              }
+      }
+    }
+    __threadfence();
+    cl.sync();
+    stamp(2 * lv + 1);
+    for (int e = P.p2ptr[lv * kCluster + rank]; e < P.p2ptr[lv * kCluster + rank + 1]; ++e) {
+      const int t = P.p2[e];
+      const int r = P.tr[t], j = P.tc[t];
+      const size_t pr0 = (size_t)P.perm[r] * TB, pc0 = (size_t)P.perm[j] * TB;
+      // an updated tile was written in place at (pr0, pc0); an untouched one is read as assembled
+      const bool tr_in = P.tmode[t] == 2;
+      __syncthreads();
+      if (r == nt) {
+        rhs_solve(pc0, j);
+        continue;
+      }
+      if (tr_in) load_tile(T0, S, lds, pc0, pr0);
+      else load_tile(T0, S, lds, pr0, pc0);
+      const double* Z = ldiag + (size_t)j * TB * TB;
+      for (int f = tid; f < TB * TB / 2; f += blockDim.x) {
+        const int c = f >> 5, m2 = (f & 31) * 2;
+        const unsigned saddr = (unsigned)__cvta_generic_to_shared(T1 + c * LDT + m2);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(Z + c * TB + m2));
+      }
+      asm volatile("cp.async.commit_group;\n" ::);
+      tile_wait();
+      __syncthreads();
+      double acc[2][2][2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) acc_zero(acc[h]);
+      cta_gemm_abt_acc(acc, T0, tr_in, T1);
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+              S[(pc0 + frag_col(h, b, i)) * lds + pr0 + frag_row(a)] = acc[h][a][b][i];
+    }
+    __threadfence();
+    cl.sync();
+  }
+
+  stamp(2 * P.n_levels);
+  // back-substitution L^T x = y on CTA 0 in reverse logical order, x indexed physically
+  if (rank != 0) return;
+  double* v = T0;
+  double* part = T0 + 64;
+  const bool xs_ok = n_pad <= 2 * TB * LDT;
+  double* xs = xs_ok ? T1 : x;
+  for (int k = nt - 1; k >= 0; --k) {
+    const size_t k0 = (size_t)P.perm[k] * TB;
+    const double* Z = ldiag + (size_t)k * TB * TB;
+    double z0[8], z1[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double* zc = Z + (size_t)(8 * w + c) * TB;
+      z0[c] = zc[lane];
+      z1[c] = zc[32 + lane];
+    }
+    double sums[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) sums[c] = 0.0;
+    for (int p = P.bptr[k]; p < P.bptr[k + 1]; ++p) {
+      const size_t r0 = (size_t)P.perm[P.brow[p]] * TB;
+      const double x0 = xs[r0 + lane], x1 = xs[r0 + 32 + lane];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const double* col = S + (k0 + 8 * w + c) * lds + r0;
+        sums[c] += col[lane] * x0 + col[32 + lane] * x1;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double s = warp_sum(sums[c]);
+      if (lane == 0) v[8 * w + c] = S[(k0 + 8 * w + c) * lds + n_pad] - s;
+    }
+    __syncthreads();
+    const double v0 = v[lane], v1 = v[32 + lane];
+    double zs[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) zs[c] = warp_sum(z0[c] * v0 + z1[c] * v1);
+    if (lane == 0) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) part[8 * w + c] = zs[c];
+    }
+    __syncthreads();
+    if (tid < TB) {
+      xs[k0 + tid] = part[tid];
+      if (xs_ok) x[k0 + tid] = part[tid];
+    }
+    __syncthreads();
+    __threadfence_block();
+  }
+  stamp(2 * P.n_levels + 1);
+}
+
 int chol_cluster_setup() {
   static bool done = false;
   if (done) return V3DBA_OK;
   V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(3 * TB * LDT * sizeof(double))));
+  V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(3 * TB * LDT * sizeof(double))));
   done = true;
   return V3DBA_OK;
@@ -492,6 +741,32 @@ int chol_cluster_solve(const TileChol& tc, double* S, double* x, int* d_fail, cu
   const size_t smem = 3 * TB * LDT * sizeof(double);
   k_chol_cluster<<<kCluster, 256, smem, st>>>(S, tc.ld, tc.nt, tc.n_pad, tc.d_panel_ptr, tc.d_panel_rows,
                                               tc.d_upd_ptr, tc.d_upd_r, tc.d_upd_c, tc.d_ldiag, x, d_fail, trace);
+  V3DBA_LAUNCH_CHECK();
+  return V3DBA_OK;
+}
+
+int chol_levels_solve(const TileChol& tc, double* S, double* x, int* d_fail, cudaStream_t st,
+                      unsigned long long* trace) {
+  if (!tc.levels || !tc.d_lv) return V3DBA_ERR_INVALID_ARGUMENT;
+  int rc = chol_cluster_setup();
+  if (rc) return rc;
+  const int* b = tc.d_lv;
+  LevelPlanPtrs P;
+  P.p1ptr = b + tc.lv_off[kLvP1Ptr];
+  P.p1 = b + tc.lv_off[kLvP1];
+  P.p2ptr = b + tc.lv_off[kLvP2Ptr];
+  P.p2 = b + tc.lv_off[kLvP2];
+  P.tr = b + tc.lv_off[kLvTaskR];
+  P.tc = b + tc.lv_off[kLvTaskC];
+  P.tmode = b + tc.lv_off[kLvTaskMode];
+  P.tcptr = b + tc.lv_off[kLvTaskCPtr];
+  P.ck = b + tc.lv_off[kLvCK];
+  P.perm = b + tc.lv_off[kLvPerm];
+  P.bptr = b + tc.lv_off[kLvBPtr];
+  P.brow = b + tc.lv_off[kLvBRow];
+  P.n_levels = tc.n_levels;
+  const size_t smem = 3 * TB * LDT * sizeof(double);
+  k_chol_levels<<<kCluster, 256, smem, st>>>(S, tc.ld, tc.nt, tc.n_pad, P, tc.d_ldiag, x, d_fail, trace);
   V3DBA_LAUNCH_CHECK();
   return V3DBA_OK;
 }

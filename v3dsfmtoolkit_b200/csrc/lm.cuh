@@ -160,7 +160,47 @@ struct TileChol {
   int* d_panel_ptr = nullptr;
   int* d_upd_ptr = nullptr;
   double* d_ldiag = nullptr;                    // nt inverted diagonal tiles (L_kk^-1)
+  // Level schedule under a nested-dissection order of the tiles (chol_order.cu).  When it
+  // shortens the chain of dependent diagonal factorisations enough, tile_chol_solve runs
+  // k_chol_levels with it instead of the column-by-column cluster kernel.
+  bool levels = false;
+  int n_levels = 0;
+  std::vector<int> h_order;                     // logical tile -> physical tile (nt + 1 entries)
+  std::vector<int> h_lv;                        // the packed plan (offsets in lv_off)
+  int lv_off[16] = {};
+  int* d_lv = nullptr;
+  double level_flops = 0.0;                     // algorithmic flops of the level schedule
+  double est_levels_us = 0.0, est_steps_us = 0.0;  // the cost model's estimates of both kernels
 };
+
+constexpr int kLvFactor = 4;
+// Offsets into TileChol::h_lv.
+enum LevelPlanField {
+  kLvP1Ptr = 0,   // [n_levels * 8 + 1] phase-1 task range of (level, cluster rank)
+  kLvP1,          // phase-1 task ids (updates from the previous level, diagonal factors)
+  kLvP2Ptr,       // [n_levels * 8 + 1] phase-2 task range of (level, cluster rank)
+  kLvP2,          // phase-2 task ids (off-diagonal tiles and the rhs row)
+  kLvTaskR,       // logical tile row of each task (nt: the rhs row)
+  kLvTaskC,       // logical tile column of each task
+  kLvTaskMode,    // where the input tile lives: 0 structurally zero, 1 S(pr, pc), 2 S(pc, pr)^T;
+                  // | kLvFactor on the phase-1 task that factors a diagonal tile
+  kLvTaskCPtr,    // [n_tasks + 1] updates of each task
+  kLvCK,          // the column k of each update A_rc -= L_rk L_ck^T (phase-1 tasks)
+  kLvPerm,        // [nt + 1] logical tile -> physical tile (entry nt: the rhs row)
+  kLvBPtr,        // [nt + 1] back-substitution: rows r > k, r < nt, of L's logical column k
+  kLvBRow,
+  kLvFields
+};
+// Orders the tiles (nested dissection of the tile graph, dense tiles last), builds the level
+// schedule and decides whether tile_chol_solve uses it.  orig: the lower-triangle tile pattern
+// before fill-in.
+int tile_levels_plan(TileChol& tc, const std::vector<uint8_t>& orig);
+// The host part of tile_levels_plan (no device work).
+int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig);
+// The nested-dissection order alone (logical -> physical tile), for tests and the cost model.
+std::vector<int> tile_nd_order(int nt, const std::vector<uint8_t>& orig);
+int chol_levels_solve(const TileChol& tc, double* S, double* x, int* d_fail, cudaStream_t st,
+                      unsigned long long* trace = nullptr);
 
 // Block-sparse reduced system for block-Jacobi PCG.
 struct PcgState {

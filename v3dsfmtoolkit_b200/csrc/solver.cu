@@ -813,6 +813,10 @@ extern "C" int v3dba_cholesky_flops(v3dba_handle h, double* flops) {
   const int rc = use_dense(h);
   if (rc) return rc;
   const TileChol& tc = h->chol;
+  if (tc.levels) {
+    *flops = tc.level_flops;
+    return V3DBA_OK;
+  }
   const double gemm = 2.0 * 64.0 * 64.0 * 64.0;
   // per tile column: the diagonal factor (L and L^-1, about 2/3 + 1/3 of 64^3) and one GEMM per
   // panel tile and per trailing tile
@@ -823,6 +827,17 @@ extern "C" int v3dba_cholesky_flops(v3dba_handle h, double* flops) {
     f += gemm * (tc.h_upd_ptr[k + 1] - tc.h_upd_ptr[k]);
   }
   *flops = f;
+  return V3DBA_OK;
+}
+
+extern "C" int v3dba_cholesky_schedule(v3dba_handle h, int* schedule, int* n_levels, int* nt) {
+  if (!h || !schedule || !n_levels || !nt) return V3DBA_ERR_INVALID_ARGUMENT;
+  const int rc = use_dense(h);
+  if (rc) return rc;
+  const TileChol& tc = h->chol;
+  *schedule = tc.levels ? 1 : 0;
+  *n_levels = tc.levels ? tc.n_levels : tc.nt;
+  *nt = tc.nt;
   return V3DBA_OK;
 }
 

@@ -242,6 +242,7 @@ int tile_chol_plan(TileChol& tc, int n, std::vector<uint8_t>& nz) {
   tc.ld = tc.n_pad + TB;
   if ((int)nz.size() != nt * nt) return V3DBA_ERR_INVALID_ARGUMENT;
   for (int k = 0; k < nt; ++k) nz[k * nt + k] = 1;
+  const std::vector<uint8_t> orig = nz;
   // tile-level symbolic factorisation (fill-in)
   std::vector<int> rows;
   for (int k = 0; k < nt; ++k) {
@@ -289,6 +290,7 @@ int tile_chol_plan(TileChol& tc, int n, std::vector<uint8_t>& nz) {
   if ((rc = up(&tc.d_upd_ptr, tc.h_upd_ptr))) return rc;
   if ((rc = up(&tc.d_tiles, tc.h_tiles))) return rc;
   V3DBA_CUDA_TRY(cudaMalloc(&tc.d_ldiag, sizeof(double) * (size_t)nt * TB * TB));
+  if ((rc = tile_levels_plan(tc, orig))) return rc;
   static bool attr_set = false;
   if (!attr_set) {
     V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -308,6 +310,7 @@ void tile_chol_free(TileChol& tc) {
   cudaFree(tc.d_upd_ptr);
   cudaFree(tc.d_tiles);
   cudaFree(tc.d_ldiag);
+  cudaFree(tc.d_lv);
   tc = TileChol();
 }
 
@@ -319,6 +322,7 @@ int tile_chol_zero(const TileChol& tc, double* S, double* /*rhs*/, cudaStream_t 
 }
 
 int tile_chol_solve(const TileChol& tc, double* S, double* x, int* d_fail, cudaStream_t st) {
+  if (tc.levels) return chol_levels_solve(tc, S, x, d_fail, st);
   return chol_cluster_solve(tc, S, x, d_fail, st);
 }
 
