@@ -446,16 +446,18 @@ int v3dba_cholesky_flops(v3dba_handle h, double* flops);
 int v3dba_cholesky_schedule(v3dba_handle h, int* schedule, int* n_levels, int* nt);
 
 /* The level schedule of the tile Cholesky for a lower-triangle tile pattern (nt x nt row-major,
- * entry (r, c) with r >= c nonzero when the tile is), computed on the host with no device work:
+ * entry (r, c) with r >= c nonzero when the tile is) and a cluster of `ranks` CTAs (2..16),
+ * computed on the host with no device work:
  * order[k] = the physical tile of logical tile k (nested dissection of the tile graph, dense
  * tiles last), the number of levels, whether the solver would use it, the cost model's estimates
  * (est_us[0] level schedule, est_us[1] column-by-column, microseconds), and the packed plan
- * (*plan_len ints, written when plan_cap is large enough; offsets[12] = where each field starts:
+ * (*plan_len ints, written when plan_cap is large enough; offsets[14] = where each field starts:
  * phase-1 ranges, phase-1 tasks, phase-2 ranges, phase-2 tasks, task rows, task columns, task
  * input modes, task update ranges, update columns, the order with the rhs row appended,
- * back-substitution ranges, back-substitution rows).  The environment variable
+ * back-substitution row ranges, back-substitution rows, back-substitution column ranges of
+ * (level, rank), back-substitution columns).  The environment variable
  * V3DBA_CHOL_SCHEDULE=levels|steps forces either kernel (tests). */
-int v3dba_tile_schedule(int nt, const uint8_t* pattern, int* order, int* n_levels, int* uses_levels,
+int v3dba_tile_schedule(int nt, const uint8_t* pattern, int ranks, int* order, int* n_levels, int* uses_levels,
                         double* est_us, int* plan, int plan_cap, int* plan_len, int* offsets);
 
 /* ---- Rotation averaging ----------------------------------------------------------------

@@ -12,7 +12,6 @@ import pytest
 from v3dsfmtoolkit_b200 import capi
 
 TB = 64
-RANKS = 8
 FACTOR = 4   # task-mode flag of the phase-1 task that factors a diagonal tile
 
 
@@ -74,6 +73,7 @@ def emulate(pat, A, b, sched):
     S[n_pad] = b
     P = sched["plan"]
     perm = P["perm"]
+    RANKS = sched["ranks"]
 
     def tile(pr, pc):
         return S[pr * TB:(pr + 1) * TB, pc * TB:(pc + 1) * TB]
@@ -104,14 +104,22 @@ def emulate(pat, A, b, sched):
                 written.add((r, j))
                 a = tile(pc, pr).T.copy() if P["task_mode"][t] == 2 else tile(pr, pc).copy()
                 tile(pr, pc)[:] = a @ Z[j].T
-    x = np.zeros(n_pad)
-    for k in range(nt - 1, -1, -1):
-        k0 = perm[k] * TB
-        v = S[n_pad, k0:k0 + TB].copy()
-        for p in range(P["bptr"][k], P["bptr"][k + 1]):
-            r0 = perm[P["brow"][p]] * TB
-            v -= S[r0:r0 + TB, k0:k0 + TB].T @ x[r0:r0 + TB]
-        x[k0:k0 + TB] = Z[k].T @ v
+    # a level reads only what the levels above it solved: each level computes from a snapshot
+    # taken before it, and an unsolved column (NaN) poisons the result
+    x = np.full(n_pad, np.nan)
+    done = []
+    for lv in range(sched["n_levels"] - 1, -1, -1):
+        before = x.copy()
+        for rank in range(RANKS):
+            for k in P["bcol"][P["blptr"][lv * RANKS + rank]:P["blptr"][lv * RANKS + rank + 1]]:
+                k0 = perm[k] * TB
+                v = S[n_pad, k0:k0 + TB].copy()
+                for p in range(P["bptr"][k], P["bptr"][k + 1]):
+                    r0 = perm[P["brow"][p]] * TB
+                    v -= S[r0:r0 + TB, k0:k0 + TB].T @ before[r0:r0 + TB]
+                x[k0:k0 + TB] = Z[k].T @ v
+                done.append(k)
+    assert sorted(done) == list(range(nt))
     return x, written
 
 
@@ -127,10 +135,11 @@ PATTERNS = [
 ]
 
 
+@pytest.mark.parametrize("ranks", [8, 16])
 @pytest.mark.parametrize("name,pat", PATTERNS, ids=[p[0] for p in PATTERNS])
-def test_level_schedule_solves_the_system(name, pat, monkeypatch):
+def test_level_schedule_solves_the_system(name, pat, ranks, monkeypatch):
     monkeypatch.setenv("V3DBA_CHOL_SCHEDULE", "levels")
-    s = capi.tile_schedule(pat)
+    s = capi.tile_schedule(pat, ranks=ranks)
     nt = pat.shape[0]
     assert sorted(s["order"].tolist()) == list(range(nt))
     A, b = spd_from_pattern(pat, seed=nt)
@@ -149,6 +158,7 @@ def test_level_schedule_solves_the_system(name, pat, monkeypatch):
 def test_plan_is_deterministic_and_tasks_are_disjoint(name, pat, monkeypatch):
     monkeypatch.setenv("V3DBA_CHOL_SCHEDULE", "levels")
     s1, s2 = capi.tile_schedule(pat), capi.tile_schedule(pat)
+    RANKS = s1["ranks"]
     assert np.array_equal(s1["order"], s2["order"])
     for f in capi.LEVEL_PLAN_FIELDS:
         assert np.array_equal(s1["plan"][f], s2["plan"][f])
@@ -201,3 +211,6 @@ def test_schedule_can_be_forced(monkeypatch):
 def test_invalid_arguments():
     with pytest.raises(capi.V3dbaError):
         capi.tile_schedule(np.zeros((0, 0), bool))
+    for ranks in (1, 17):
+        with pytest.raises(capi.V3dbaError):
+            capi.tile_schedule(band_arrow(5), ranks=ranks)

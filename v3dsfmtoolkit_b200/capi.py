@@ -138,8 +138,8 @@ def _lib():
         L.v3dba_measure_fp64_mma_peak.argtypes = [_dp]
         L.v3dba_cholesky_flops.argtypes = [C.c_void_p, _dp]
         L.v3dba_cholesky_schedule.argtypes = [C.c_void_p, _ip, _ip, _ip]
-        L.v3dba_tile_schedule.argtypes = [C.c_int, C.POINTER(C.c_uint8), _ip, _ip, _ip, _dp, _ip, C.c_int, _ip,
-                                          _ip]
+        L.v3dba_tile_schedule.argtypes = [C.c_int, C.POINTER(C.c_uint8), C.c_int, _ip, _ip, _ip, _dp, _ip, C.c_int,
+                                          _ip, _ip]
         L.v3dba_structure.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int)] + [_ip] * 8
         _fp = C.POINTER(C.c_float)
         L.v3dba_precond_model_size.argtypes = []
@@ -358,12 +358,13 @@ class Handle:
 
 
 LEVEL_PLAN_FIELDS = ("p1ptr", "p1", "p2ptr", "p2", "task_r", "task_c", "task_mode", "task_cptr", "ck", "perm",
-                     "bptr", "brow")
+                     "bptr", "brow", "blptr", "bcol")
 
 
-def tile_schedule(pattern):
-    """The level schedule of the tile Cholesky for a lower-triangle tile pattern (nt x nt bool):
-    dict(order, n_levels, uses_levels, est_levels_us, est_steps_us, plan={field: int array})."""
+def tile_schedule(pattern, ranks=16):
+    """The level schedule of the tile Cholesky for a lower-triangle tile pattern (nt x nt bool) on
+    a cluster of `ranks` CTAs: dict(order, n_levels, ranks, uses_levels, est_levels_us,
+    est_steps_us, plan={field: int array})."""
     pat = np.ascontiguousarray(np.asarray(pattern, dtype=bool).astype(np.uint8))
     nt = pat.shape[0]
     L = _lib()
@@ -372,14 +373,14 @@ def tile_schedule(pattern):
     est = np.zeros(2)
     offs = np.zeros(len(LEVEL_PLAN_FIELDS), np.int32)
     u8 = pat.ctypes.data_as(C.POINTER(C.c_uint8))
-    check(L.v3dba_tile_schedule(nt, u8, _i(order), C.byref(nl), C.byref(use), _d(est), None, 0, C.byref(plen),
-                                _i(offs)), "v3dba_tile_schedule")
+    check(L.v3dba_tile_schedule(nt, u8, ranks, _i(order), C.byref(nl), C.byref(use), _d(est), None, 0,
+                                C.byref(plen), _i(offs)), "v3dba_tile_schedule")
     buf = np.zeros(max(plen.value, 1), np.int32)
-    check(L.v3dba_tile_schedule(nt, u8, _i(order), C.byref(nl), C.byref(use), _d(est), _i(buf), len(buf),
+    check(L.v3dba_tile_schedule(nt, u8, ranks, _i(order), C.byref(nl), C.byref(use), _d(est), _i(buf), len(buf),
                                 C.byref(plen), _i(offs)), "v3dba_tile_schedule")
     bounds = list(offs) + [plen.value]
     plan = {f: buf[bounds[i]:bounds[i + 1]].copy() for i, f in enumerate(LEVEL_PLAN_FIELDS)} if plen.value else {}
-    return dict(order=order, n_levels=nl.value, uses_levels=bool(use.value), est_levels_us=float(est[0]),
+    return dict(order=order, n_levels=nl.value, ranks=ranks, uses_levels=bool(use.value), est_levels_us=float(est[0]),
                 est_steps_us=float(est[1]), plan=plan)
 
 

@@ -501,7 +501,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
 
 // Pointers into the packed level plan (TileChol::h_lv on the device).
 struct LevelPlanPtrs {
-  const int *p1ptr, *p1, *p2ptr, *p2, *tr, *tc, *tmode, *tcptr, *ck, *perm, *bptr, *brow;
+  const int *p1ptr, *p1, *p2ptr, *p2, *tr, *tc, *tmode, *tcptr, *ck, *perm, *bptr, *brow, *blptr, *bcol;
   int n_levels;
 };
 
@@ -517,14 +517,16 @@ struct LevelPlanPtrs {
 //            included);
 // the tasks of a phase are spread over the CTAs by the host, one cluster barrier after each
 // phase.  Every tile is written by one CTA per phase and its updates are summed in a fixed
-// order, so the result does not depend on timing.  Then the back-substitution, as in
-// k_chol_cluster.
-__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
+// order, so the result does not depend on timing.  Then the back-substitution, level by level
+// from the top with the columns of a level spread over the CTAs.  The cluster size (8, or 16
+// where the device allows it) is the one the plan was made for.
+__global__ void __launch_bounds__(256)
     k_chol_levels(double* __restrict__ S, int ld, int nt, int n_pad, LevelPlanPtrs P,
                   double* __restrict__ ldiag, double* __restrict__ x, int* __restrict__ fail,
                   unsigned long long* __restrict__ trace) {
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
+  const int ranks = (int)cl.num_blocks();   // the cluster size the plan was made for
   extern __shared__ double sm[];
   double* T0 = sm;
   double* T1 = sm + TB * LDT;
@@ -535,7 +537,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
     if (trace != nullptr && tid == 0) {
       unsigned long long t;
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-      trace[(size_t)slot * kCluster + rank] = t;
+      trace[(size_t)slot * ranks + rank] = t;
     }
   };
   // rhs row of tile column j (at physical column pc0): b_j -= sum_k L_jk y_k (phase 1) and
@@ -571,7 +573,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
 
   for (int lv = 0; lv < P.n_levels; ++lv) {
     stamp(2 * lv);
-    for (int e = P.p1ptr[lv * kCluster + rank]; e < P.p1ptr[lv * kCluster + rank + 1]; ++e) {
+    for (int e = P.p1ptr[lv * ranks + rank]; e < P.p1ptr[lv * ranks + rank + 1]; ++e) {
       const int t = P.p1[e];
       const int r = P.tr[t], j = P.tc[t], mode = P.tmode[t] & 3;
       const size_t pr0 = (size_t)P.perm[r] * TB, pc0 = (size_t)P.perm[j] * TB;
@@ -629,7 +631,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
     __threadfence();
     cl.sync();
     stamp(2 * lv + 1);
-    for (int e = P.p2ptr[lv * kCluster + rank]; e < P.p2ptr[lv * kCluster + rank + 1]; ++e) {
+    for (int e = P.p2ptr[lv * ranks + rank]; e < P.p2ptr[lv * ranks + rank + 1]; ++e) {
       const int t = P.p2[e];
       const int r = P.tr[t], j = P.tc[t];
       const size_t pr0 = (size_t)P.perm[r] * TB, pc0 = (size_t)P.perm[j] * TB;
@@ -670,55 +672,55 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
   }
 
   stamp(2 * P.n_levels);
-  // back-substitution L^T x = y on CTA 0 in reverse logical order, x indexed physically
-  if (rank != 0) return;
+  // back-substitution L^T x = y, x_k = Z_k^T (y_k - sum_{r > k} L_rk^T x_r), level by level from
+  // the top: the columns of one level are spread over the CTAs (x in global memory, indexed
+  // physically), a cluster barrier after each level
   double* v = T0;
   double* part = T0 + 64;
-  const bool xs_ok = n_pad <= 2 * TB * LDT;
-  double* xs = xs_ok ? T1 : x;
-  for (int k = nt - 1; k >= 0; --k) {
-    const size_t k0 = (size_t)P.perm[k] * TB;
-    const double* Z = ldiag + (size_t)k * TB * TB;
-    double z0[8], z1[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const double* zc = Z + (size_t)(8 * w + c) * TB;
-      z0[c] = zc[lane];
-      z1[c] = zc[32 + lane];
-    }
-    double sums[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) sums[c] = 0.0;
-    for (int p = P.bptr[k]; p < P.bptr[k + 1]; ++p) {
-      const size_t r0 = (size_t)P.perm[P.brow[p]] * TB;
-      const double x0 = xs[r0 + lane], x1 = xs[r0 + 32 + lane];
+  for (int lv = P.n_levels - 1; lv >= 0; --lv) {
+    for (int e = P.blptr[lv * ranks + rank]; e < P.blptr[lv * ranks + rank + 1]; ++e) {
+      const int k = P.bcol[e];
+      const size_t k0 = (size_t)P.perm[k] * TB;
+      const double* Z = ldiag + (size_t)k * TB * TB;
+      double z0[8], z1[8];
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
-        const double* col = S + (k0 + 8 * w + c) * lds + r0;
-        sums[c] += col[lane] * x0 + col[32 + lane] * x1;
+        const double* zc = Z + (size_t)(8 * w + c) * TB;
+        z0[c] = zc[lane];
+        z1[c] = zc[32 + lane];
       }
-    }
+      double sums[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const double s = warp_sum(sums[c]);
-      if (lane == 0) v[8 * w + c] = S[(k0 + 8 * w + c) * lds + n_pad] - s;
-    }
-    __syncthreads();
-    const double v0 = v[lane], v1 = v[32 + lane];
-    double zs[8];
+      for (int c = 0; c < 8; ++c) sums[c] = 0.0;
+      for (int p = P.bptr[k]; p < P.bptr[k + 1]; ++p) {
+        const size_t r0 = (size_t)P.perm[P.brow[p]] * TB;
+        const double x0 = __ldcg(x + r0 + lane), x1 = __ldcg(x + r0 + 32 + lane);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) zs[c] = warp_sum(z0[c] * v0 + z1[c] * v1);
-    if (lane == 0) {
+        for (int c = 0; c < 8; ++c) {
+          const double* col = S + (k0 + 8 * w + c) * lds + r0;
+          sums[c] += col[lane] * x0 + col[32 + lane] * x1;
+        }
+      }
+      __syncthreads();   // v / part of the previous column are consumed
 #pragma unroll
-      for (int c = 0; c < 8; ++c) part[8 * w + c] = zs[c];
+      for (int c = 0; c < 8; ++c) {
+        const double s = warp_sum(sums[c]);
+        if (lane == 0) v[8 * w + c] = S[(k0 + 8 * w + c) * lds + n_pad] - s;
+      }
+      __syncthreads();
+      const double v0 = v[lane], v1 = v[32 + lane];
+      double zs[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) zs[c] = warp_sum(z0[c] * v0 + z1[c] * v1);
+      if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) part[8 * w + c] = zs[c];
+      }
+      __syncthreads();
+      if (tid < TB) x[k0 + tid] = part[tid];
     }
-    __syncthreads();
-    if (tid < TB) {
-      xs[k0 + tid] = part[tid];
-      if (xs_ok) x[k0 + tid] = part[tid];
-    }
-    __syncthreads();
-    __threadfence_block();
+    __threadfence();
+    cl.sync();
   }
   stamp(2 * P.n_levels + 1);
 }
@@ -764,11 +766,52 @@ int chol_levels_solve(const TileChol& tc, double* S, double* x, int* d_fail, cud
   P.perm = b + tc.lv_off[kLvPerm];
   P.bptr = b + tc.lv_off[kLvBPtr];
   P.brow = b + tc.lv_off[kLvBRow];
+  P.blptr = b + tc.lv_off[kLvBLvPtr];
+  P.bcol = b + tc.lv_off[kLvBCol];
   P.n_levels = tc.n_levels;
-  const size_t smem = 3 * TB * LDT * sizeof(double);
-  k_chol_levels<<<kCluster, 256, smem, st>>>(S, tc.ld, tc.nt, tc.n_pad, P, tc.d_ldiag, x, d_fail, trace);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tc.lv_ranks, 1, 1);
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = 3 * TB * LDT * sizeof(double);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = tc.lv_ranks;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  V3DBA_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_chol_levels, S, tc.ld, tc.nt, tc.n_pad, P, tc.d_ldiag, x, d_fail, trace));
   V3DBA_LAUNCH_CHECK();
   return V3DBA_OK;
+}
+
+int chol_levels_ranks() {
+  static int ranks = 0;
+  if (ranks) return ranks;
+  ranks = 8;
+  if (chol_cluster_setup() != V3DBA_OK) {
+    cudaGetLastError();
+    return ranks;
+  }
+  const size_t smem = 3 * TB * LDT * sizeof(double);
+  if (cudaFuncSetAttribute(k_chol_levels, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 16;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_chol_levels, &cfg) == cudaSuccess && n >= 1) ranks = 16;
+  }
+  cudaGetLastError();
+  return ranks;
 }
 
 }  // namespace v3dba

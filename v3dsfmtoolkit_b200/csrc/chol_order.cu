@@ -33,7 +33,6 @@ namespace v3dba {
 
 namespace {
 
-constexpr int kClusterRanks = 8;
 // cost model of one CTA, in microseconds: a 64x64x64 DMMA tile product with its operand loads,
 // the factor + inverse of one diagonal tile, a cluster barrier, and the store of an updated tile
 constexpr double kGemmUs = 2.0, kFactorUs = 20.0, kBarrierUs = 1.0, kStoreUs = 0.5;
@@ -120,23 +119,23 @@ void nd_order(const TileGraph& g, std::vector<int> V, std::vector<int>& in_set, 
   out.insert(out.end(), S.begin(), S.end());
 }
 
-// Greedy longest-processing-time assignment of tasks (cost) to the cluster's CTAs; ties go to
-// the lowest rank and equal costs keep their order, so the schedule is deterministic.
-std::vector<std::vector<int>> assign_lpt(const std::vector<int>& tasks, const std::vector<double>& cost,
+// Greedy longest-processing-time assignment of tasks (cost) to the cluster's `ranks` CTAs; ties
+// go to the lowest rank and equal costs keep their order, so the schedule is deterministic.
+std::vector<std::vector<int>> assign_lpt(const std::vector<int>& tasks, const std::vector<double>& cost, int ranks,
                                          double* makespan) {
   std::vector<int> idx(tasks.size());
   for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
   std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-  std::vector<std::vector<int>> per(kClusterRanks);
-  double load[kClusterRanks] = {};
+  std::vector<std::vector<int>> per(ranks);
+  std::vector<double> load(ranks, 0.0);
   for (int i : idx) {
     int best = 0;
-    for (int r = 1; r < kClusterRanks; ++r)
+    for (int r = 1; r < ranks; ++r)
       if (load[r] < load[best]) best = r;
     load[best] += cost[i];
     per[best].push_back(tasks[i]);
   }
-  *makespan = *std::max_element(load, load + kClusterRanks);
+  *makespan = *std::max_element(load.begin(), load.end());
   return per;
 }
 
@@ -163,8 +162,10 @@ std::vector<int> tile_nd_order(int nt, const std::vector<uint8_t>& orig) {
   return out;
 }
 
-int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig) {
+int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks) {
   const int nt = tc.nt;
+  if (ranks < 2) return V3DBA_ERR_INVALID_ARGUMENT;
+  tc.lv_ranks = ranks;
   tc.levels = false;
   tc.h_lv.clear();
   tc.h_order.clear();
@@ -262,9 +263,9 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig) {
       }
     }
     double m1 = 0.0, m2 = 0.0;
-    auto a1 = assign_lpt(ph1, cost1, &m1);
-    auto a2 = assign_lpt(ph2, cost2, &m2);
-    for (int r = 0; r < kClusterRanks; ++r) {
+    auto a1 = assign_lpt(ph1, cost1, ranks, &m1);
+    auto a2 = assign_lpt(ph2, cost2, ranks, &m2);
+    for (int r = 0; r < ranks; ++r) {
       p1.insert(p1.end(), a1[r].begin(), a1[r].end());
       p1ptr.push_back((int)p1.size());
       p2.insert(p2.end(), a2[r].begin(), a2[r].end());
@@ -277,6 +278,14 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig) {
     brow.insert(brow.end(), colrows[k].begin(), colrows[k].end());
     bptr.push_back((int)brow.size());
   }
+  // back-substitution: the columns of a level are independent once their ancestors (higher
+  // levels) are solved; column i of a level goes to rank i mod ranks
+  std::vector<int> blptr(1, 0), bcol;
+  for (int lv = 0; lv < n_levels; ++lv)
+    for (int r = 0; r < ranks; ++r) {
+      for (size_t i = r; i < lv_cols[lv].size(); i += ranks) bcol.push_back(lv_cols[lv][i]);
+      blptr.push_back((int)bcol.size());
+    }
   perm.push_back(nt);
 
   tc.n_levels = n_levels;
@@ -284,8 +293,9 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig) {
   tc.est_levels_us = est;
   tc.est_steps_us = nt * (kFactorUs + 3.0 * kGemmUs + 2.0 * kBarrierUs);
   tc.h_order = perm;
-  const std::vector<int>* parts[kLvFields] = {&p1ptr, &p1, &p2ptr, &p2, &t_r, &t_c, &t_mode,
-                                              &t_cptr, &c_k, &perm, &bptr, &brow};
+  static_assert(kLvFields <= kLvFieldsMax, "level plan fields");
+  const std::vector<int>* parts[kLvFields] = {&p1ptr, &p1, &p2ptr, &p2, &t_r, &t_c, &t_mode, &t_cptr,
+                                              &c_k, &perm, &bptr, &brow, &blptr, &bcol};
   for (int f = 0; f < kLvFields; ++f) {
     tc.lv_off[f] = (int)tc.h_lv.size();
     tc.h_lv.insert(tc.h_lv.end(), parts[f]->begin(), parts[f]->end());
@@ -299,7 +309,7 @@ int tile_levels_plan(TileChol& tc, const std::vector<uint8_t>& orig) {
     cudaFree(tc.d_lv);
     tc.d_lv = nullptr;
   }
-  const int rc = tile_levels_build(tc, orig);
+  const int rc = tile_levels_build(tc, orig, chol_levels_ranks());
   if (rc || !tc.levels) return rc;
   V3DBA_CUDA_TRY(cudaMalloc(&tc.d_lv, sizeof(int) * std::max<size_t>(tc.h_lv.size(), 1)));
   V3DBA_CUDA_TRY(cudaMemcpy(tc.d_lv, tc.h_lv.data(), sizeof(int) * tc.h_lv.size(), cudaMemcpyHostToDevice));
@@ -308,9 +318,11 @@ int tile_levels_plan(TileChol& tc, const std::vector<uint8_t>& orig) {
 
 }  // namespace v3dba
 
-extern "C" int v3dba_tile_schedule(int nt, const uint8_t* pattern, int* order, int* n_levels, int* uses_levels,
-                                   double* est_us, int* plan, int plan_cap, int* plan_len, int* offsets) {
-  if (nt <= 0 || !pattern || !order || !n_levels || !uses_levels || !est_us || !plan_len || !offsets)
+extern "C" int v3dba_tile_schedule(int nt, const uint8_t* pattern, int ranks, int* order, int* n_levels,
+                                   int* uses_levels, double* est_us, int* plan, int plan_cap, int* plan_len,
+                                   int* offsets) {
+  if (nt <= 0 || !pattern || ranks < 2 || ranks > 16 || !order || !n_levels || !uses_levels || !est_us ||
+      !plan_len || !offsets)
     return V3DBA_ERR_INVALID_ARGUMENT;
   v3dba::TileChol tc;
   tc.nt = nt;
@@ -319,7 +331,7 @@ extern "C" int v3dba_tile_schedule(int nt, const uint8_t* pattern, int* order, i
   tc.ld = tc.n_pad + v3dba::TileChol::TB;
   std::vector<uint8_t> orig(pattern, pattern + (size_t)nt * nt);
   for (int k = 0; k < nt; ++k) orig[(size_t)k * nt + k] = 1;
-  const int rc = v3dba::tile_levels_build(tc, orig);
+  const int rc = v3dba::tile_levels_build(tc, orig, ranks);
   if (rc) return rc;
   if (tc.h_order.empty()) {   // the column-by-column schedule was forced: natural order
     for (int k = 0; k < nt; ++k) order[k] = k;

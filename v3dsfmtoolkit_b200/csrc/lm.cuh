@@ -146,6 +146,8 @@ size_t partial_doubles(const DevState& s);
 
 const LmOps* lm_ops(int model, int DA, int DC, bool fp64);
 
+constexpr int kLvFieldsMax = 16;   // room for the fields of LevelPlanField
+
 // Tile-sparse dense FP64 Cholesky of the reduced system.
 struct TileChol {
   int n = 0, n_pad = 0, nt = 0, ld = 0;
@@ -165,9 +167,10 @@ struct TileChol {
   // k_chol_levels with it instead of the column-by-column cluster kernel.
   bool levels = false;
   int n_levels = 0;
+  int lv_ranks = 8;                             // CTAs of the cluster the plan was made for
   std::vector<int> h_order;                     // logical tile -> physical tile (nt + 1 entries)
   std::vector<int> h_lv;                        // the packed plan (offsets in lv_off)
-  int lv_off[16] = {};
+  int lv_off[kLvFieldsMax] = {};
   int* d_lv = nullptr;
   double level_flops = 0.0;                     // algorithmic flops of the level schedule
   double est_levels_us = 0.0, est_steps_us = 0.0;  // the cost model's estimates of both kernels
@@ -176,9 +179,9 @@ struct TileChol {
 constexpr int kLvFactor = 4;
 // Offsets into TileChol::h_lv.
 enum LevelPlanField {
-  kLvP1Ptr = 0,   // [n_levels * 8 + 1] phase-1 task range of (level, cluster rank)
+  kLvP1Ptr = 0,   // [n_levels * ranks + 1] phase-1 task range of (level, cluster rank)
   kLvP1,          // phase-1 task ids (updates from the previous level, diagonal factors)
-  kLvP2Ptr,       // [n_levels * 8 + 1] phase-2 task range of (level, cluster rank)
+  kLvP2Ptr,       // [n_levels * ranks + 1] phase-2 task range of (level, cluster rank)
   kLvP2,          // phase-2 task ids (off-diagonal tiles and the rhs row)
   kLvTaskR,       // logical tile row of each task (nt: the rhs row)
   kLvTaskC,       // logical tile column of each task
@@ -189,14 +192,19 @@ enum LevelPlanField {
   kLvPerm,        // [nt + 1] logical tile -> physical tile (entry nt: the rhs row)
   kLvBPtr,        // [nt + 1] back-substitution: rows r > k, r < nt, of L's logical column k
   kLvBRow,
+  kLvBLvPtr,      // [n_levels * ranks + 1] back-substitution columns of (level, cluster rank)
+  kLvBCol,
   kLvFields
 };
 // Orders the tiles (nested dissection of the tile graph, dense tiles last), builds the level
 // schedule and decides whether tile_chol_solve uses it.  orig: the lower-triangle tile pattern
 // before fill-in.
 int tile_levels_plan(TileChol& tc, const std::vector<uint8_t>& orig);
-// The host part of tile_levels_plan (no device work).
-int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig);
+// The host part of tile_levels_plan (no device work), for a cluster of `ranks` CTAs.
+int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks);
+// CTAs per cluster of k_chol_levels on this device: 16 where a 16-CTA cluster with its shared
+// memory can be resident (a non-portable size, allowed on B200), else 8.
+int chol_levels_ranks();
 // The nested-dissection order alone (logical -> physical tile), for tests and the cost model.
 std::vector<int> tile_nd_order(int nt, const std::vector<uint8_t>& orig);
 int chol_levels_solve(const TileChol& tc, double* S, double* x, int* d_fail, cudaStream_t st,
