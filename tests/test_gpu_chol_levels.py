@@ -89,3 +89,23 @@ def test_sequence_scene_runs_on_the_level_schedule(monkeypatch):
     for a, b in zip(p_lv, p_st):
         if a is not None:
             assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
+
+
+def test_stereo_rig_scene_runs_on_the_level_schedule(monkeypatch):
+    sc = scenes.stereo_rig_scene(n_poses=150, n_points=12000, seed=4, window=6, outlier_frac=0.01)
+    h = capi.Handle.from_scene(sc)
+    kind, n_levels, nt = h.cholesky_schedule()
+    assert kind == "levels" and n_levels < nt
+    r_lv = h.minimize(max_iterations=12, precision=capi.PRECISION_FP64)
+    p_lv = h.get_params()
+    h.close()
+    monkeypatch.setenv("V3DBA_CHOL_SCHEDULE", "steps")
+    h2 = capi.Handle.from_scene(sc)
+    r_st = h2.minimize(max_iterations=12, precision=capi.PRECISION_FP64)
+    p_st = h2.get_params()
+    h2.close()
+    assert r_lv.status == r_st.status and r_lv.iterations == r_st.iterations
+    assert abs(r_lv.cost - r_st.cost) <= 1e-9 * r_st.cost
+    for a, b in zip(p_lv, p_st):
+        if a is not None:
+            assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)

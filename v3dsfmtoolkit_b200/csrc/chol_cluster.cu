@@ -349,7 +349,6 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
     tile_wait();
     factor_resident(0);
   }
-  __threadfence();
   cl.sync();
   // Per tile step k: CTA 0 owns the chain along the diagonal (panel L_{k+1,k} with Z_k resident,
   // the update of the next diagonal tile in shared memory, its factor); CTAs 1.. form the other
@@ -375,8 +374,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
           store_acc(acc, k0 + TB, k0, 0, T0);
         }
       }
-      __threadfence();
-      cluster_arrive();                           // L_{k+1,k} is published
+      cluster_arrive();                           // L_{k+1,k} is published (release)
       if (has_next) {
         tile_wait();
         __syncthreads();
@@ -422,7 +420,6 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
         cta_gemm_abt(acc, T0, T1);
         store_acc(acc, r0, k0, 0, nullptr);
       }
-      __threadfence();
       cluster_arrive();
       cluster_wait();
       stamp(2 * k + 1);
@@ -435,7 +432,6 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
         update_tile(k, ur[u0 + t], uc[u0 + t]);
       }
     }
-    __threadfence();
     cl.sync();
   }
 
@@ -628,8 +624,7 @@ __global__ void __launch_bounds__(256)
               }
       }
     }
-    __threadfence();
-    cl.sync();
+    cl.sync();   // arrive.release / wait.acquire at cluster scope: the CTAs' writes are visible
     stamp(2 * lv + 1);
     for (int e = P.p2ptr[lv * ranks + rank]; e < P.p2ptr[lv * ranks + rank + 1]; ++e) {
       const int t = P.p2[e];
@@ -667,8 +662,7 @@ __global__ void __launch_bounds__(256)
             for (int i = 0; i < 2; ++i)
               S[(pc0 + frag_col(h, b, i)) * lds + pr0 + frag_row(a)] = acc[h][a][b][i];
     }
-    __threadfence();
-    cl.sync();
+    cl.sync();   // arrive.release / wait.acquire at cluster scope: the CTAs' writes are visible
   }
 
   stamp(2 * P.n_levels);
@@ -719,8 +713,7 @@ __global__ void __launch_bounds__(256)
       __syncthreads();
       if (tid < TB) x[k0 + tid] = part[tid];
     }
-    __threadfence();
-    cl.sync();
+    cl.sync();   // arrive.release / wait.acquire at cluster scope: the CTAs' writes are visible
   }
   stamp(2 * P.n_levels + 1);
 }
