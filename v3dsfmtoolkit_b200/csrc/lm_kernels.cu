@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
   constexpr int NS = RelinNV<DC>::NS, NV = RelinNV<DC>::NV, NZ = L::NZ;
   __shared__ double red[(kPtThreads / 32) * NV];
   const Dims& D = s.d;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tp = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = tp < D.M ? s.p_order[tp] : D.M;   // longest tracks first, equal lengths per warp
   double v[NV];
 #pragma unroll
   for (int t = 0; t < NV; ++t) v[t] = (t < NS) ? 0.0 : -1e30;

@@ -216,6 +216,14 @@ int use_gnn(v3dba_handle h, bool learned) {
 }
 
 // o_sub[k] = subcamera of the caller's observation o_orig[k] (point-major order)
+// Sort key of point j for the track-length order: longer tracks first, lengths of at least
+// kTrackBuckets - 1 share the first bucket.
+constexpr int kTrackBuckets = 64;
+__global__ void k_track_keys(const int* __restrict__ p_ptr, int M, int* __restrict__ keys) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < M) keys[j] = kTrackBuckets - 1 - min(p_ptr[j + 1] - p_ptr[j], kTrackBuckets - 1);
+}
+
 __global__ void k_gather_sub(const int* __restrict__ sub, const int* __restrict__ orig, int K, int* __restrict__ out) {
   const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (k < K) out[k] = sub[orig[k]];
@@ -376,6 +384,17 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   s.o_orig = ds.o_orig;
   s.o_meas = ds.o_meas;
   s.p_ptr = ds.p_ptr;
+  {   // points by descending track length (stable: equal lengths keep their order)
+    int *keys, *kptr;
+    TRY(dalloc(h, &s.p_order, (size_t)std::max(M, 1)));
+    TRY(dalloc(h, &keys, (size_t)std::max(M, 1)));
+    TRY(dalloc(h, &kptr, (size_t)kTrackBuckets + 1));
+    if (M > 0) {
+      k_track_keys<<<(M + 255) / 256, 256, 0, h->stream>>>(s.p_ptr, M, keys);
+      CTRY(cudaGetLastError());
+      TRY(group_by_key_device(keys, M, kTrackBuckets, s.p_order, kptr, h->stream));
+    }
+  }
   s.c_ptr = ds.c_ptr;
   s.c_obs = ds.c_obs;
   s.nb = (int)ds.h_b_i.size();
