@@ -97,7 +97,7 @@ struct DevState {
   // scalars
   double* d_lambda = nullptr;
   double* d_relin = nullptr;  // {err, gmax, maxdiag}
-  double* d_trial = nullptr;  // {new_err, d2, dg}
+  double* d_trial = nullptr;  // {new_err, d2, dg, failed}: d_relin + 4 (one readback for both)
   int* d_fail = nullptr;
   // reduction partials
   double* part = nullptr;

@@ -888,6 +888,7 @@ __global__ void __launch_bounds__(256) k_trial_finalize(DevState s, const double
     s.d_trial[0] = c[0];
     s.d_trial[1] = a[0] + b[0];
     s.d_trial[2] = a[1] + b[1];
+    s.d_trial[3] = *s.d_fail != 0 ? 1.0 : 0.0;   // every kernel that can fail ran before this one
   }
 }
 

@@ -215,6 +215,13 @@ int use_gnn(v3dba_handle h, bool learned) {
   return V3DBA_OK;
 }
 
+// Start of a trial: the damping and a cleared failure flag, set on the device in stream order
+// (no host-to-device copy on the critical path).
+__global__ void k_trial_setup(double lambda, double* __restrict__ d_lambda, int* __restrict__ d_fail) {
+  *d_lambda = lambda;
+  *d_fail = 0;
+}
+
 // o_sub[k] = subcamera of the caller's observation o_orig[k] (point-major order)
 // Sort key of point j for the track-length order: longer tracks first, lengths of at least
 // kTrackBuckets - 1 share the first bucket.
@@ -373,7 +380,7 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   CTRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   CTRY(cudaEventCreate(&h->ev0));
   CTRY(cudaEventCreate(&h->ev1));
-  CTRY(cudaMallocHost(&h->h_scalars, 16 * sizeof(double)));
+  CTRY(cudaMallocHost(&h->h_scalars, 24 * sizeof(double)));
 
   trace.mark("stream");
   DeviceStructure ds;
@@ -464,8 +471,8 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   TRY(dalloc(h, &s.g_Z, 64));
   TRY(dalloc(h, &s.g_gc, 8));
   TRY(dalloc(h, &s.d_lambda, 1));
-  TRY(dalloc(h, &s.d_relin, 4));
-  TRY(dalloc(h, &s.d_trial, 4));
+  TRY(dalloc(h, &s.d_relin, 8));   // relinearisation scalars, then the trial's: read back together
+  s.d_trial = s.d_relin + 4;
   TRY(dalloc(h, &s.d_fail, 1));
   s.part_cap = partial_doubles(s);
   TRY(dalloc(h, &s.part, s.part_cap));
@@ -579,9 +586,8 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
               const v3dba_options& o, double out[6]) {
   DevState& s = h->s;
   cudaStream_t st = h->stream;
-  h->h_scalars[8] = lambda;
-  V3DBA_CUDA_TRY(cudaMemcpyAsync(s.d_lambda, h->h_scalars + 8, sizeof(double), cudaMemcpyHostToDevice, st));
-  V3DBA_CUDA_TRY(cudaMemsetAsync(s.d_fail, 0, sizeof(int), st));
+  k_trial_setup<<<1, 1, 0, st>>>(lambda, s.d_lambda, s.d_fail);
+  V3DBA_LAUNCH_CHECK();
   int rc;
   if (!pcg && (rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
   if ((rc = ops->build_reduced(s, st))) return rc;
@@ -630,14 +636,15 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
     return rc;
   }
   if ((rc = ops->finish_trial(s, st))) return rc;
-  V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars, s.d_trial, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-  V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 3, s.d_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+  // one copy: the relinearisation scalars (h_scalars[16..18]) and the trial's {new cost, |d|^2,
+  // d.g, failure flag} (h_scalars[20..23], the flag stored by k_trial_finalize)
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 16, s.d_relin, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
   V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
-  out[0] = h->h_scalars[0];
-  out[1] = h->h_scalars[1];
-  out[2] = h->h_scalars[2];
-  int fail, its = 0;
-  std::memcpy(&fail, h->h_scalars + 3, sizeof(int));
+  out[0] = h->h_scalars[20];
+  out[1] = h->h_scalars[21];
+  out[2] = h->h_scalars[22];
+  const int fail = h->h_scalars[23] != 0.0 ? 1 : 0;
+  int its = 0;
   if (pcg) std::memcpy(&its, h->h_scalars + 9, sizeof(int));
   out[3] = fail ? 1.0 : 0.0;
   out[4] = its + (fallback ? h->h_scalars[10] : 0.0);   // iterations of a failed attempt count too
@@ -700,12 +707,14 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
       if ((rc = ops->relinearize(s, false, o.tau, st))) return rc;
     }
     relinearize_again = false;
-    if (compute_derivatives) {
-      if ((rc = ops->relinearize(s, it == 0, o.tau, st))) return rc;
-      V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 4, s.d_relin, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
-      err = h->h_scalars[4];
-      const double gmax = h->h_scalars[5], dmax = h->h_scalars[6];
+    // The relinearisation's cost, gradient maximum and diagonal maximum are read back with the
+    // trial's results (one synchronisation per iteration); only the first iteration, which
+    // needs the diagonal maximum for the initial lambda, waits for them.  When they end the run
+    // (stop cost, gradient), the trial just computed is discarded.
+    bool relin_pending = false, stop = false;
+    auto take_relin = [&]() {
+      err = h->h_scalars[16];
+      const double gmax = h->h_scalars[17], dmax = h->h_scalars[18];
       if (res->n_relinearizations == 0) res->initial_cost = err;
       res->n_relinearizations++;
       res->cost = err;
@@ -713,20 +722,37 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
       if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: lambda = %.17g\n", lambda);
       if (o.stop_cost > 0.0 && err <= o.stop_cost) {
         res->reached_stop_cost = 1;
-        break;
+        stop = true;
+        return;
       }
       if (gmax < o.gradient_threshold) {   // cpp:857-861
         res->status = V3DBA_STATUS_CONVERGED;
-        break;
+        stop = true;
+        return;
       }
       if (it == 0) {
         lambda = o.tau * dmax;             // cpp:981-1052
         if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: initial lambda = %.17g\n", lambda);
       }
+    };
+    if (compute_derivatives) {
+      if ((rc = ops->relinearize(s, it == 0, o.tau, st))) return rc;
+      if (it == 0) {
+        V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 16, s.d_relin, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+        take_relin();
+        if (stop) break;
+      } else {
+        relin_pending = true;
+      }
     }
     double t[6];
     if ((rc = run_trial(h, ops, lambda, pcg, pcg ? o.preconditioner : V3DBA_PRECOND_BLOCK_JACOBI, fp64, o, t)))
       return rc;
+    if (relin_pending) {   // run_trial read the relinearisation scalars back with its own
+      take_relin();
+      if (stop) break;
+    }
     res->pcg_iterations += (int)t[4];
     res->pcg_fallbacks += (int)t[5];
     const bool success = t[3] == 0.0;
