@@ -2,11 +2,16 @@
 //
 // Same factorisation as tile_cholesky.cu (right-looking over 64x64 tiles, rhs carried as tile row
 // nt, tiles that are structurally zero in L skipped), but the whole factor + solve runs in ONE
-// launch of an 8-CTA cluster: the phases of a tile step are separated by cluster barriers
-// (barrier.cluster, sub-microsecond) instead of kernel boundaries, which removes the launch and
-// drain latency that dominates small reduced systems (hundreds to a few thousand unknowns).
+// launch of a cluster: the phases are separated by cluster barriers (barrier.cluster,
+// sub-microsecond) instead of kernel boundaries, which removes the launch and drain latency that
+// dominates small reduced systems (hundreds to a few thousand unknowns).  Two kernels:
+//   k_chol_cluster (8 CTAs) goes column by column in the caller's order;
+//   k_chol_levels (16 CTAs where the device allows, else 8) runs the level schedule of
+//   chol_order.cu, the independent columns of an elimination-tree level side by side.
+// Both use the same diagonal tile factor (cta_factor_tile).
 //
-// Per tile column k, CTA 0 owns the chain along the diagonal and keeps it in shared memory:
+// k_chol_cluster: per tile column k, CTA 0 owns the chain along the diagonal and keeps it in
+// shared memory:
 //   with Z_k = L_kk^-1 resident it forms the panel tile next to the diagonal,
 //   L_{k+1,k} = A_{k+1,k} Z_k^T, publishes it (split cluster barrier: arrive, keep working), applies
 //   it to the next diagonal tile (fetched meanwhile) and factors that tile: 16-column blocking,
@@ -15,7 +20,7 @@
 //   CTAs 1.. form the other panel tiles (and the rhs row), L_rk = A_rk Z_k^T, one 64x64x64 DMMA
 //   GEMM per tile, then the other trailing tiles, A_rc -= L_rk L_ck^T (DMMA).
 // Then the back-substitution L^T x = y (y = the factored rhs row) by CTA 0, with x kept in
-// shared memory and Z_kk fetched ahead of the dependent sums.
+// shared memory and Z_kk fetched ahead of the dependent sums.  (Its CTAs are kCluster = 8.)
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -501,8 +506,8 @@ struct LevelPlanPtrs {
   int n_levels;
 };
 
-// Level-scheduled tile Cholesky + solve in one launch of an 8-CTA cluster, under the tile order
-// and schedule of tile_levels_plan.  Logical tile (r, c) lives at physical tile (perm r, perm c)
+// Level-scheduled tile Cholesky + solve in one launch of a cluster, under the tile order and
+// schedule of tile_levels_plan.  Logical tile (r, c) lives at physical tile (perm r, perm c)
 // of S; its input, when the assembled tile is the mirrored (perm c, perm r), is read transposed.
 // Per level (columns that are independent of each other):
 //   phase 1: the columns of the previous level update every tile they reach,
