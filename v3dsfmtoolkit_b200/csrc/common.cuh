@@ -73,6 +73,31 @@ int ensure_pool();
 
 constexpr int kWarp = 32;
 
+// Programmatic dependent launch (sm_90 and later).  A kernel launched with launch_pdl may be
+// scheduled while its predecessor in the stream is still running: it must call pdl_wait(), which
+// returns once the predecessor grid has completed and its writes are visible, before it touches
+// anything the predecessor writes.  pdl_trigger() lets the next kernel be scheduled once every
+// block of this one has issued it (so all of this kernel's blocks are resident by then).  In a
+// kernel launched the usual way both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

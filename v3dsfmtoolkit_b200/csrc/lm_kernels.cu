@@ -162,6 +162,8 @@ struct RelinNV {
 // blocks, and accumulate V_j, gb_j, Y_j; Z, gc and the cost go to per-block partials.
 template <int MODEL, int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, DC>;
   constexpr int DCc = L::DCc;
   constexpr int NS = RelinNV<DC>::NS, NV = RelinNV<DC>::NV, NZ = L::NZ;
@@ -300,6 +302,8 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
 // X = sum A^T C (FP64 sums); the partials of a camera are folded in chunk order afterwards.
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_camera_chunks(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, DC>;
   using CV = CamV<DA, DC>;
   constexpr int DCc = L::DCc;
@@ -345,6 +349,8 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_camera_chunks(DevState s, do
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_camera_finish(DevState s, const double* __restrict__ cpart,
                                                                    double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, DC>;
   using CV = CamV<DA, DC>;
   constexpr int DCc = L::DCc;
@@ -400,6 +406,8 @@ template <int DC>
 __global__ void __launch_bounds__(256) k_relin_finalize(DevState s, const double* __restrict__ part_pt, int nbp,
                                                         const double* __restrict__ part_cam, int nbc,
                                                         int init_lambda, double tau) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   constexpr int NS = RelinNV<DC>::NS, NV = RelinNV<DC>::NV, NZ = nsym(DC);
   constexpr int DCc = DC > 0 ? DC : 1;
   __shared__ double red[8 * (NV > 2 ? NV : 2)];
@@ -460,6 +468,8 @@ __device__ __forceinline__ bool inv3(const double a[6], double o[6]) {
 // T_k = W_k Vinv_j for its observations; Y^T Vinv Y and Y^T q go to per-block partials.
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, DC>;
   constexpr int DCc = L::DCc;
   constexpr int NV = ElimNV<DC>::NV;
@@ -545,6 +555,8 @@ __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, doub
 // One warp per chunk of a camera-pair block's observation pairs: partial sum T_k W_m^T.
 template <int DA, typename Real>
 __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, 0>;
   using SV = SchurV<DA>;
   const int lane = threadIdx.x & 31;
@@ -575,6 +587,8 @@ __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __rest
 // partials, written into the lower triangle of the dense column-major S.
 template <int DA, typename Real>
 __global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, 0>;
   using SV = SchurV<DA>;
   constexpr int PER = SV::VP / 32;
@@ -610,6 +624,8 @@ __global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* 
 // One warp per chunk of a camera's observations: partial sum_k W_k q_j(k) and sum_k T_k Y_j(k).
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, DC>;
   using RV = RhsV<DA, DC>;
   constexpr int DCc = L::DCc;
@@ -651,6 +667,8 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, doubl
 // identity block, zero rhs and zero border for fixed cameras.
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const double* __restrict__ cpart) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, DC>;
   using RV = RhsV<DA, DC>;
   constexpr int DCc = L::DCc;
@@ -695,6 +713,8 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const
 // Global block: S_cc = Z + lambda I - sum_j Y_j^T Vinv_j Y_j, rhs_c = gc - sum_j Y_j^T q_j.
 template <int DA, int DC>
 __global__ void __launch_bounds__(256) k_global_block(DevState s, const double* __restrict__ part, int nbp) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   constexpr int NV = ElimNV<DC>::NV;
   constexpr int DCc = DC > 0 ? DC : 1;
   __shared__ double red[8 * NV];
@@ -722,6 +742,8 @@ __global__ void __launch_bounds__(256) k_global_block(DevState s, const double* 
 // One thread per point: db_j = q_j - sum_k T_k^T da_i(k) - (Vinv Y_j) dc; X' = X + db.
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   using L = Lay<DA, DC>;
   constexpr int DCc = L::DCc;
   __shared__ double red[(kPtThreads / 32) * 2];
@@ -778,6 +800,8 @@ __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double
 // One thread per camera (plus the globals on thread 0 of block 0): trial parameters.
 template <int MODEL, int DA, int DC>
 __global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   __shared__ double red[4 * 2];
   const Dims& D = s.d;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -857,6 +881,8 @@ __global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __res
 // with weights recomputed at P.
 template <int MODEL>
 __global__ void __launch_bounds__(256) k_obs_cost(DevState s, ParamSet P, int recompute_w, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   __shared__ double red[8];
   const Dims& D = s.d;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -879,6 +905,8 @@ __global__ void __launch_bounds__(256) k_obs_cost(DevState s, ParamSet P, int re
 __global__ void __launch_bounds__(256) k_trial_finalize(DevState s, const double* __restrict__ pb, int nbp,
                                                         const double* __restrict__ pc, int nbc,
                                                         const double* __restrict__ po, int nbo) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
   __shared__ double red[8 * 2];
   double a[2], b[2], c[1];
   fold_partials<2, 2>(pb, nbp, a, red);
@@ -932,57 +960,67 @@ struct Ops {
     const int bc = cdiv(std::max(s.d.N, 1), kCamWarps);
     const int bu = cdiv(std::max(s.d.N, 1), 128);
     const int bo = cdiv(std::max(s.d.K, 1), 256);
+    cudaError_t e = cudaSuccess;
     switch (id) {
       case kStageLinearize:
-        k_linearize<MODEL, DA, DC, Real><<<bp, kPtThreads, 0, st>>>(s, s.part + pl.relin_pt);
+        e = launch_pdl(k_linearize<MODEL, DA, DC, Real>, dim3(bp), dim3(kPtThreads), 0, st, s, s.part + pl.relin_pt);
         break;
       case kStageCameraChunks:
         if (s.nch_cam == 0) return V3DBA_OK;
-        k_camera_chunks<DA, DC, Real><<<cdiv(s.nch_cam, kCamWarps), kCamWarps * 32, 0, st>>>(s, s.part_cc);
+        e = launch_pdl(k_camera_chunks<DA, DC, Real>, dim3(cdiv(s.nch_cam, kCamWarps)), dim3(kCamWarps * 32), 0, st, s,
+                       s.part_cc);
         break;
       case kStageCameraFinish:
-        k_camera_finish<DA, DC, Real><<<bc, kCamWarps * 32, 0, st>>>(s, s.part_cc, s.part + pl.relin_cam);
+        e = launch_pdl(k_camera_finish<DA, DC, Real>, dim3(bc), dim3(kCamWarps * 32), 0, st, s, (const double*)s.part_cc,
+                       s.part + pl.relin_cam);
         break;
       case kStageRelinFinalize:
-        k_relin_finalize<DC><<<1, 256, 0, st>>>(s, s.part + pl.relin_pt, bp, s.part + pl.relin_cam, bc,
-                                                 init_lambda, tau);
+        e = launch_pdl(k_relin_finalize<DC>, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.relin_pt), bp,
+                       (const double*)(s.part + pl.relin_cam), bc, init_lambda, tau);
         break;
       case kStagePointEliminate:
-        k_point_eliminate<DA, DC, Real><<<bp, kPtThreads, 0, st>>>(s, s.part + pl.elim);
+        e = launch_pdl(k_point_eliminate<DA, DC, Real>, dim3(bp), dim3(kPtThreads), 0, st, s, s.part + pl.elim);
         break;
       case kStageSchurChunks:
         if (s.nch_blk == 0) return V3DBA_OK;
-        k_schur_chunks<DA, Real><<<cdiv(s.nch_blk, 4), 128, 0, st>>>(s, s.part_bc);
+        e = launch_pdl(k_schur_chunks<DA, Real>, dim3(cdiv(s.nch_blk, 4)), dim3(128), 0, st, s, s.part_bc);
         break;
       case kStageSchurFinish:
         if (s.nb == 0) return V3DBA_OK;
-        k_schur_finish<DA, Real><<<cdiv(s.nb, 4), 128, 0, st>>>(s, s.part_bc);
+        e = launch_pdl(k_schur_finish<DA, Real>, dim3(cdiv(s.nb, 4)), dim3(128), 0, st, s, (const double*)s.part_bc);
         break;
       case kStageRhsChunks:
         if (s.nch_cam == 0) return V3DBA_OK;
-        k_rhs_chunks<DA, DC, Real><<<cdiv(s.nch_cam, kCamWarps), kCamWarps * 32, 0, st>>>(s, s.part_cc);
+        e = launch_pdl(k_rhs_chunks<DA, DC, Real>, dim3(cdiv(s.nch_cam, kCamWarps)), dim3(kCamWarps * 32), 0, st, s,
+                       s.part_cc);
         break;
       case kStageRhsFinish:
-        k_rhs_finish<DA, DC, Real><<<bc, kCamWarps * 32, 0, st>>>(s, s.part_cc);
+        e = launch_pdl(k_rhs_finish<DA, DC, Real>, dim3(bc), dim3(kCamWarps * 32), 0, st, s, (const double*)s.part_cc);
         break;
       case kStageGlobalBlock:
         if (DC == 0) return V3DBA_OK;
-        k_global_block<DA, DC><<<1, 256, 0, st>>>(s, s.part + pl.elim, bp);
+        e = launch_pdl(k_global_block<DA, DC>, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.elim), bp);
         break;
       case kStagePointBacksub:
-        k_point_backsub<DA, DC, Real><<<bp, kPtThreads, 0, st>>>(s, s.part + pl.backsub);
+        e = launch_pdl(k_point_backsub<DA, DC, Real>, dim3(bp), dim3(kPtThreads), 0, st, s, s.part + pl.backsub);
         break;
       case kStageCameraUpdate:
-        k_camera_update<MODEL, DA, DC><<<bu, 128, 0, st>>>(s, s.part + pl.camupd);
+        e = launch_pdl(k_camera_update<MODEL, DA, DC>, dim3(bu), dim3(128), 0, st, s, s.part + pl.camupd);
         break;
       case kStageTrialCost:
-        k_obs_cost<MODEL><<<bo, 256, 0, st>>>(s, s.trial, 0, s.part + pl.obs);
+        e = launch_pdl(k_obs_cost<MODEL>, dim3(bo), dim3(256), 0, st, s, (ParamSet)s.trial, 0, s.part + pl.obs);
         break;
       case kStageTrialFinalize:
-        k_trial_finalize<<<1, 256, 0, st>>>(s, s.part + pl.backsub, bp, s.part + pl.camupd, bu, s.part + pl.obs, bo);
+        e = launch_pdl(k_trial_finalize, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.backsub), bp,
+                       (const double*)(s.part + pl.camupd), bu, (const double*)(s.part + pl.obs), bo);
         break;
       default:
         return V3DBA_ERR_INVALID_ARGUMENT;
+    }
+    if (e != cudaSuccess) {
+      fprintf(stderr, "v3dba: launch of stage %d failed: %s\n", id, cudaGetErrorString(e));
+      cudaGetLastError();
+      return V3DBA_ERR_CUDA;
     }
     V3DBA_LAUNCH_CHECK();
     return V3DBA_OK;
