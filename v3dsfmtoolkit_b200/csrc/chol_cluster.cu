@@ -525,6 +525,8 @@ __global__ void __launch_bounds__(256)
     k_chol_levels(double* __restrict__ S, int ld, int nt, int n_pad, LevelPlanPtrs P,
                   double* __restrict__ ldiag, double* __restrict__ x, int* __restrict__ fail,
                   unsigned long long* __restrict__ trace) {
+  pdl_wait();      // launched as a dependent of the system's assembly
+  pdl_trigger();
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   const int ranks = (int)cl.num_blocks();   // the cluster size the plan was made for
@@ -772,13 +774,15 @@ int chol_levels_solve(const TileChol& tc, double* S, double* x, int* d_fail, cud
   cfg.blockDim = dim3(256, 1, 1);
   cfg.dynamicSmemBytes = 3 * TB * LDT * sizeof(double);
   cfg.stream = st;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = tc.lv_ranks;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;   // see pdl_wait()
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = 2;
   V3DBA_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_chol_levels, S, tc.ld, tc.nt, tc.n_pad, P, tc.d_ldiag, x, d_fail, trace));
   V3DBA_LAUNCH_CHECK();
   return V3DBA_OK;

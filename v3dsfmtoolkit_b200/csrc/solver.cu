@@ -218,6 +218,8 @@ int use_gnn(v3dba_handle h, bool learned) {
 // Start of a trial: the damping and a cleared failure flag, set on the device in stream order
 // (no host-to-device copy on the critical path).
 __global__ void k_trial_setup(double lambda, double* __restrict__ d_lambda, int* __restrict__ d_fail) {
+  pdl_wait();
+  pdl_trigger();
   *d_lambda = lambda;
   *d_fail = 0;
 }
@@ -586,7 +588,7 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
               const v3dba_options& o, double out[6]) {
   DevState& s = h->s;
   cudaStream_t st = h->stream;
-  k_trial_setup<<<1, 1, 0, st>>>(lambda, s.d_lambda, s.d_fail);
+  V3DBA_CUDA_TRY(launch_pdl(k_trial_setup, dim3(1), dim3(1), 0, st, lambda, s.d_lambda, s.d_fail));
   V3DBA_LAUNCH_CHECK();
   int rc;
   if (!pcg && (rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;

@@ -222,6 +222,8 @@ __global__ void __launch_bounds__(256) k_chol_backsolve(const double* __restrict
 
 __global__ void __launch_bounds__(256) k_chol_zero(double* __restrict__ S, int ld, int nt, int n, int n_pad,
                                                    const int* __restrict__ tiles) {
+  pdl_wait();
+  pdl_trigger();
   const int t = tiles[blockIdx.x];
   const int tr = t / (nt + 1) , tc = t % (nt + 1);
   const size_t r0 = (size_t)tr * TB, c0 = (size_t)tc * TB;
@@ -316,7 +318,8 @@ void tile_chol_free(TileChol& tc) {
 
 int tile_chol_zero(const TileChol& tc, double* S, double* /*rhs*/, cudaStream_t st) {
   if (tc.h_tiles.empty()) return V3DBA_OK;
-  k_chol_zero<<<(unsigned)tc.h_tiles.size(), 256, 0, st>>>(S, tc.ld, tc.nt, tc.n, tc.n_pad, tc.d_tiles);
+  V3DBA_CUDA_TRY(launch_pdl(k_chol_zero, dim3((unsigned)tc.h_tiles.size()), dim3(256), 0, st, S, tc.ld, tc.nt, tc.n,
+                            tc.n_pad, (const int*)tc.d_tiles));
   V3DBA_LAUNCH_CHECK();
   return V3DBA_OK;
 }
