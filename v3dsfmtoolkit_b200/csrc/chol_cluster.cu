@@ -24,6 +24,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <vector>
 
@@ -725,14 +726,18 @@ __global__ void __launch_bounds__(256)
   stamp(2 * P.n_levels + 1);
 }
 
+// Function attributes are set once per device (a process may drive several GPUs).
 int chol_cluster_setup() {
-  static bool done = false;
-  if (done) return V3DBA_OK;
+  static std::atomic<uint64_t> done_mask{0};
+  int dev = 0;
+  V3DBA_CUDA_TRY(cudaGetDevice(&dev));
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done_mask.load() & bit) return V3DBA_OK;
   V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(3 * TB * LDT * sizeof(double))));
   V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(3 * TB * LDT * sizeof(double))));
-  done = true;
+  done_mask.fetch_or(bit);
   return V3DBA_OK;
 }
 
@@ -789,9 +794,15 @@ int chol_levels_solve(const TileChol& tc, double* S, double* x, int* d_fail, cud
 }
 
 int chol_levels_ranks() {
-  static int ranks = 0;
-  if (ranks) return ranks;
-  ranks = 8;
+  static std::atomic<int> ranks_of[64];   // per device: 0 until decided
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 8;
+  }
+  std::atomic<int>& cached = ranks_of[dev & 63];
+  if (cached.load()) return cached.load();
+  int ranks = 8;
   if (chol_cluster_setup() != V3DBA_OK) {
     cudaGetLastError();
     return ranks;
@@ -813,6 +824,7 @@ int chol_levels_ranks() {
     if (cudaOccupancyMaxActiveClusters(&n, k_chol_levels, &cfg) == cudaSuccess && n >= 1) ranks = 16;
   }
   cudaGetLastError();
+  cached.store(ranks);
   return ranks;
 }
 
