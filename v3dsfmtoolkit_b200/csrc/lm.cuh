@@ -39,8 +39,9 @@ struct DevState {
   int* o_orig = nullptr;    // [K] caller's index of permuted observation k
   double* o_meas = nullptr; // [2K]
   int* p_ptr = nullptr;     // [M+1] track of point j = [p_ptr[j], p_ptr[j+1])
-  int* p_order = nullptr;   // [M] points by descending track length: the per-point kernels take
-                            // point p_order[t] in thread t, so a warp's tracks are equally long
+  int* p_order = nullptr;   // [M] points by descending track length, or null (large problems):
+                            // k_linearize takes point p_order[t] in thread t, so a warp's
+                            // tracks are equally long
   int* c_ptr = nullptr;     // [N+1]
   int* c_obs = nullptr;     // [K] permuted observation ids grouped by camera
   int* o_sub = nullptr;     // [K] rig camera of permuted observation k (STEREO)

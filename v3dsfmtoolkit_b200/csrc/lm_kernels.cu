@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
   __shared__ double red[(kPtThreads / 32) * NV];
   const Dims& D = s.d;
   const int tp = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = tp < D.M ? s.p_order[tp] : D.M;   // longest tracks first, equal lengths per warp
+  const int j = tp < D.M ? (s.p_order ? s.p_order[tp] : tp) : D.M;   // longest tracks first (p_order)
   double v[NV];
 #pragma unroll
   for (int t = 0; t < NV; ++t) v[t] = (t < NS) ? 0.0 : -1e30;
