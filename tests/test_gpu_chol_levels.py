@@ -109,3 +109,25 @@ def test_stereo_rig_scene_runs_on_the_level_schedule(monkeypatch):
     for a, b in zip(p_lv, p_st):
         if a is not None:
             assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
+
+
+def test_varying_intrinsics_scene_runs_on_the_level_schedule(monkeypatch):
+    """VaryingInternals: 13 unknowns per camera, so the camera blocks straddle tiles differently
+    and the band is wider than the 6-unknown sequences'."""
+    sc = scenes.varying_scene(n_cams=150, n_points=15000, seed=2)
+    h = capi.Handle.from_scene(sc)
+    kind, n_levels, nt = h.cholesky_schedule()
+    assert kind == "levels" and n_levels < nt
+    r_lv = h.minimize(max_iterations=10, precision=capi.PRECISION_FP64)
+    p_lv = h.get_params()
+    h.close()
+    monkeypatch.setenv("V3DBA_CHOL_SCHEDULE", "steps")
+    h2 = capi.Handle.from_scene(sc)
+    r_st = h2.minimize(max_iterations=10, precision=capi.PRECISION_FP64)
+    p_st = h2.get_params()
+    h2.close()
+    assert r_lv.status == r_st.status and r_lv.iterations == r_st.iterations
+    assert abs(r_lv.cost - r_st.cost) <= 1e-9 * r_st.cost
+    for a, b in zip(p_lv, p_st):
+        if a is not None:
+            assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
