@@ -161,7 +161,7 @@ def test_reset_and_repeat_are_deterministic():
 
 
 def test_circle20_full_size_matches_reference():
-    """BASELINE config 1 at full size (20 cameras, 2000 points, 8000 observations), plain LS."""
+    """The 20-camera circle scene at full size (2000 points, 8000 observations), plain LS."""
     from oracle.bindings import Reference, reference_available
     if not reference_available():
         pytest.skip("compiled reference not present")
@@ -181,7 +181,8 @@ def test_circle20_full_size_matches_reference():
 
 
 def test_sequence200_full_size_matches_reference_cost():
-    """BASELINE config 2 at full size.  The reference stops on its iteration limit (TIMEOUT at
+    """The 200-camera distortion sequence at full size (50,000 points, ~375k observations).  The
+    reference stops on its iteration limit (TIMEOUT at
     100) while the Huber re-weighting still lowers the cost by ~1e-6 per iteration, so accept /
     reject decisions near rho = 0 depend on rounding and the paths differ after a few tens of
     steps.  About one path in ten (tau scaled by 1 + k * 1e-12) ends in a region where the
