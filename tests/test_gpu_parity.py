@@ -182,10 +182,9 @@ def test_circle20_full_size_matches_reference():
 
 def test_sequence200_full_size_matches_reference_cost():
     """The 200-camera distortion sequence at full size (50,000 points, ~375k observations).  The
-    reference stops on its iteration limit (TIMEOUT at
-    100) while the Huber re-weighting still lowers the cost by ~1e-6 per iteration, so accept /
-    reject decisions near rho = 0 depend on rounding and the paths differ after a few tens of
-    steps.  About one path in ten (tau scaled by 1 + k * 1e-12) ends in a region where the
+    reference stops on its iteration limit (TIMEOUT at 100) while the Huber re-weighting still
+    lowers the cost by ~1e-6 per iteration, so accept / reject decisions near rho = 0 depend on
+    rounding and the paths differ after a few tens of steps.  About one path in ten (tau scaled by 1 + k * 1e-12) ends in a region where the
     reference's LM stalls: rho stays near 0.003 for ever smaller steps until SMALL_UPDATE, a few
     1e-4 above the reference cost (the reference optimizer started from such a state stalls the
     same way).  So: FP64 at 100 iterations lands within 1e-5 of the reference cost, and of eight
