@@ -214,3 +214,20 @@ def test_invalid_arguments():
     for ranks in (1, 17):
         with pytest.raises(capi.V3dbaError):
             capi.tile_schedule(band_arrow(5), ranks=ranks)
+
+
+def test_independent_and_arrow_patterns_have_one_and_two_levels(monkeypatch):
+    monkeypatch.setenv("V3DBA_CHOL_SCHEDULE", "levels")
+    diag = np.eye(20, dtype=bool)                        # no coupling: every column is a leaf
+    s = capi.tile_schedule(diag)
+    assert s["n_levels"] == 1
+    arrow = np.eye(20, dtype=bool)
+    arrow[19, :] = True                                 # one dense row (shared intrinsics alone)
+    s = capi.tile_schedule(arrow)
+    assert s["n_levels"] == 2 and s["order"][-1] == 19
+    for pat in (diag, arrow):
+        s = capi.tile_schedule(pat)
+        A, b = spd_from_pattern(pat, seed=3)
+        x, _ = emulate(pat, A, b, s)
+        xr = np.linalg.solve(A, b)
+        assert np.abs(x - xr).max() <= 1e-12 * np.abs(xr).max()
