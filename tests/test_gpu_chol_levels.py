@@ -37,6 +37,8 @@ CASES = [
     ("random20", random_pattern(20, 0.15, 3), 20 * 64 - 1),
     ("groups24", groups(24, 6, 5), 24 * 64),
     ("small5", band_arrow(5), 5 * 64 - 30),
+    ("blockdiag16", np.eye(16, dtype=bool), 16 * 64 - 3),          # one level
+    ("arrow16", np.eye(16, dtype=bool) | (np.arange(16)[:, None] == 15), 16 * 64 - 7),  # two
 ]
 
 
