@@ -621,7 +621,8 @@ __global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* 
   }
 }
 
-// One warp per chunk of a camera's observations: partial sum_k W_k q_j(k) and sum_k T_k Y_j(k).
+// One warp per chunk of a camera's observations: partial sum_k W_k q_j(k) and sum_k T_k Y_j(k),
+// the latter as sum_k W_k (Vinv Y)_j(k).
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
@@ -636,7 +637,6 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, doubl
 #pragma unroll
   for (int t = 0; t < RV::VP; ++t) acc[t] = 0.0;
   const Real* oW = reinterpret_cast<const Real*>(s.o_W);
-  const Real* oT = reinterpret_cast<const Real*>(s.o_T);
   for (int idx = s.cc_beg[ch] + lane; idx < s.cc_end[ch]; idx += 32) {
     const int k = s.c_obs[idx];
     const int j = s.o_pt[k];
@@ -647,15 +647,15 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, doubl
 #pragma unroll
     for (int a = 0; a < DA; ++a) acc[a] += double(w[a * 3]) * q[0] + double(w[a * 3 + 1]) * q[1] + double(w[a * 3 + 2]) * q[2];
     if (DC > 0) {
-      Real t[L::SW], y[L::SY];
-      vload(oT + (size_t)k * L::SW, t);
-      vload(reinterpret_cast<const Real*>(s.p_Y) + (size_t)j * L::SY, y);
+      // T_k Y_j = W_k (Vinv_j Y_j): the point's Vinv Y is already stored, so no T_k gather
+      Real yv[L::SY];
+      vload(reinterpret_cast<const Real*>(s.p_YV) + (size_t)j * L::SY, yv);
 #pragma unroll
       for (int a = 0; a < DA; ++a)
 #pragma unroll
         for (int c = 0; c < DCc; ++c)
-          acc[DA + a * DCc + c] += double(t[a * 3]) * double(y[c]) + double(t[a * 3 + 1]) * double(y[DCc + c]) +
-                                   double(t[a * 3 + 2]) * double(y[2 * DCc + c]);
+          acc[DA + a * DCc + c] += double(w[a * 3]) * double(yv[c]) + double(w[a * 3 + 1]) * double(yv[DCc + c]) +
+                                   double(w[a * 3 + 2]) * double(yv[2 * DCc + c]);
     }
   }
   warp_reduce_transpose(acc);
