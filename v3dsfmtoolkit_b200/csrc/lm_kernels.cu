@@ -567,16 +567,35 @@ __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __rest
   for (int t = 0; t < SV::VP; ++t) acc[t] = Real(0);
   const Real* oT = reinterpret_cast<const Real*>(s.o_T);
   const Real* oW = reinterpret_cast<const Real*>(s.o_W);
-  for (int p = s.bc_beg[ch] + lane; p < s.bc_end[ch]; p += 32) {
-    const int k = s.pr_k[p], m = s.pr_m[p];
-    Real t[L::SW], w[L::SW];
-    vload(oT + (size_t)k * L::SW, t);
-    vload(oW + (size_t)m * L::SW, w);
+  // FP32 blocks: a lane takes its pairs p and p + 32 in one trip, so both pairs' gathers are in
+  // flight together (same summation order as one pair per trip); FP64 blocks keep one pair per
+  // trip, which already fills the register file (as do the 13-unknown FP32 blocks).
+  constexpr int U = sizeof(Real) == 4 && DA <= 11 ? 2 : 1;
+  const int end = s.bc_end[ch];
+  for (int p = s.bc_beg[ch] + lane; p < end; p += 32 * U) {
+    int k[U], m[U];
 #pragma unroll
-    for (int a = 0; a < DA; ++a)
+    for (int u = 0; u < U; ++u) {
+      const int q = p + 32 * u < end ? p + 32 * u : p;   // a missing second pair re-reads the first
+      k[u] = s.pr_k[q];
+      m[u] = s.pr_m[q];
+    }
+    Real t[U][L::SW], w[U][L::SW];
 #pragma unroll
-      for (int c = 0; c < DA; ++c)
-        acc[a * DA + c] += t[a * 3] * w[c * 3] + t[a * 3 + 1] * w[c * 3 + 1] + t[a * 3 + 2] * w[c * 3 + 2];
+    for (int u = 0; u < U; ++u) {
+      vload(oT + (size_t)k[u] * L::SW, t[u]);
+      vload(oW + (size_t)m[u] * L::SW, w[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (u > 0 && p + 32 * u >= end) break;
+#pragma unroll
+      for (int a = 0; a < DA; ++a)
+#pragma unroll
+        for (int c = 0; c < DA; ++c)
+          acc[a * DA + c] += t[u][a * 3] * w[u][c * 3] + t[u][a * 3 + 1] * w[u][c * 3 + 1] +
+                             t[u][a * 3 + 2] * w[u][c * 3 + 2];
+    }
   }
   warp_reduce_transpose(acc);
 #pragma unroll
