@@ -226,7 +226,8 @@ int v3dba_dense_cholesky_solve(int n, const double* S, const double* rhs, double
  * the library (about 0.8 MB per GPU, held until the process exits), so n must not exceed
  * V3DBA_NOALLOC_MAX_N (larger n is rejected with V3DBA_ERR_INVALID_ARGUMENT).  Calls share that
  * array: calls that overlap on the GPU race and must not be issued.  The first call on a device
- * looks up the array's device address and should come before any stream capture.  The work is
+ * looks up the array's device address (cached for the rest of the process) and should come before
+ * any stream capture.  The work is
  * enqueued on `stream` (a cudaStream_t, NULL for the default stream); synchronise before
  * reading x or fail (1 when a pivot is not positive). */
 #define V3DBA_NOALLOC_MAX_N 256
@@ -499,6 +500,13 @@ int v3dba_rotations_autotune(v3dba_rotations h, int* group);
 uint64_t v3dba_launch_count(void);
 
 const char* v3dba_error_string(int code);
+
+/* Allocation-failure injection for tests (no counterpart in the reference).  With k >= 0 the
+ * k-th device allocation the library requests from now on (0: the next one) fails as an
+ * exhausted cudaMalloc would: the entry point that asked returns V3DBA_ERR_OUT_OF_MEMORY after
+ * releasing what it holds, and later allocations succeed again.  k = -1 switches it off.
+ * Process-wide; not for production use. */
+int v3dba_debug_fail_allocation(long long k);
 
 #ifdef __cplusplus
 }

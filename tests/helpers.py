@@ -39,6 +39,29 @@ def param_rel(pa, pb):
     return out
 
 
+def similarity_align(R, T, X, R_ref, T_ref, X_ref):
+    """Moves the reconstruction (R, T, X) by the 7-DoF similarity (scale s, rotation Q,
+    translation t) that best maps its points onto X_ref in the least-squares sense (Umeyama's
+    closed form), and returns the moved (R', T', X'): X' = s Q X + t, R_i' = R_i Q^T,
+    T_i' = s T_i - R_i' t.  Every projection K (R_i X_j + T_i) is unchanged (up to the scale s of
+    the homogeneous point), so a bundle adjustment cannot tell the two apart: this is the gauge
+    freedom of metric BA, and two solvers that reach the same minimum may differ by it."""
+    X, X_ref = np.asarray(X, np.float64), np.asarray(X_ref, np.float64)
+    mu, mu_ref = X.mean(axis=0), X_ref.mean(axis=0)
+    A, B = X - mu, X_ref - mu_ref
+    U, sig, Vt = np.linalg.svd(B.T @ A / len(X))
+    D = np.eye(3)
+    if np.linalg.det(U) * np.linalg.det(Vt) < 0:
+        D[2, 2] = -1.0
+    Q = U @ D @ Vt
+    s = float(np.trace(np.diag(sig) @ D) / (A * A).sum(axis=1).mean())
+    t = mu_ref - s * Q @ mu
+    Xa = s * X @ Q.T + t
+    Ra = np.asarray(R, np.float64) @ Q.T
+    Ta = s * np.asarray(T, np.float64) - np.einsum("nij,j->ni", Ra, t)
+    return Ra, Ta, Xa
+
+
 ROT_GOLDEN = os.path.join(GOLDEN, "rotations")
 
 

@@ -34,12 +34,12 @@ def _headers():
     return sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h")))
 
 
-def _compile(src, verbose):
+def _compile(src, verbose, flags):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
     newest_dep = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _headers()])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
         return obj
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+    cmd = [NVCC, *ARCH, *flags, "-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -53,11 +53,10 @@ def _compile(src, verbose):
 def build(verbose: bool = False, extra_flags: list[str] | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    if extra_flags:
-        FLAGS.extend(extra_flags)
+    flags = FLAGS + list(extra_flags or [])   # per call: FLAGS itself stays as defined
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
+        objs = list(ex.map(lambda s: _compile(s, verbose, flags), srcs))
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lcuda"]
         if verbose:

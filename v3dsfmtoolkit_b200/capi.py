@@ -44,7 +44,7 @@ EXPORTS = (
     "v3dba_rotations_create", "v3dba_rotations_destroy", "v3dba_rotations_minimize", "v3dba_rotations_get",
     "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost", "v3dba_rotations_set_group",
     "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
-    "v3dba_triplet_stage_flat", "v3dba_cholesky_schedule", "v3dba_tile_schedule",
+    "v3dba_triplet_stage_flat", "v3dba_cholesky_schedule", "v3dba_tile_schedule", "v3dba_debug_fail_allocation",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -182,6 +182,7 @@ def _lib():
         L.v3dba_launch_count.argtypes = []
         L.v3dba_error_string.restype = C.c_char_p
         L.v3dba_error_string.argtypes = [C.c_int]
+        L.v3dba_debug_fail_allocation.argtypes = [C.c_longlong]
         _LIB = L
     return _LIB
 
@@ -230,6 +231,12 @@ def fp64_mma_peak_tflops() -> float:
 
 def launch_count() -> int:
     return int(_lib().v3dba_launch_count())
+
+
+def debug_fail_allocation(k: int):
+    """Makes the k-th device allocation from now on fail as an exhausted cudaMalloc would
+    (tests); -1 switches the injection off."""
+    check(_lib().v3dba_debug_fail_allocation(int(k)), "v3dba_debug_fail_allocation")
 
 
 class Handle:

@@ -535,6 +535,7 @@ namespace {
 template <typename T>
 int balloc(v3dba_batch_t h, T** p, size_t n) {
   void* q = nullptr;
+  if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
   cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
   if (e != cudaSuccess) { cudaGetLastError(); return V3DBA_ERR_OUT_OF_MEMORY; }
   h->allocs.push_back(q);

@@ -311,6 +311,7 @@ int tile_levels_plan(TileChol& tc, const std::vector<uint8_t>& orig) {
   }
   const int rc = tile_levels_build(tc, orig, chol_levels_ranks());
   if (rc || !tc.levels) return rc;
+  if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
   V3DBA_CUDA_TRY(cudaMalloc(&tc.d_lv, sizeof(int) * std::max<size_t>(tc.h_lv.size(), 1)));
   V3DBA_CUDA_TRY(cudaMemcpy(tc.d_lv, tc.h_lv.data(), sizeof(int) * tc.h_lv.size(), cudaMemcpyHostToDevice));
   return V3DBA_OK;

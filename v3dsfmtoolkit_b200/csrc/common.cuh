@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
@@ -17,6 +18,15 @@ void note_launches(uint64_t n);
 // True when no value is Inf or NaN (host; branch-free so the scan vectorises).
 bool all_finite(const double* p, size_t n);
 bool all_finite_f(const float* p, size_t n);
+
+// NVTX range for the scope of the object (names the LM stages on an Nsight timeline).  NVTX is
+// header-only: without a tool attached each push / pop is a branch on a null function pointer.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Host phase timings on stderr when the environment variable `env` is set (diagnostics).
 struct PhaseTrace {
@@ -45,6 +55,11 @@ struct Arena {
   };
   std::vector<Req> req_;
 };
+
+// Allocation-failure injection for tests (v3dba_debug_fail_allocation): true when the device
+// allocation about to be made is to report out-of-memory instead, as a failed cudaMalloc would.
+// Every device allocation of the handle / batch / structure paths asks first.
+bool injected_alloc_failure();
 
 // Raises the release threshold of the current device's stream-ordered pool once, so memory
 // freed by one handle is kept for the next (handles are created and destroyed in loops).

@@ -44,11 +44,23 @@ void PhaseTrace::mark(const char* phase, cudaStream_t st) {
   t = n;
 }
 
+// -1: off; k >= 0: the allocation k requests from now reports out-of-memory (then off again)
+static std::atomic<long long> g_alloc_countdown{-1};
+
+bool injected_alloc_failure() {
+  if (g_alloc_countdown.load(std::memory_order_relaxed) < 0) return false;
+  long long c = g_alloc_countdown.load(std::memory_order_relaxed);
+  while (c >= 0 && !g_alloc_countdown.compare_exchange_weak(c, c - 1, std::memory_order_relaxed)) {
+  }
+  return c == 0;
+}
+
 int Arena::commit(cudaStream_t st) {
   size_t total = 0;
   for (const Req& r : req_) total += r.bytes;
   int rc = ensure_pool();
   if (rc) return rc;
+  if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
   void* q = nullptr;
   V3DBA_CUDA_TRY(cudaMallocAsync(&q, std::max<size_t>(total, 256), st));
   base = static_cast<char*>(q);
@@ -80,3 +92,9 @@ int ensure_pool() {
 }
 
 }  // namespace v3dba
+
+extern "C" int v3dba_debug_fail_allocation(long long k) {
+  if (k < -1) return V3DBA_ERR_INVALID_ARGUMENT;
+  v3dba::g_alloc_countdown.store(k);
+  return V3DBA_OK;
+}

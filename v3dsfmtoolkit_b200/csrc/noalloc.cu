@@ -17,6 +17,7 @@
 // device looks up the array's device address (cudaGetSymbolAddress) with that device current;
 // make that first call before any stream capture.  The work is enqueued on the caller's stream
 // and the call returns without waiting; synchronise the stream before reading x or fail.
+#include <atomic>
 #include <cstdio>
 
 #include "common.cuh"
@@ -89,21 +90,28 @@ __global__ void k_na_unpack(const double* __restrict__ xs, int n, double* __rest
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = xs[i];
 }
 
-// Device address of g_noalloc_scratch for each device, looked up once with that device current.
+// Device address of g_noalloc_scratch for each device, looked up once per process with that
+// device current and cached.  The cache entries are atomics: two host threads making their first
+// call on one device at once both look the address up (the same value) and store it, with no data
+// race.  The cached address belongs to the device's primary context; after a cudaDeviceReset the
+// next call must come from a fresh process.
 double* scratch_address(int dev) {
   constexpr int kMaxDevices = 64;
-  static double* addr[kMaxDevices] = {nullptr};
+  static std::atomic<double*> addr[kMaxDevices];
   if (dev < 0 || dev >= kMaxDevices) return nullptr;
-  if (addr[dev] == nullptr) {
+  double* a = addr[dev].load(std::memory_order_acquire);
+  if (a == nullptr) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) {
+      cudaGetLastError();
       fprintf(stderr, "v3dba: cudaGetSymbolAddress of the no-allocation scratch failed: %s\n", cudaGetErrorString(e));
       return nullptr;
     }
-    addr[dev] = static_cast<double*>(p);
+    a = static_cast<double*>(p);
+    addr[dev].store(a, std::memory_order_release);
   }
-  return addr[dev];
+  return a;
 }
 
 }  // namespace

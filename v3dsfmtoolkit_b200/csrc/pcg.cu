@@ -586,6 +586,7 @@ int pcg_plan(PcgState& ps, const std::vector<int>& b_i, const std::vector<int>& 
   }
   auto up = [](auto** d, const auto& h) -> int {
     using T = typename std::remove_reference<decltype(h)>::type::value_type;
+    if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
     V3DBA_CUDA_TRY(cudaMalloc(d, sizeof(T) * std::max<size_t>(h.size(), 1)));
     if (!h.empty()) V3DBA_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
     return V3DBA_OK;
@@ -599,13 +600,19 @@ int pcg_plan(PcgState& ps, const std::vector<int>& b_i, const std::vector<int>& 
 
 int pcg_alloc(PcgState& ps, int nb, int N, int DA) {
   const size_t n = (size_t)N * DA;
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.Sb, sizeof(double) * (size_t)std::max(nb, 1) * DA * DA));
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.Pinv, sizeof(double) * (size_t)std::max(N, 1) * DA * DA));
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.vec, sizeof(double) * 8 * std::max<size_t>(n, 1)));   // b r z p Ap t p2 r2
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.part, sizeof(double) * 2 * kPartStride * kPcgMaxGrid));
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.gauge_rows, sizeof(double) * kGaugeTri * (size_t)std::max(N, 1)));
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.gauge_L, sizeof(double) * (kGaugeTri + 1)));
-  V3DBA_CUDA_TRY(cudaMalloc(&ps.iters, sizeof(int)));
+  auto get = [](auto** d, size_t bytes) -> int {
+    if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
+    V3DBA_CUDA_TRY(cudaMalloc(d, bytes));
+    return V3DBA_OK;
+  };
+  int rc;
+  if ((rc = get(&ps.Sb, sizeof(double) * (size_t)std::max(nb, 1) * DA * DA)) ||
+      (rc = get(&ps.Pinv, sizeof(double) * (size_t)std::max(N, 1) * DA * DA)) ||
+      (rc = get(&ps.vec, sizeof(double) * 8 * std::max<size_t>(n, 1))) ||   // b r z p Ap t p2 r2
+      (rc = get(&ps.part, sizeof(double) * 2 * kPartStride * kPcgMaxGrid)) ||
+      (rc = get(&ps.gauge_rows, sizeof(double) * kGaugeTri * (size_t)std::max(N, 1))) ||
+      (rc = get(&ps.gauge_L, sizeof(double) * (kGaugeTri + 1))) || (rc = get(&ps.iters, sizeof(int))))
+    return rc;
   ps.b = ps.vec;
   ps.ready = true;
   return V3DBA_OK;

@@ -86,6 +86,7 @@ int dalloc(v3dba_handle h, T** p, size_t count) {
   const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
   int rc0 = ensure_pool();
   if (rc0) return rc0;
+  if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
   cudaError_t e = cudaMallocAsync(&q, bytes, h->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -161,8 +162,8 @@ int use_dense(v3dba_handle h) {
     std::vector<uint8_t> nz = h->tile_nz;
     int rc = tile_chol_plan(h->chol, std::max(s.n, 1), nz);
     if (rc) return rc;
-    if ((rc = dalloc(h, &h->S_dense, (size_t)h->chol.ld * h->chol.n_pad))) return rc;
-    if ((rc = dalloc(h, &h->x_dense, (size_t)h->chol.n_pad))) return rc;
+    if (!h->S_dense && (rc = dalloc(h, &h->S_dense, (size_t)h->chol.ld * h->chol.n_pad))) return rc;
+    if (!h->x_dense && (rc = dalloc(h, &h->x_dense, (size_t)h->chol.n_pad))) return rc;
     h->dense_ready = true;
   }
   s.n_pad = h->chol.n_pad;
@@ -180,10 +181,17 @@ int use_dense(v3dba_handle h) {
 int use_pcg(v3dba_handle h) {
   DevState& s = h->s;
   if (!h->pcg.ready) {
+    pcg_free(h->pcg);   // a retry after a failed attempt (out of memory) starts clean
     int rc = pcg_plan(h->pcg, h->blk_i, h->blk_l, s.d.N);
+    if (!rc) rc = pcg_alloc(h->pcg, s.nb, s.d.N, s.d.DA);
+    if (rc) {
+      pcg_free(h->pcg);
+      return rc;
+    }
+  }
+  if (!h->x_pcg) {
+    const int rc = dalloc(h, &h->x_pcg, (size_t)std::max(s.n, 1));
     if (rc) return rc;
-    if ((rc = pcg_alloc(h->pcg, s.nb, s.d.N, s.d.DA))) return rc;
-    if ((rc = dalloc(h, &h->x_pcg, (size_t)std::max(s.n, 1)))) return rc;
   }
   s.n_pad = s.n;
   s.ld = 1;
@@ -316,6 +324,7 @@ uint64_t v3dba_launch_count(void) { return g_launches.load(); }
 
 int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   if (!p || !out) return V3DBA_ERR_INVALID_ARGUMENT;
+  NvtxRange nvtx("v3dba_create");
   PhaseTrace trace("V3DBA_TRACE_CREATE", "v3dba_create");
   *out = nullptr;
   int dA, dC;
@@ -592,55 +601,67 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
               const v3dba_options& o, double out[6]) {
   DevState& s = h->s;
   cudaStream_t st = h->stream;
-  V3DBA_CUDA_TRY(launch_pdl(k_trial_setup, dim3(1), dim3(1), 0, st, lambda, s.d_lambda, s.d_fail));
-  V3DBA_LAUNCH_CHECK();
+  NvtxRange nvtx_trial("v3dba.trial");
   int rc;
-  if (!pcg && (rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
-  if ((rc = ops->build_reduced(s, st))) return rc;
+  {
+    NvtxRange nvtx("v3dba.reduced_system");
+    V3DBA_CUDA_TRY(launch_pdl(k_trial_setup, dim3(1), dim3(1), 0, st, lambda, s.d_lambda, s.d_fail));
+    V3DBA_LAUNCH_CHECK();
+    if (!pcg && (rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
+    if ((rc = ops->build_reduced(s, st))) return rc;
+  }
   int fallback = 0;
-  if (pcg && precond != V3DBA_PRECOND_BLOCK_JACOBI) {
-    // learned factor or block-Jacobi + gauge space; plain block-Jacobi re-solves the trial when
-    // that breaks down
-    const bool learned = precond == V3DBA_PRECOND_LEARNED;
-    V3DBA_CUDA_TRY(cudaMemsetAsync(h->gnn_fail, 0, sizeof(int), st));
-    if ((rc = gauge_frames(s.cur.R, s.cur.T, s.d.N, s.d.nnA, h->gauge_frames, st))) return rc;
-    if (learned &&
-        ((rc = gnn_features(h->gnn, s.Sb, fp64, s.diag_blk, h->gnn_cinv, h->gnn_xe, h->gnn_xn, h->gnn_fail, st)) ||
-         (rc = gnn_precond_blocks(h->precond, h->gnn, h->gnn_cinv, h->gnn_xe, h->gnn_xn, h->gnn_ehat, st))))
-      return rc;
-    int ffail = 0;
-    V3DBA_CUDA_TRY(cudaMemcpyAsync(&ffail, h->gnn_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
-    V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
-    int its = 0;
-    if (!ffail) {
-      PcgPrecond P;
-      if (learned) { P.cinv = h->gnn_cinv; P.ehat = h->gnn_ehat; }
-      else P.frames = h->gauge_frames;
-      if ((rc = pcg_solve_precond(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x,
-                                  h->gnn_fail, st, P)))
+  auto solve = [&]() -> int {
+    if (pcg && precond != V3DBA_PRECOND_BLOCK_JACOBI) {
+      // learned factor or block-Jacobi + gauge space; plain block-Jacobi re-solves the trial when
+      // that breaks down
+      const bool learned = precond == V3DBA_PRECOND_LEARNED;
+      V3DBA_CUDA_TRY(cudaMemsetAsync(h->gnn_fail, 0, sizeof(int), st));
+      if ((rc = gauge_frames(s.cur.R, s.cur.T, s.d.N, s.d.nnA, h->gauge_frames, st))) return rc;
+      if (learned &&
+          ((rc = gnn_features(h->gnn, s.Sb, fp64, s.diag_blk, h->gnn_cinv, h->gnn_xe, h->gnn_xn, h->gnn_fail, st)) ||
+           (rc = gnn_precond_blocks(h->precond, h->gnn, h->gnn_cinv, h->gnn_xe, h->gnn_xn, h->gnn_ehat, st))))
         return rc;
-      V3DBA_CUDA_TRY(cudaMemcpyAsync(&its, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+      int ffail = 0;
       V3DBA_CUDA_TRY(cudaMemcpyAsync(&ffail, h->gnn_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
       V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
-    }
-    h->h_scalars[10] = its;
-    // an iteration-capped solve is an inexact step, as with block-Jacobi; only a breakdown (a
-    // diagonal block that is not positive definite, or p.Ap <= 0) falls back
-    if (ffail) {
-      fallback = 1;
+      int its = 0;
+      if (!ffail) {
+        PcgPrecond P;
+        if (learned) { P.cinv = h->gnn_cinv; P.ehat = h->gnn_ehat; }
+        else P.frames = h->gauge_frames;
+        if ((rc = pcg_solve_precond(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x,
+                                    h->gnn_fail, st, P)))
+          return rc;
+        V3DBA_CUDA_TRY(cudaMemcpyAsync(&its, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+        V3DBA_CUDA_TRY(cudaMemcpyAsync(&ffail, h->gnn_fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+        V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+      }
+      h->h_scalars[10] = its;
+      // an iteration-capped solve is an inexact step, as with block-Jacobi; only a breakdown (a
+      // diagonal block that is not positive definite, or p.Ap <= 0) falls back
+      if (ffail) {
+        fallback = 1;
+        if ((rc = pcg_solve(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x, s.d_fail, st)))
+          return rc;
+        V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 9, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
+      } else {
+        std::memcpy(h->h_scalars + 9, &its, sizeof(int));
+      }
+    } else if (pcg) {
       if ((rc = pcg_solve(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x, s.d_fail, st)))
         return rc;
       V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 9, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
-    } else {
-      std::memcpy(h->h_scalars + 9, &its, sizeof(int));
-    }
-  } else if (pcg) {
-    if ((rc = pcg_solve(h->pcg, s.d.N, s.d.DA, fp64, o.pcg_tolerance, o.pcg_max_iterations, s.x, s.d_fail, st)))
+    } else if ((rc = tile_chol_solve(h->chol, s.S, s.x, s.d_fail, st))) {
       return rc;
-    V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 9, h->pcg.iters, sizeof(int), cudaMemcpyDeviceToHost, st));
-  } else if ((rc = tile_chol_solve(h->chol, s.S, s.x, s.d_fail, st))) {
-    return rc;
+    }
+    return V3DBA_OK;
+  };
+  {
+    NvtxRange nvtx("v3dba.reduced_solve");
+    if ((rc = solve())) return rc;
   }
+  NvtxRange nvtx_finish("v3dba.backsub_update_cost");
   if ((rc = ops->finish_trial(s, st))) return rc;
   // one copy: the relinearisation scalars (h_scalars[16..18]) and the trial's {new cost, |d|^2,
   // d.g, failure flag} (h_scalars[20..23], the flag stored by k_trial_finalize)
@@ -667,6 +688,7 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
   std::memset(res, 0, sizeof(*res));
   res->status = V3DBA_STATUS_TIMEOUT;
   res->fp64_from_iteration = -1;
+  NvtxRange nvtx("v3dba_minimize");
   DevState& s = h->s;
   const Dims& D = s.d;
   bool fp64 = (o.precision == V3DBA_PRECISION_FP64);
@@ -710,6 +732,7 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
     if (o.verbosity >= 2) printf("SparseLevenbergOptimizer: currentIteration: %d\n", it);
     if (relinearize_again && !compute_derivatives) {
       // same parameters, same FP64 cost and gradient; only the block precision changes
+      NvtxRange nvtx_relin("v3dba.relinearize");
       if ((rc = ops->relinearize(s, false, o.tau, st))) return rc;
     }
     relinearize_again = false;
@@ -742,6 +765,7 @@ extern "C" int v3dba_minimize(v3dba_handle h, const v3dba_options* opts, v3dba_r
       }
     };
     if (compute_derivatives) {
+      NvtxRange nvtx_relin("v3dba.relinearize");
       if ((rc = ops->relinearize(s, it == 0, o.tau, st))) return rc;
       V3DBA_CUDA_TRY(cudaMemcpyAsync(h->h_scalars + 16, s.d_relin, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
       V3DBA_CUDA_TRY(cudaStreamSynchronize(st));

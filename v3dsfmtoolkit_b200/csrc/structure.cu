@@ -225,6 +225,7 @@ struct Scratch {
   template <typename T>
   int get(T** p, size_t n) {
     void* q = nullptr;
+    if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
     cudaError_t e = cudaMallocAsync(&q, sizeof(T) * std::max<size_t>(n, 1), st);
     if (e != cudaSuccess) {
       cudaGetLastError();

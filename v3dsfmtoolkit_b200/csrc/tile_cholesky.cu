@@ -237,6 +237,7 @@ __global__ void __launch_bounds__(256) k_chol_zero(double* __restrict__ S, int l
 // ---- host ----------------------------------------------------------------------------------
 
 int tile_chol_plan(TileChol& tc, int n, std::vector<uint8_t>& nz) {
+  tile_chol_free(tc);   // a plan retried after a failed one (out of memory) starts clean
   const int nt = (n + TB - 1) / TB;
   tc.n = n;
   tc.nt = nt;
@@ -280,6 +281,7 @@ int tile_chol_plan(TileChol& tc, int n, std::vector<uint8_t>& nz) {
       if (r == nt || nz[r * nt + c]) tc.h_tiles.push_back(r * (nt + 1) + c);
 
   auto up = [](int** d, const std::vector<int>& h) -> int {
+    if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
     V3DBA_CUDA_TRY(cudaMalloc(d, sizeof(int) * std::max<size_t>(h.size(), 1)));
     if (!h.empty()) V3DBA_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
     return V3DBA_OK;
@@ -291,6 +293,7 @@ int tile_chol_plan(TileChol& tc, int n, std::vector<uint8_t>& nz) {
   if ((rc = up(&tc.d_upd_c, tc.h_upd_c))) return rc;
   if ((rc = up(&tc.d_upd_ptr, tc.h_upd_ptr))) return rc;
   if ((rc = up(&tc.d_tiles, tc.h_tiles))) return rc;
+  if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
   V3DBA_CUDA_TRY(cudaMalloc(&tc.d_ldiag, sizeof(double) * (size_t)nt * TB * TB));
   if ((rc = tile_levels_plan(tc, orig))) return rc;
   static bool attr_set = false;
