@@ -15,7 +15,9 @@ reduced-system Cholesky (dtype "f32+f64").
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 
 --impl reference times the reference's own CPU optimizer (compiled from its sources) on the same
-scene, on a bounded sample of LM iterations per step, single-threaded as the reference is.
+scene: complete minimize() runs to its own stop, setup included, single-threaded as the reference
+is (one run on the 200-camera scene, ~75 s).  --workload circle20 is the 20-camera plain metric
+BA (FP64).
 With N > 1 every rank solves its own replica (a single BA does not shard; "replicas only").
 
 --workload cluster2000 measures the large-scene path: 2,000 cameras in 20 clusters, 1M points,
@@ -65,10 +67,15 @@ WORKLOAD = "sequence200"
 METRIC = "LM iterations/s to the reference cost (distortion BA, 200 cams / 50k pts / ~375k obs)"
 # bundle-adjustment workloads timed to the reference optimizer's own final cost
 BA_WORKLOADS = {
-    "sequence200": dict(metric=METRIC, model="CommonInternalsMetricBundleOptimizer RADIAL_TANGENTIAL"),
+    "sequence200": dict(metric=METRIC, model="CommonInternalsMetricBundleOptimizer RADIAL_TANGENTIAL",
+                        precision="mixed"),
+    "circle20": dict(metric="LM iterations/s to the reference cost (plain metric BA, 20 cams / 2k pts / 8k obs)",
+                     model="StdMetricBundleOptimizer (plain least squares, inlier threshold 1e6 px)", precision="fp64"),
     "stereo300": dict(metric="LM iterations/s to the reference cost (rig BA, 300 poses x 2 cameras / 39k pts / "
-                             "~450k obs)", model="StereoMetricBundleOptimizer (binocular rig)"),
+                             "~450k obs)", model="StereoMetricBundleOptimizer (binocular rig)", precision="mixed"),
 }
+PRECISION_TEXT = {"mixed": "FP32 normal-equation blocks, FP64 residual/gradient/cost/Cholesky",
+                  "fp64": "FP64 throughout"}
 UNIT = "LM iterations/s"
 REL_TOL = 1e-6
 TAU = 1e-3           # the reference's default initial damping factor
@@ -83,8 +90,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["sequence200", "stereo300", "triplets4096", "tripletstage4096", "cluster2000",
-                                           "rotations10000"],
+    ap.add_argument("--workload", choices=["sequence200", "circle20", "stereo300", "triplets4096", "tripletstage4096",
+                                           "cluster2000", "rotations10000"],
                     default="sequence200")
     ap.add_argument("--profile-stages", type=int, default=0, metavar="R",
                     help="run every stage of one LM iteration R times (mixed precision) and exit; "
@@ -110,7 +117,20 @@ def make_scene(workload=WORKLOAD):
     from v3dsfmtoolkit_b200 import scenes
     if workload == "stereo300":
         return scenes.stereo_rig_scene(n_poses=300, n_points=40000, seed=0, window=6, outlier_frac=0.01)
+    if workload == "circle20":
+        return scenes.circle_scene()
     return scenes.sequence_scene()
+
+
+def ba_config(wl, sc, ref):
+    """The workload's `config` object: the same keys and values in both arms (the GPU arm and the
+    reference arm), so that the two lines describe one workload."""
+    return {"workload": wl, "n_cameras": sc.n_cams, "n_points": sc.n_points, "n_observations": sc.n_obs,
+            "model": BA_WORKLOADS[wl]["model"], "huber_threshold_px": sc.inlier_threshold,
+            "stop": f"cost <= reference cost * (1 + {REL_TOL})", "reference_cost": ref["cost"],
+            "reference_iterations": ref["iterations"],
+            "l2": "GPU arm: flushed (256 MiB write) before every step",
+            "parallelism": "one problem per device; replicas for N > 1"}
 
 
 def scene_digest(sc):
@@ -211,8 +231,10 @@ def run_ours(args, rank, world, local_rank):
     if scene_digest(sc) != ref["digest"]:
         raise RuntimeError("generated scene differs from the one the reference cost was recorded on")
     target = ref["cost"] * (1.0 + REL_TOL)
+    prec = BA_WORKLOADS[wl]["precision"]
     h = capi.Handle.from_scene(sc)
-    opts = capi.default_options(max_iterations=2000, stop_cost=target, precision=capi.PRECISION_MIXED)
+    opts = capi.default_options(max_iterations=2000, stop_cost=target,
+                                precision=capi.PRECISION_FP64 if prec == "fp64" else capi.PRECISION_MIXED)
     flush = torch.empty(int(256 * 2 ** 20), dtype=torch.uint8, device="cuda")
 
     # Each step solves the same scene with tau scaled by (1 + k * 1e-12), k = the step index.  The
@@ -266,7 +288,7 @@ def run_ours(args, rank, world, local_rank):
     # rooflines: the dominant kernel of an LM iteration (the tile Cholesky, FP64 tensor pipe) and
     # the largest HBM-bound kernel (linearisation); durations with CUDA events on the library's
     # stream, DRAM traffic per launch from the committed ncu capture (profiles/traffic.json)
-    st_ms = h.profile_stages(capi.PRECISION_MIXED, reps=20)
+    st_ms = h.profile_stages(opts.precision, reps=20)
     peak, peak_kind = measured_peaks()
     traffic = {}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
@@ -301,9 +323,9 @@ def run_ours(args, rank, world, local_rank):
     e2e = None
     if not args.no_e2e:
         e2e_steps = max(1, min(3, args.steps))
-        hb = sum(np.asarray(a).nbytes for a in (sc.K, sc.R, sc.T, sc.dist, sc.X, sc.meas)) + \
+        hb = sum(np.asarray(a).nbytes for a in (sc.K, sc.R, sc.T, sc.dist, sc.X, sc.meas) if a is not None) + \
             sc.view.astype(np.int32).nbytes + sc.point.astype(np.int32).nbytes
-        db = sum(np.asarray(a).nbytes for a in (sc.K, sc.R, sc.T, sc.dist, sc.X))
+        db = sum(np.asarray(a).nbytes for a in (sc.K, sc.R, sc.T, sc.dist, sc.X) if a is not None)
         it_e, t_e = 0, 0.0
         parts = {"create_s": 0.0, "minimize_s": 0.0, "get_params_s": 0.0}
         # one untimed call first, like the warm-up steps above: the main handle still holds its
@@ -345,7 +367,7 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(sc, iters_per_sample=10 if wl == "sequence200" else 4, workload=wl)
+        cpu = cpu_baseline_sample(sc, iters_per_sample={"sequence200": 10, "circle20": 100}.get(wl, 4), workload=wl)
         cpu["reference_iterations_to_cost"] = ref["iterations"]
         cpu["time_to_reference_cost_s_est"] = round(ref["iterations"] / cpu["value"], 2)
 
@@ -353,13 +375,9 @@ def run_ours(args, rank, world, local_rank):
         "metric": BA_WORKLOADS[wl]["metric"], "value": round(total_it_all / (total_ms_max * 1e-3), 3), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total_ms_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
-        "config": {"workload": wl, "n_cameras": sc.n_cams, "n_points": sc.n_points,
-                   "n_observations": sc.n_obs, "model": BA_WORKLOADS[wl]["model"],
-                   "huber_threshold_px": sc.inlier_threshold, "stop": f"cost <= reference cost * (1 + {REL_TOL})",
-                   "reference_cost": ref["cost"], "l2": "flushed (256 MiB write) before every step",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "precision": "FP32 normal-equation blocks, FP64 residual/gradient/cost/Cholesky"},
+        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64", "data": "synthetic (seeded)",
+        "config": ba_config(wl, sc, ref),
+        "precision": PRECISION_TEXT[prec], "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "time_to_reference_cost_s": (round(float(np.mean([m for m, ok in zip(dev_ms, reached) if ok])) * 1e-3, 5)
                                      if any(reached) else None),
         "lm_iterations_per_step": round(total_it / args.steps, 2),
@@ -485,30 +503,41 @@ def run_reference(args, rank, world):
         return
     from oracle.bindings import Reference, Restatement, reference_available
     wl = args.workload if args.workload in BA_WORKLOADS else WORKLOAD
+    ref = load_reference_target(wl)
     sc = make_scene(wl)
     kind = "reference" if reference_available() else "port"
     eng = Reference() if kind == "reference" else Restatement()
-    m = max(2, min(10, 100 // max(args.steps, 1)))
-    if wl == "stereo300":
-        m = 2   # ~1.5 s per iteration on one core
-    for _ in range(args.warmup):
-        eng.minimize(sc, max_iterations=1)
-    t0 = time.perf_counter()
-    its = 0
-    for _ in range(args.steps):
-        _, info = eng.minimize(sc, max_iterations=m)
+    # One step = one complete minimize() from the scene's start to the reference's own stop (its
+    # recorded iteration limit or stopping test), its one-time setup (structure, SYMAMD ordering)
+    # included once, as a caller pays it.  On the 200-camera scene one run is ~75 s of one host
+    # core, so the arm times complete runs until K are done or 60 s have passed, with at least
+    # one: the whole arm ends within a few minutes for any K.
+    small = make_scene("circle20")
+    for _ in range(min(args.warmup, 1)):
+        eng.minimize(small, max_iterations=2)
+    its, runs, t_total = 0, 0, 0.0
+    statuses = []
+    while runs < max(1, args.steps) and (runs == 0 or t_total < 60.0):
+        t0 = time.perf_counter()
+        params, info = eng.minimize(sc, max_iterations=ref["max_iterations"])
+        t_total += time.perf_counter() - t0
         its += info["iterations"]
-    dt = time.perf_counter() - t0
-    v = its / dt
+        runs += 1
+        statuses.append(info["status"])
+    cost = eng.cost(sc, params)
+    v = its / t_total
+    sample = (f"{runs} complete minimize() run(s) of {its // runs} LM iterations (the reference's own stop, status "
+              f"{statuses[-1]}), setup included, {t_total:.1f} s on 1 host core")
     line = {
         "impl": "reference", "metric": BA_WORKLOADS[wl]["metric"], "value": round(v, 4), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded)",
-        "config": {"workload": wl, "n_cameras": sc.n_cams, "n_points": sc.n_points,
-                   "n_observations": sc.n_obs, "sample": f"{m} LM iterations of minimize() per step"},
-        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": kind,
-                         "sample": f"{args.steps} x minimize() of {m} LM iterations on {wl}"},
+        "steps": runs, "warmup": args.warmup, "steps_requested": args.steps,
+        "ms_per_step": round(t_total / runs * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": ba_config(wl, sc, ref),
+        "precision": "FP64 throughout (the reference's own LDL^T of the full normal equations)",
+        "parallelism": "1 host core (the reference is single-threaded)",
+        "time_to_reference_cost_s": round(t_total / runs, 3), "final_cost": cost,
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -516,6 +545,8 @@ def run_reference(args, rank, world):
 
 TRIPLET_METRIC = "triplet BAs/s (4096 triplets, 3 cams, 50-800 points, 5 LM iterations)"
 TRIPLET_UNIT = "triplet BAs/s"
+TRIPLETS_PER_GPU = 4096
+C_RESULT_BYTES = 64   # one v3dba_result per problem
 
 
 def run_triplets(args, rank, world, local_rank):
@@ -523,9 +554,13 @@ def run_triplets(args, rank, world, local_rank):
     from v3dsfmtoolkit_b200 import capi, distributed, scenes
     torch.cuda.set_device(local_rank)
     dist = distributed.init("nccl")
-    trips = scenes.triplet_batch(seed=rank)
+    # the job: `world` blocks of 4096 seeded triplets (block k has seed k); each rank solves its
+    # contiguous shard of the world x 4096 triplets, which is exactly one block
+    lo, hi = distributed.shard_range(world * TRIPLETS_PER_GPU, rank, world)
+    trips = scenes.triplet_batch(n_triplets=hi - lo, seed=lo // TRIPLETS_PER_GPU)
     n = len(trips)
-    b = capi.Batch(trips)
+    flat = capi.concat_problems(trips)   # the caller's arrays, built once
+    b = capi.Batch.from_flat(flat)
     opts = capi.default_options(max_iterations=5)
     sched = b.autotune(opts)
     flush = torch.empty(int(256 * 2 ** 20), dtype=torch.uint8, device="cuda")
@@ -553,20 +588,30 @@ def run_triplets(args, rank, world, local_rank):
     done = distributed.reduce_scalar(dist, n * args.steps, "sum", device="cuda")
     e2e = None
     if not args.no_e2e:
-        t0 = time.perf_counter()
         steps_e = max(1, min(3, args.steps))
+        parts = {"create_s": 0.0, "minimize_s": 0.0, "get_params_s": 0.0}
+        te_local = 0.0
         for _ in range(steps_e):
-            b2 = capi.Batch(trips)            # host -> device copy of every triplet
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b2 = capi.Batch.from_flat(flat)   # host -> device copy and layout of every triplet
+            t1 = time.perf_counter()
             b2.set_schedule(*sched)
-            b2.minimize(opts)
-            for i in range(n):
-                b2.get_params(i)              # device -> host of every solution
+            b2.minimize(opts)                 # results of every triplet back on the host
+            t2 = time.perf_counter()
+            b2.get_all_params()               # device -> host of every solution
+            t3 = time.perf_counter()
             b2.close()
-        te = distributed.reduce_scalar(dist, time.perf_counter() - t0, "max", device="cuda")
-        hb = sum(sc.K.nbytes + sc.R.nbytes + sc.T.nbytes + sc.X.nbytes + sc.meas.nbytes + 8 * sc.n_obs for sc in trips)
-        db = sum(sc.R.nbytes + sc.T.nbytes + sc.X.nbytes for sc in trips)
+            te_local += time.perf_counter() - t0
+            parts["create_s"] += t1 - t0
+            parts["minimize_s"] += t2 - t1
+            parts["get_params_s"] += t3 - t2
+        te = distributed.reduce_scalar(dist, te_local, "max", device="cuda")
+        hb = sum(int(a.nbytes) for a in flat.values())
+        db = int(flat["R"].nbytes + flat["T"].nbytes + flat["X"].nbytes) + n * C_RESULT_BYTES
         e2e = {"value": round(steps_e * n * world / te, 2), "unit": TRIPLET_UNIT, "h2d_bytes_per_step": int(hb),
-               "d2h_bytes_per_step": int(db)}
+               "d2h_bytes_per_step": int(db), "per_step_s": {k: round(v / steps_e, 5) for k, v in parts.items()}}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.bindings import Reference, Restatement, reference_available

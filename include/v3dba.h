@@ -342,6 +342,15 @@ int v3dba_profile_stages(v3dba_handle h, int precision, int reps, double* ms);
  * problem, one thread block per problem at a time, largest problems first. */
 typedef struct v3dba_batch_s* v3dba_batch_t;
 int v3dba_batch_create(const v3dba_problem* problems, int count, v3dba_batch_t* out);
+/* The same batch from flat arrays, for callers that keep all problems in one set of buffers:
+ * problem p has n_cameras[p] cameras, n_points[p] points and n_measurements[p] observations;
+ * K, R (9 per camera), T (3 per camera), X (3 per point), measurements (2 per observation),
+ * view and point (one per observation, indices local to the problem) hold the problems one
+ * after another in order.  Same checks and results as v3dba_batch_create. */
+int v3dba_batch_create_flat(int count, const int* n_cameras, const int* n_points, const int* n_measurements,
+                            const double* inlier_threshold, const double* K, const double* R, const double* T,
+                            const double* X, const double* measurements, const int* view, const int* point,
+                            v3dba_batch_t* out);
 int v3dba_batch_destroy(v3dba_batch_t b);
 /* results (may be NULL) receives one entry per problem; device_ms (may be NULL) the device time. */
 int v3dba_batch_minimize(v3dba_batch_t b, const v3dba_options* opts, v3dba_result* results, double* device_ms);

@@ -45,6 +45,7 @@ EXPORTS = (
     "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost", "v3dba_rotations_set_group",
     "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
     "v3dba_triplet_stage_flat", "v3dba_cholesky_schedule", "v3dba_tile_schedule", "v3dba_debug_fail_allocation",
+    "v3dba_batch_create_flat",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -128,6 +129,8 @@ def _lib():
             [C.POINTER(_dp)] * 5 + [C.POINTER(Result)]
         L.v3dba_profile_stages.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.v3dba_batch_create.argtypes = [C.POINTER(Problem), C.c_int, C.POINTER(C.c_void_p)]
+        L.v3dba_batch_create_flat.argtypes = [C.c_int, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
+                                              C.POINTER(C.c_void_p)]
         L.v3dba_batch_destroy.argtypes = [C.c_void_p]
         L.v3dba_batch_minimize.argtypes = [C.c_void_p, C.POINTER(Options), C.POINTER(Result), _dp]
         L.v3dba_batch_reset.argtypes = [C.c_void_p]
@@ -579,8 +582,11 @@ class Batch:
     """Many small independent problems (StdMetricBundleOptimizer, <= 4 cameras each) solved in one
     persistent launch (wraps v3dba_batch_*)."""
 
-    def __init__(self, scenes):
+    def __init__(self, scenes=None, flat=None):
         L = _lib()
+        if flat is not None:
+            self._init_flat(L, flat)
+            return
         self.scenes = list(scenes)
         self._keep = []
         probs = (Problem * len(self.scenes))()
@@ -595,6 +601,29 @@ class Batch:
         check(L.v3dba_batch_create(probs, len(self.scenes), C.byref(h)), "v3dba_batch_create")
         self.h = h
         self.count = len(self.scenes)
+
+    def _init_flat(self, L, f):
+        self.scenes = None
+        self.flat = f
+        h = C.c_void_p()
+        check(L.v3dba_batch_create_flat(len(f["n_cams"]), _i(f["n_cams"]), _i(f["n_points"]), _i(f["n_obs"]),
+                                        _d(f["thr"]), _d(f["K"]), _d(f["R"]), _d(f["T"]), _d(f["X"]), _d(f["meas"]),
+                                        _i(f["view"]), _i(f["point"]), C.byref(h)), "v3dba_batch_create_flat")
+        self.h = h
+        self.count = len(f["n_cams"])
+
+    @classmethod
+    def from_flat(cls, flat):
+        """A batch from the flat arrays of :func:`concat_problems` (v3dba_batch_create_flat)."""
+        return cls(flat=flat)
+
+    def get_all_params(self):
+        """(R, T, X) of every problem, concatenated in problem order (v3dba_batch_get_all_params)."""
+        f = self.flat if self.scenes is None else concat_problems(self.scenes)
+        nc, npt = int(f["n_cams"].sum()), int(f["n_points"].sum())
+        R, T, X = np.zeros((nc, 3, 3)), np.zeros((nc, 3)), np.zeros((npt, 3))
+        check(_lib().v3dba_batch_get_all_params(self.h, _d(R), _d(T), _d(X)), "v3dba_batch_get_all_params")
+        return R, T, X
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
@@ -631,6 +660,23 @@ class Batch:
         R, T, X = np.zeros((sc.n_cams, 3, 3)), np.zeros((sc.n_cams, 3)), np.zeros((sc.n_points, 3))
         check(_lib().v3dba_batch_get_params(self.h, i, _d(R), _d(T), _d(X)), "v3dba_batch_get_params")
         return R, T, X
+
+
+def concat_problems(scenes):
+    """The flat arrays v3dba_batch_create_flat takes, for a list of StdMetricBundleOptimizer scenes:
+    per-problem counts and thresholds, and every problem's K, R, T, X, measurements, view and
+    point one after another (indices local to each problem)."""
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+    return {
+        "n_cams": i32([sc.n_cams for sc in scenes]), "n_points": i32([sc.n_points for sc in scenes]),
+        "n_obs": i32([sc.n_obs for sc in scenes]),
+        "thr": _f64([sc.inlier_threshold for sc in scenes]),
+        "K": _f64(np.concatenate([np.reshape(sc.K, (-1, 3, 3)) for sc in scenes])),
+        "R": _f64(np.concatenate([sc.R for sc in scenes])), "T": _f64(np.concatenate([sc.T for sc in scenes])),
+        "X": _f64(np.concatenate([sc.X for sc in scenes])), "meas": _f64(np.concatenate([sc.meas for sc in scenes])),
+        "view": i32(np.concatenate([sc.view for sc in scenes])),
+        "point": i32(np.concatenate([sc.point for sc in scenes])),
+    }
 
 
 def _f32p(a):

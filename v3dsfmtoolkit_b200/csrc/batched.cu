@@ -704,6 +704,40 @@ int v3dba_batch_create(const v3dba_problem* problems, int count, v3dba_batch_t* 
   return V3DBA_OK;
 }
 
+int v3dba_batch_create_flat(int count, const int* n_cameras, const int* n_points, const int* n_measurements,
+                            const double* inlier_threshold, const double* K, const double* R, const double* T,
+                            const double* X, const double* measurements, const int* view, const int* point,
+                            v3dba_batch_t* out) {
+  if (count <= 0 || !n_cameras || !n_points || !n_measurements || !inlier_threshold || !K || !R || !T || !out)
+    return V3DBA_ERR_INVALID_ARGUMENT;
+  std::vector<v3dba_problem> probs((size_t)count);
+  size_t co = 0, po = 0, oo = 0;
+  for (int p = 0; p < count; ++p) {
+    if (n_cameras[p] < 0 || n_points[p] < 0 || n_measurements[p] < 0) return V3DBA_ERR_INVALID_ARGUMENT;
+    if ((n_points[p] && !X) || (n_measurements[p] && (!measurements || !view || !point)))
+      return V3DBA_ERR_INVALID_ARGUMENT;
+    v3dba_problem q;
+    std::memset(&q, 0, sizeof(q));
+    q.model = V3DBA_MODEL_STD;
+    q.n_cameras = n_cameras[p];
+    q.n_points = n_points[p];
+    q.n_measurements = n_measurements[p];
+    q.inlier_threshold = inlier_threshold[p];
+    q.K = K + 9 * co;
+    q.R = R + 9 * co;
+    q.T = T + 3 * co;
+    q.X = X ? X + 3 * po : nullptr;
+    q.measurements = measurements ? measurements + 2 * oo : nullptr;
+    q.view = view ? view + oo : nullptr;
+    q.point = point ? point + oo : nullptr;
+    probs[p] = q;
+    co += (size_t)n_cameras[p];
+    po += (size_t)n_points[p];
+    oo += (size_t)n_measurements[p];
+  }
+  return v3dba_batch_create(probs.data(), count, out);
+}
+
 int v3dba_batch_destroy(v3dba_batch_t h) {
   if (!h) return V3DBA_ERR_INVALID_ARGUMENT;
   batch_free(h);
