@@ -218,6 +218,20 @@ int v3dba_dims(int model, int mode, int* dA, int* dC);
  * host memory).  Returns V3DBA_OK and *fail = 1 when a pivot is not positive. */
 int v3dba_dense_cholesky_solve(int n, const double* S, const double* rhs, double* x, int* fail);
 
+/* Benchmark support (no counterpart in the reference): the same tile Cholesky factor + solve
+ * timed alone on the GPU, `reps` times from the same input; *ms receives the mean device time of
+ * one factor + solve (CUDA events), x and *fail the result.  trace (may be NULL, up to trace_cap
+ * entries) receives the level kernel's phase timestamps of the last repetition ((2 * levels + 2)
+ * slots per cluster rank, nanoseconds), *trace_len how many, *ranks the cluster size (0 when the
+ * column kernel ran).  V3DBA_CHOL_SCHEDULE=levels|steps forces either kernel. */
+int v3dba_dense_cholesky_profile(int n, const double* S, const double* rhs, int reps, double* ms, double* x,
+                                 int* fail, unsigned long long* trace, int trace_cap, int* trace_len, int* ranks);
+
+/* Accuracy check support (no counterpart in the reference): evaluates on the GPU, for each of
+ * the n positive x (host array), the refined reciprocal square root the tile Cholesky takes of
+ * its pivots, beside CUDA's rsqrt(x): out[2 i] = refined, out[2 i + 1] = rsqrt(x). */
+int v3dba_check_pivot_reciprocals(int n, const double* x, double* out);
+
 /* Dense SPD solve that allocates nothing (no counterpart in the reference).  For callers that
  * cannot allocate device memory where they solve: a loop that reserved its GPU memory up front
  * and cannot afford cudaMalloc's implicit device synchronisation, or a host framework that owns

@@ -30,7 +30,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TAU_STEP = 1e-12
-PREFIX_ITERATIONS = 20   # iterations over which both implementations take the same LM decisions
+PREFIX_ITERATIONS = 40   # iterations over which both implementations take the same LM decisions
 
 
 def _reference_run(args):

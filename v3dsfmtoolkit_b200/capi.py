@@ -45,7 +45,7 @@ EXPORTS = (
     "v3dba_rotations_set", "v3dba_rotations_reset", "v3dba_rotations_cost", "v3dba_rotations_set_group",
     "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
     "v3dba_triplet_stage_flat", "v3dba_cholesky_schedule", "v3dba_tile_schedule", "v3dba_debug_fail_allocation",
-    "v3dba_batch_create_flat",
+    "v3dba_batch_create_flat", "v3dba_dense_cholesky_profile", "v3dba_check_pivot_reciprocals",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -125,6 +125,10 @@ def _lib():
         L.v3dba_reduced_system.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
         L.v3dba_dims.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.v3dba_dense_cholesky_solve.argtypes = [C.c_int, _dp, _dp, _dp, C.POINTER(C.c_int)]
+        L.v3dba_check_pivot_reciprocals.argtypes = [C.c_int, _dp, _dp]
+        L.v3dba_dense_cholesky_profile.argtypes = [C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.POINTER(C.c_int),
+                                                   C.POINTER(C.c_uint64), C.c_int, C.POINTER(C.c_int),
+                                                   C.POINTER(C.c_int)]
         L.v3dba_minimize_batched.argtypes = [C.POINTER(Problem), C.c_int, C.POINTER(Options)] + \
             [C.POINTER(_dp)] * 5 + [C.POINTER(Result)]
         L.v3dba_profile_stages.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
@@ -394,6 +398,28 @@ def tile_schedule(pattern, ranks=16):
                 est_steps_us=float(est[1]), plan=plan)
 
 
+def check_pivot_reciprocals(x):
+    """(n, 2) array: the tile Cholesky's refined 1/sqrt(x) and CUDA's rsqrt(x), on the GPU."""
+    x = _f64(x)
+    out = np.zeros((x.size, 2))
+    check(_lib().v3dba_check_pivot_reciprocals(x.size, _d(x), _d(out)), "v3dba_check_pivot_reciprocals")
+    return out
+
+
+def dense_cholesky_profile(S, rhs, reps=20, trace_cap=4096):
+    """(x, fail, ms per factor + solve, trace (levels, ranks) array or None) of the tile Cholesky
+    timed alone on the GPU (v3dba_dense_cholesky_profile)."""
+    S, rhs = _f64(S), _f64(rhs)
+    x, fail, ms = np.zeros(S.shape[0]), C.c_int(), C.c_double()
+    tr = np.zeros(trace_cap, dtype=np.uint64)
+    tl, rk = C.c_int(), C.c_int()
+    check(_lib().v3dba_dense_cholesky_profile(S.shape[0], _d(S), _d(rhs), reps, C.byref(ms), _d(x), C.byref(fail),
+                                              tr.ctypes.data_as(C.POINTER(C.c_uint64)), trace_cap, C.byref(tl),
+                                              C.byref(rk)), "v3dba_dense_cholesky_profile")
+    trace = tr[:tl.value].reshape(-1, rk.value) if rk.value and tl.value else None
+    return x, bool(fail.value), ms.value, trace
+
+
 def dense_cholesky_solve(S, rhs):
     S = _f64(S)
     rhs = _f64(rhs)
@@ -656,8 +682,11 @@ class Batch:
         return a.value, b.value, c.value
 
     def get_params(self, i):
-        sc = self.scenes[i]
-        R, T, X = np.zeros((sc.n_cams, 3, 3)), np.zeros((sc.n_cams, 3)), np.zeros((sc.n_points, 3))
+        if self.scenes is not None:
+            nc, npt = self.scenes[i].n_cams, self.scenes[i].n_points
+        else:
+            nc, npt = int(self.flat["n_cams"][i]), int(self.flat["n_points"][i])
+        R, T, X = np.zeros((nc, 3, 3)), np.zeros((nc, 3)), np.zeros((npt, 3))
         check(_lib().v3dba_batch_get_params(self.h, i, _d(R), _d(T), _d(X)), "v3dba_batch_get_params")
         return R, T, X
 

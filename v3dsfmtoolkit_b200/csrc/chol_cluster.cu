@@ -8,14 +8,14 @@
 //   k_chol_cluster (8 CTAs) goes column by column in the caller's order;
 //   k_chol_levels (16 CTAs where the device allows, else 8) runs the level schedule of
 //   chol_order.cu, the independent columns of an elimination-tree level side by side.
-// Both use the same diagonal tile factor (cta_factor_tile).
+// Both use the same diagonal tile factor (cta_factor_tile8).
 //
 // k_chol_cluster: per tile column k, CTA 0 owns the chain along the diagonal and keeps it in
 // shared memory:
 //   with Z_k = L_kk^-1 resident it forms the panel tile next to the diagonal,
 //   L_{k+1,k} = A_{k+1,k} Z_k^T, publishes it (split cluster barrier: arrive, keep working), applies
-//   it to the next diagonal tile (fetched meanwhile) and factors that tile: 16-column blocking,
-//   each 16x16 diagonal block factored and inverted by one warp in registers, panels and trailing
+//   it to the next diagonal tile (fetched meanwhile) and factors that tile: 8-column blocking,
+//   each 8x8 diagonal block factored and inverted by one warp in registers, panels and trailing
 //   blocks updated with FP64 tensor-core MMAs (DMMA m8n8k4), Z_{k+1} assembled;
 //   CTAs 1.. form the other panel tiles (and the rhs row), L_rk = A_rk Z_k^T, one 64x64x64 DMMA
 //   GEMM per tile, then the other trailing tiles, A_rc -= L_rk L_ck^T (DMMA).
@@ -84,158 +84,155 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
   return y;
 }
 
-// 1/x for a positive pivot: the hardware approximation (rcp.approx.ftz.f64) refined by two
-// Newton-Raphson steps for the reciprocal, y <- y + y (1 - x y), each of which roughly doubles
-// the number of correct bits (two dependent FMAs per step).
-__device__ __forceinline__ double rcp_nr(double x) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  return y;
+// ---- 8-column blocking -----------------------------------------------------------------------
+
+// acc(8x8 block of one warp) += sum_t A(m,t) B(t,n), t in [0,K), A(m,t) = A[m*ars + t*acs],
+// B(t,n) = B[t*bks + n*bns]; acc[i] is element (g, 2q + i), g = lane/4, q = lane%4.
+__device__ __forceinline__ void warp_mma8(double (&acc)[2], const double* A, int ars, int acs, const double* B,
+                                          int bks, int bns, int K) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  for (int s = 0; s < K / 4; ++s) {
+    const int t = 4 * s + q;
+    dmma(acc[0], acc[1], A[g * ars + t * acs], B[t * bks + g * bns]);
+  }
 }
 
-// One warp: Cholesky of the 16x16 block D (lower, col-major ld LDT) in place and its inverse
-// into Z (16x16, col-major, zero upper part).  Returns false on a non-positive pivot.
-// Gaussian elimination in registers, both halves of the warp running the same instructions:
-// lane c < 16 holds column c of the symmetric trailing matrix (both triangles), lane 16 + c
-// column c of W, which starts as the identity and receives the same row operations.  At pivot j
-// the pivot column (lane j) is broadcast with shuffles and every lane applies
-// v[r] -= A[r][j] (v[j] / A[j][j]) for r > j (lanes c <= j of the first half are done).  Then
-// A = U D U^T with U unit lower (column c of U D is lane c's column at its pivot), W = U^-1, and
-// L = U D^1/2, L^-1 = D^-1/2 W.  Only a reciprocal of the pivot is on the chain from one pivot
-// to the next; the square roots are taken once at the end.
-__device__ __noinline__ bool warp_chol_inv16(double* D, double* Z) {
-  const int lane = threadIdx.x & 31;
-  const int c = lane & 15;
-  const bool a_half = lane < 16;
-  double v[16];
+// C(8x8 at C, col-major ldc) = alpha * acc + beta * C
+__device__ __forceinline__ void acc_store8(const double (&acc)[2], double* C, int ldc, double alpha, double beta) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
 #pragma unroll
-  for (int r = 0; r < 16; ++r)
-    v[r] = a_half ? (r >= c ? D[c * LDT + r] : D[r * LDT + c]) : (r == c ? 1.0 : 0.0);
-  __shared__ double rs_all[8][16];   // per warp: 1/sqrt of the pivots
-  double* rs = rs_all[threadIdx.x >> 5];
+  for (int i = 0; i < 2; ++i) {
+    double* p = C + (2 * q + i) * ldc + g;
+    *p = alpha * acc[i] + (beta != 0.0 ? beta * *p : 0.0);
+  }
+}
+
+// Packed position of element (r, c), r >= c, of an 8x8 lower triangle stored column by column.
+__host__ __device__ constexpr int pk8(int r, int c) { return c * 8 - (c * (c - 1)) / 2 + (r - c); }
+
+// One warp: Z = L^-1 for the Cholesky factor L of the 8x8 SPD block D (lower triangle read,
+// col-major LDT), written to the lower triangle of Zd (the caller zeroes its upper part).  Every
+// lane computes the whole factor and inverse in registers from the same broadcast reads: no
+// shuffles and no lane waits for another, so the chain from one pivot to the next is one
+// reciprocal square root and two dependent FMAs.  Returns false on a non-positive pivot.
+__device__ __noinline__ bool warp_chol_inv8(const double* D, double* Zd) {
+  double a[36];
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+#pragma unroll
+    for (int r = c; r < 8; ++r) a[pk8(r, c)] = D[c * LDT + r];
   bool ok = true;
-  double piv = 1.0;   // this lane's column's pivot
+  double s[8];
+  // right-looking Cholesky, L over a
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    const double d = __shfl_sync(FULL, v[j], j);
+  for (int j = 0; j < 8; ++j) {
+    const double d = a[pk8(j, j)];
     if (!(d > 0.0)) ok = false;
-    if (c == j) piv = d;
-    const double m = v[j] * rcp_nr(d > 0.0 ? d : 1.0);
-    const bool upd = !a_half || c > j;
+    const double sj = rsqrt_nr(d > 0.0 ? d : 1.0);
+    s[j] = sj;
 #pragma unroll
-    for (int r = j + 1; r < 16; ++r) {
-      const double col = __shfl_sync(FULL, v[r], j);
-      if (upd) v[r] = fma(-col, m, v[r]);
+    for (int r = j + 1; r < 8; ++r) a[pk8(r, j)] *= sj;
+#pragma unroll
+    for (int c = j + 1; c < 8; ++c)
+#pragma unroll
+      for (int r = c; r < 8; ++r) a[pk8(r, c)] = fma(-a[pk8(r, j)], a[pk8(c, j)], a[pk8(r, c)]);
+  }
+  // Z = L^-1: Z_cc = 1 / L_cc = s_c, Z_rc = -s_r sum_{t=c}^{r-1} L_rt Z_tc
+  double z[36];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    z[pk8(c, c)] = s[c];
+#pragma unroll
+    for (int r = c + 1; r < 8; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int t = c; t < r; ++t) acc = fma(a[pk8(r, t)], z[pk8(t, c)], acc);
+      z[pk8(r, c)] = -acc * s[r];
     }
   }
-  const double sc = rsqrt_nr(piv > 0.0 ? piv : 1.0);
-  if (a_half) rs[c] = sc;
-  __syncwarp();
-  if (a_half) {
+  if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) D[c * LDT + r] = r >= c ? v[r] * sc : 0.0;
-  } else {
+    for (int c = 0; c < 8; ++c)
 #pragma unroll
-    for (int r = 0; r < 16; ++r) Z[c * LDT + r] = r >= c ? v[r] * rs[r] : 0.0;
+      for (int r = c; r < 8; ++r) Zd[c * LDT + r] = z[pk8(r, c)];
   }
   __syncwarp();
   return ok;
 }
 
-// C(16x16 at C, col-major ldc) = alpha * acc + beta * C
-__device__ __forceinline__ void acc_store(const double (&acc)[2][2][2], double* C, int ldc, double alpha, double beta) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b)
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        double* p = C + (8 * b + 2 * q + i) * ldc + 8 * a + g;
-        *p = alpha * acc[a][b][i] + (beta != 0.0 ? beta * *p : 0.0);
-      }
-}
-
-// CTA (256 threads): factor the 64x64 tile A (shared, col-major LDT, lower triangle valid) in
-// place and write Z = L^-1 (full 64x64, zero upper part) into Zs.  Blocked by 16 columns with
-// lookahead: warp 0 carries the chain of diagonal blocks (update of the next diagonal block by
-// the panel just formed, then its factor and inverse, warp_chol_inv16) while warps 1..7 apply the
-// other trailing updates (A_ij -= L_ip L_jp^T) and form block row p of Z
-// (Z_pj = -Z_pp sum_{t=j}^{p-1} L_pt Z_tj); the panel blocks L_ip = A_ip Z_pp^T are formed by
-// the first warps between.  All products are 16x16 DMMA tiles.  Returns false on a non-positive
-// pivot.  (The upper blocks of Zs are zeroed before the first block is factored, not beside it:
-// on B200 the first block factor ran an order of magnitude slower with the zeroing stores of the
-// other warps alongside.)
-__device__ bool cta_factor_tile(double* A, double* Zs) {
+// CTA (256 threads): Z = L^-1 (full 64x64, zero upper part) into Zs for the Cholesky factor L of
+// the 64x64 tile A (shared, col-major LDT, lower triangle valid; A is overwritten).  Blocked by
+// 8 columns with lookahead: warp 0 carries the chain of diagonal blocks (the update of the next
+// diagonal block by the panel just formed, then its inverse factor, warp_chol_inv8) while warps
+// 1..7 apply the other trailing updates (A_ij -= L_ip L_jp^T) and form block row p of Z
+// (Z_pj = -Z_pp sum_{t=j}^{p-1} L_pt Z_tj); the panel blocks L_ip = A_ip Z_pp^T are formed by the
+// first warps between.  All products are 8x8 DMMA blocks.  Returns false on a non-positive pivot.
+__device__ bool cta_factor_tile8(double* A, double* Zs) {
   const int tid = threadIdx.x, w = tid >> 5;
-  __shared__ int s_ok;
-  if (tid == 0) s_ok = 1;
-  for (int e = tid; e < 6 * 256; e += blockDim.x) {   // the strictly upper blocks (bi < bj)
-    const int b = e >> 8, q = e & 255;
-    const int bi = b < 3 ? 0 : b < 5 ? 1 : 2;
-    const int bj = b < 3 ? 1 + b : b < 5 ? b - 1 : 3;
-    Zs[(16 * bj + (q >> 4)) * LDT + 16 * bi + (q & 15)] = 0.0;
+  __shared__ int s_ok8;
+  if (tid == 0) s_ok8 = 1;
+  // the upper part of Z: column c is zeroed from row 0 to the end of its diagonal block with
+  // 16-byte stores (the lower entries of the diagonal block are written by its factor later)
+  for (int c = tid >> 2; c < TB; c += blockDim.x >> 2) {
+    double2* col = reinterpret_cast<double2*>(Zs + c * LDT);
+    for (int r2 = tid & 3; r2 < 4 * (c >> 3) + 4; r2 += 4) col[r2] = make_double2(0.0, 0.0);
   }
   __syncthreads();
-  if (w == 0 && !warp_chol_inv16(A, Zs) && (tid & 31) == 0) s_ok = 0;
+  if (w == 0 && !warp_chol_inv8(A, Zs) && (tid & 31) == 0) s_ok8 = 0;
   __syncthreads();
-  for (int p = 0; p < 4; ++p) {
-    if (p < 3) {
-      if (w < 3 - p) {   // panel blocks L_ip = A_ip Z_pp^T
+  for (int p = 0; p < 8; ++p) {
+    const double* Zpp = Zs + 8 * p * LDT + 8 * p;
+    if (p < 7) {
+      if (w < 7 - p) {   // panel blocks L_ip = A_ip Z_pp^T
         const int i = p + 1 + w;
-        double acc[2][2][2];
-        acc_zero(acc);
-        warp_mma16(acc, A + 16 * p * LDT + 16 * i, 1, LDT, Zs + 16 * p * LDT + 16 * p, LDT, 1, 16);
+        double acc[2] = {0.0, 0.0};
+        warp_mma8(acc, A + 8 * p * LDT + 8 * i, 1, LDT, Zpp, LDT, 1, 8);
         __syncwarp();
-        acc_store(acc, A + 16 * p * LDT + 16 * i, LDT, 1.0, 0.0);
+        acc_store8(acc, A + 8 * p * LDT + 8 * i, LDT, 1.0, 0.0);
       }
       __syncthreads();
     }
     if (w == 0) {
-      if (p < 3) {   // the next diagonal block: A_qq -= L_qp L_qp^T, then its factor and inverse
+      if (p < 7) {   // the next diagonal block: A_qq -= L_qp L_qp^T, then its inverse factor
         const int q1 = p + 1;
-        double acc[2][2][2];
-        acc_zero(acc);
-        warp_mma16(acc, A + 16 * p * LDT + 16 * q1, 1, LDT, A + 16 * p * LDT + 16 * q1, LDT, 1, 16);
-        acc_store(acc, A + 16 * q1 * LDT + 16 * q1, LDT, -1.0, 1.0);
+        double acc[2] = {0.0, 0.0};
+        warp_mma8(acc, A + 8 * p * LDT + 8 * q1, 1, LDT, A + 8 * p * LDT + 8 * q1, LDT, 1, 8);
+        acc_store8(acc, A + 8 * q1 * LDT + 8 * q1, LDT, -1.0, 1.0);
         __syncwarp();
-        if (!warp_chol_inv16(A + 16 * q1 * LDT + 16 * q1, Zs + 16 * q1 * LDT + 16 * q1) && (tid & 31) == 0)
-          s_ok = 0;
+        if (!warp_chol_inv8(A + 8 * q1 * LDT + 8 * q1, Zs + 8 * q1 * LDT + 8 * q1) && (tid & 31) == 0) s_ok8 = 0;
       }
     } else {
-      int task = 0;
-      for (int i = p + 1; i < 4; ++i)
-        for (int j = p + 1; j <= i; ++j) {
-          if (i == p + 1 && j == p + 1) continue;
-          if (task++ % 7 != w - 1) continue;
-          double acc[2][2][2];
-          acc_zero(acc);
-          warp_mma16(acc, A + 16 * p * LDT + 16 * i, 1, LDT, A + 16 * p * LDT + 16 * j, LDT, 1, 16);
-          acc_store(acc, A + 16 * j * LDT + 16 * i, LDT, -1.0, 1.0);
-        }
-      for (int j = 0; j < p; ++j) {
-        if (task++ % 7 != w - 1) continue;
-        double acc[2][2][2];
-        acc_zero(acc);
+      // Tasks of this iteration, dealt to warps 1..7 in turn: first the trailing blocks (i, j),
+      // p+1 <= j <= i < 8, other than (p+1, p+1) (the lower triangle of the trailing block matrix
+      // numbered row by row: u -> (ii, jj), ii(ii+1)/2 <= u < (ii+1)(ii+2)/2), then block row p of
+      // Z.  Each warp steps straight to its own tasks.
+      const int m = 7 - p;
+      const int n_upd = m * (m + 1) / 2 - 1;
+      for (int k = w - 1; k < n_upd; k += 7) {
+        const int u = k + 1;
+        int ii = 0;
+        while ((ii + 1) * (ii + 2) / 2 <= u) ++ii;
+        const int i = p + 1 + ii, j = p + 1 + (u - ii * (ii + 1) / 2);
+        double acc[2] = {0.0, 0.0};
+        warp_mma8(acc, A + 8 * p * LDT + 8 * i, 1, LDT, A + 8 * p * LDT + 8 * j, LDT, 1, 8);
+        acc_store8(acc, A + 8 * j * LDT + 8 * i, LDT, -1.0, 1.0);
+      }
+      for (int j = ((w - 1 - n_upd) % 7 + 7) % 7; j < p; j += 7) {
+        double acc[2] = {0.0, 0.0};
         for (int t = j; t < p; ++t)
-          warp_mma16(acc, A + 16 * t * LDT + 16 * p, 1, LDT, Zs + 16 * j * LDT + 16 * t, 1, LDT, 16);
-        double* Wpj = Zs + 16 * j * LDT + 16 * p;   // the block itself holds W = sum L Z meanwhile
-        acc_store(acc, Wpj, LDT, 1.0, 0.0);
+          warp_mma8(acc, A + 8 * t * LDT + 8 * p, 1, LDT, Zs + 8 * j * LDT + 8 * t, 1, LDT, 8);
+        double* Wpj = Zs + 8 * j * LDT + 8 * p;   // the block itself holds W = sum L Z meanwhile
+        acc_store8(acc, Wpj, LDT, 1.0, 0.0);
         __syncwarp();
-        double acc2[2][2][2];
-        acc_zero(acc2);
-        warp_mma16(acc2, Zs + 16 * p * LDT + 16 * p, 1, LDT, Wpj, 1, LDT, 16);
+        double acc2[2] = {0.0, 0.0};
+        warp_mma8(acc2, Zpp, 1, LDT, Wpj, 1, LDT, 8);
         __syncwarp();
-        acc_store(acc2, Wpj, LDT, -1.0, 0.0);
+        acc_store8(acc2, Wpj, LDT, -1.0, 0.0);
       }
     }
     __syncthreads();
   }
-  return s_ok != 0;
+  return s_ok8 != 0;
 }
 
 // CTA: C(64x64) = A B^T for shared tiles A, B (col-major LDT); the result stays in the warps'
@@ -325,7 +322,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(256)
   // global (for the other CTAs' panels and the back-substitution)
   auto factor_resident = [&](int k) {
     __syncthreads();
-    const bool ok = cta_factor_tile(T2, T1);
+    const bool ok = cta_factor_tile8(T2, T1);
     if (!ok && tid == 0) atomicExch(fail, 1);
     double* Z = ldiag + (size_t)k * TB * TB;
     for (int e = tid; e < TB * TB; e += blockDim.x) Z[e] = T1[(e >> 6) * LDT + (e & 63)];
@@ -613,7 +610,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
               for (int i = 0; i < 2; ++i) T2[frag_col(h, b, i) * LDT + frag_row(a)] -= acc[h][a][b][i];
         __syncthreads();
-        const bool ok = cta_factor_tile(T2, T1);
+        const bool ok = cta_factor_tile8(T2, T1);
         if (!ok && tid == 0) atomicExch(fail, 1);
         double* Z = ldiag + (size_t)j * TB * TB;
         for (int f = tid; f < TB * TB; f += blockDim.x) Z[f] = T1[(f >> 6) * LDT + (f & 63)];
@@ -726,6 +723,16 @@ __global__ void __launch_bounds__(256)
   stamp(2 * P.n_levels + 1);
 }
 
+// Accuracy check of the pivot reciprocal square root (tests): out[2 i] = rsqrt_nr(x_i),
+// out[2 i + 1] = rsqrt(x_i) (CUDA's), both evaluated on the device.
+__global__ void k_recip_check(const double* __restrict__ x, int n, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = x[i];
+  out[2 * i] = rsqrt_nr(v);
+  out[2 * i + 1] = rsqrt(v);
+}
+
 // Function attributes are set once per device (a process may drive several GPUs).
 int chol_cluster_setup() {
   static std::atomic<uint64_t> done_mask{0};
@@ -829,3 +836,22 @@ int chol_levels_ranks() {
 }
 
 }  // namespace v3dba
+
+extern "C" int v3dba_check_pivot_reciprocals(int n, const double* x, double* out) {
+  if (n <= 0 || !x || !out) return V3DBA_ERR_INVALID_ARGUMENT;
+  double *dx = nullptr, *dout = nullptr;
+  V3DBA_CUDA_TRY(cudaMalloc(&dx, sizeof(double) * n));
+  if (cudaMalloc(&dout, sizeof(double) * 2 * n) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(dx);
+    return V3DBA_ERR_OUT_OF_MEMORY;
+  }
+  cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  v3dba::k_recip_check<<<(n + 255) / 256, 256>>>(dx, n, dout);
+  v3dba::note_launches(1);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  cudaFree(dout);
+  return e == cudaSuccess ? V3DBA_OK : V3DBA_ERR_CUDA;
+}

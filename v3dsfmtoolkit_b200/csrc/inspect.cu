@@ -206,6 +206,77 @@ extern "C" int v3dba_dense_cholesky_solve(int n, const double* S, const double* 
   return rc;
 }
 
+// Benchmark support: the tile Cholesky factor + solve of one dense SPD system (row-major, host),
+// timed alone.  The system is uploaded once; every repetition restores the factorised matrix
+// from that copy (not timed) and times one solve with CUDA events on the launching stream.
+// trace (host, may be NULL): the phase timestamps (globaltimer, ns) of the last repetition of
+// the level kernel, (2 * n_levels + 2) slots per cluster rank, slot-major; *trace_len receives
+// the number written (0 when the column kernel ran).
+extern "C" int v3dba_dense_cholesky_profile(int n, const double* S, const double* rhs, int reps, double* ms,
+                                            double* x, int* fail, unsigned long long* trace, int trace_cap,
+                                            int* trace_len, int* ranks) {
+  if (n <= 0 || !S || !rhs || reps <= 0 || !ms || !x || !fail) return V3DBA_ERR_INVALID_ARGUMENT;
+  TileChol tc;
+  const int nt = (n + TileChol::TB - 1) / TileChol::TB;
+  std::vector<uint8_t> nz((size_t)nt * nt, 0);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c <= r; ++c)
+      if (S[(size_t)r * n + c] != 0.0) nz[(size_t)(r / 64) * nt + c / 64] = 1;
+  int rc = tile_chol_plan(tc, n, nz);
+  if (rc) { tile_chol_free(tc); return rc; }
+  std::vector<double> full((size_t)tc.ld * tc.n_pad, 0.0);
+  for (int c = 0; c < n; ++c) {
+    for (int r = c; r < n; ++r) full[(size_t)c * tc.ld + r] = S[(size_t)r * n + c];
+    full[(size_t)c * tc.ld + tc.n_pad] = rhs[c];
+  }
+  for (int d = n; d < tc.n_pad; ++d) full[(size_t)d * tc.ld + d] = 1.0;
+  const size_t slots = tc.levels ? (size_t)(2 * tc.n_levels + 2) * tc.lv_ranks : 0;
+  DevBuf d0, dS, dx, df, dt;
+  if ((rc = d0.alloc<double>(full.size())) || (rc = dS.alloc<double>(full.size())) ||
+      (rc = dx.alloc<double>(tc.n_pad)) || (rc = df.alloc<int>(1)) ||
+      (rc = dt.alloc<unsigned long long>(std::max<size_t>(slots, 1)))) {
+    tile_chol_free(tc);
+    return rc;
+  }
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    tile_chol_free(tc);
+    return V3DBA_ERR_CUDA;
+  }
+  cudaMemcpy(d0.p, full.data(), sizeof(double) * full.size(), cudaMemcpyHostToDevice);
+  double total = 0.0;
+  for (int r = 0; r < reps && rc == V3DBA_OK; ++r) {
+    cudaMemcpyAsync(dS.p, d0.p, sizeof(double) * full.size(), cudaMemcpyDeviceToDevice, st);
+    cudaMemsetAsync(df.p, 0, sizeof(int), st);
+    cudaEventRecord(e0, st);
+    rc = tc.levels ? chol_levels_solve(tc, dS.as<double>(), dx.as<double>(), df.as<int>(), st,
+                                       r == reps - 1 ? dt.as<unsigned long long>() : nullptr)
+                   : tile_chol_solve(tc, dS.as<double>(), dx.as<double>(), df.as<int>(), st);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) rc = V3DBA_ERR_CUDA;
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    total += t;
+  }
+  if (rc == V3DBA_OK) {
+    *ms = total / reps;
+    cudaMemcpy(x, dx.p, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(fail, df.p, sizeof(int), cudaMemcpyDeviceToHost);
+    const size_t w = trace ? std::min<size_t>(slots, (size_t)std::max(trace_cap, 0)) : 0;
+    if (w) cudaMemcpy(trace, dt.p, sizeof(unsigned long long) * w, cudaMemcpyDeviceToHost);
+    if (trace_len) *trace_len = (int)w;
+    if (ranks) *ranks = tc.levels ? tc.lv_ranks : 0;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  tile_chol_free(tc);
+  return rc;
+}
+
 // The structure built by v3dba_create: sizes always; every array pointer that is not NULL
 // receives its array (o_orig, c_ptr, c_obs [K], [N+1], [K]; b_i, b_l [nb], b_ptr [nb+1];
 // pr_k, pr_m [P]).
