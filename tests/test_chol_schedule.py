@@ -168,7 +168,9 @@ def test_plan_is_deterministic_and_tasks_are_disjoint(name, pat, monkeypatch):
         assert len(ptr) == s1["n_levels"] * RANKS + 1 and ptr[-1] == len(ids)
         assert len(set(ids.tolist())) == len(ids)      # a task is in one phase list once
     # the level of a column is where its diagonal tile is factored; phase 1 of level L applies
-    # the updates of level L-1's columns only, phase 2 of level L forms level L's panels only
+    # updates of columns of earlier levels only (formed by then) to tiles whose column is not yet
+    # factored, each target tile in at most one task per phase; phase 2 of level L forms level L's
+    # panels only
     lvl = {}
     for lv in range(s1["n_levels"]):
         for e in range(P["p1ptr"][lv * RANKS], P["p1ptr"][(lv + 1) * RANKS]):
@@ -179,8 +181,11 @@ def test_plan_is_deterministic_and_tasks_are_disjoint(name, pat, monkeypatch):
         for e in range(P["p1ptr"][lv * RANKS], P["p1ptr"][(lv + 1) * RANKS]):
             t = P["p1"][e]
             for u in range(P["task_cptr"][t], P["task_cptr"][t + 1]):
-                assert lvl[P["ck"][u]] == lv - 1
+                assert lvl[P["ck"][u]] <= lv - 1
             assert lvl[P["task_c"][t]] >= lv
+        targets = [(P["task_r"][P["p1"][e]], P["task_c"][P["p1"][e]])
+                   for e in range(P["p1ptr"][lv * RANKS], P["p1ptr"][(lv + 1) * RANKS])]
+        assert len(set(targets)) == len(targets)
         for e in range(P["p2ptr"][lv * RANKS], P["p2ptr"][(lv + 1) * RANKS]):
             t = P["p2"][e]
             assert lvl[P["task_c"][t]] == lv and P["task_cptr"][t + 1] == P["task_cptr"][t]

@@ -21,8 +21,10 @@
 // factorisation; this one minimises the height of the elimination tree (the critical path on a
 // parallel machine) rather than the fill.
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <iterator>
 #include <map>
 #include <vector>
 
@@ -38,6 +40,10 @@ namespace {
 constexpr double kGemmUs = 2.0, kFactorUs = 20.0, kBarrierUs = 1.0, kStoreUs = 0.5;
 // the same for one update or solve of the rhs row (a GEMV over one tile)
 constexpr double kGemvUs = 0.6;
+// Measured on B200 (sequence200 pattern, per CTA): one tile update with its operand loads, the
+// factor of a diagonal tile, the load + store of an updated tile.  They size the phase budget
+// into which updates that are not yet due are moved.
+constexpr double kMeasGemmUs = 3.5, kMeasFactorUs = 9.0, kMeasTileUs = 1.5, kMeasGemvUs = 1.0;
 
 struct TileGraph {
   int nt = 0;
@@ -196,14 +202,18 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks)
     if (!colrows[k].empty()) level[colrows[k][0]] = std::max(level[colrows[k][0]], level[k] + 1);
     n_levels = std::max(n_levels, level[k] + 1);
   }
-  // Tasks.  Phase 1 of level L applies the updates of the columns of level L-1 (formed in the
-  // phase before) to every tile they reach, A_ab -= L_ak L_bk^T for rows a >= b of column k and
-  // the rhs row (one task per target tile, its columns k ascending), and factors the diagonal
-  // tiles of level L once their last updates are in.  Phase 2 of level L forms
-  // L_rj = A_rj Z_j^T for the off-diagonal tiles of level L's columns.  Applying the updates as
-  // soon as their column is formed (right-looking) spreads them over the levels instead of
-  // piling them onto the last ones.  A tile is read as assembled (mode 0/1/2) the first time it
-  // is touched and in place (mode 1) after that; kLvFactor marks the diagonal tasks that factor.
+  // Tasks.  An update A_ab -= L_ak L_bk^T (rows a >= b of column k, and the rhs row) can run in
+  // phase 1 of any level after column k's panels are formed (the phase 2 of level[k]) and must
+  // have run by phase 1 of level[b], where tile (a, b) is factored (a == b) or consumed by the
+  // panel product of phase 2 (a > b).  Phase 1 of level L takes, as one task per target tile
+  // (its columns k ascending), every pending update that is due at L, and factors the diagonal
+  // tiles of level L once their last updates are in; the CTAs are loaded by longest processing
+  // time first.  Updates not yet due then fill the CTAs up to that phase's longest load (earliest
+  // due first), and what does not fit waits for a later phase: the phase lasts no longer, and the
+  // later, narrower levels take work off the wide early ones.  Phase 2 of level L forms
+  // L_rj = A_rj Z_j^T for the off-diagonal tiles of level L's columns.  A tile is read as
+  // assembled (mode 0/1/2) the first time it is touched and in place (mode 1) after that;
+  // kLvFactor marks the diagonal tasks that factor.
   std::vector<int> t_r, t_c, t_mode, t_cptr(1, 0), c_k;
   std::vector<std::vector<int>> lv_cols(n_levels);
   for (int j = 0; j < nt; ++j) lv_cols[level[j]].push_back(j);
@@ -217,34 +227,82 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks)
   bool consistent = true;
   double est = 0.0, flops = 0.0;
   const double gemm = 2.0 * 64.0 * 64.0 * 64.0;
+  auto make_task = [&](int r, int c, const int* ks, int nk, bool factor) {
+    const int id = (int)t_r.size();
+    t_r.push_back(r);
+    t_c.push_back(c);
+    t_mode.push_back(input_mode(r, c) | (factor ? kLvFactor : 0));
+    touched[(size_t)r * nt + c] = 1;
+    for (int u = 0; u < nk; ++u) c_k.push_back(ks[u]);
+    t_cptr.push_back((int)c_k.size());
+    flops += (r == nt ? 2.0 * 64.0 * 64.0 : gemm) * nk + (factor ? 64.0 * 64.0 * 64.0 : 0.0);
+    return id;
+  };
+  std::map<std::pair<int, int>, std::vector<int>> pending;   // target (r, c) -> columns k not yet applied
   for (int lv = 0; lv < n_levels; ++lv) {
-    std::map<std::pair<int, int>, std::vector<int>> upd;   // target (r, c) -> columns k
     if (lv > 0)
       for (int k : lv_cols[lv - 1]) {
         std::vector<int> rows = colrows[k];
         rows.push_back(nt);
         for (size_t a = 0; a < rows.size(); ++a)
           for (size_t b = 0; b <= a; ++b)
-            if (rows[b] < nt) upd[{rows[a], rows[b]}].push_back(k);
+            if (rows[b] < nt) pending[{rows[a], rows[b]}].push_back(k);
       }
-    for (int j : lv_cols[lv]) upd[{j, j}];
+    for (int j : lv_cols[lv]) pending[{j, j}];
+    // the updates due at this level, one task per target
     std::vector<int> ph1, ph2;
-    std::vector<double> cost1, cost2;
-    for (auto& tk : upd) {
-      const int r = tk.first.first, c = tk.first.second;
-      const bool factor = r == c && level[c] == lv;
-      const int id = (int)t_r.size();
-      t_r.push_back(r);
-      t_c.push_back(c);
-      t_mode.push_back(input_mode(r, c) | (factor ? kLvFactor : 0));
-      touched[(size_t)r * nt + c] = 1;
-      for (int k : tk.second) c_k.push_back(k);
-      t_cptr.push_back((int)c_k.size());
-      const int nc = (int)tk.second.size();
-      flops += (r == nt ? 2.0 * 64.0 * 64.0 : gemm) * nc + (factor ? 64.0 * 64.0 * 64.0 : 0.0);
-      ph1.push_back(id);
+    std::vector<double> cost1, meas1, cost2;
+    for (auto it = pending.begin(); it != pending.end();) {
+      const int r = it->first.first, c = it->first.second;
+      if (level[c] != lv) {
+        ++it;
+        continue;
+      }
+      const bool factor = r == c;
+      const int nc = (int)it->second.size();
+      if (!factor && nc == 0) {   // all of its updates ran early
+        it = pending.erase(it);
+        continue;
+      }
+      ph1.push_back(make_task(r, c, it->second.data(), nc, factor));
       cost1.push_back(factor ? kFactorUs + kGemmUs * nc : (r == nt ? kGemvUs : kGemmUs) * nc + kStoreUs);
+      meas1.push_back(factor ? kMeasFactorUs + kMeasTileUs + kMeasGemmUs * nc
+                             : r == nt ? kMeasGemvUs * nc : kMeasGemmUs * nc + kMeasTileUs);
+      it = pending.erase(it);
     }
+    double m1 = 0.0, m2 = 0.0, mm = 0.0;
+    auto a1 = assign_lpt(ph1, cost1, ranks, &m1);
+    std::vector<double> load(ranks, 0.0);
+    {   // the loads of that assignment under the measured costs
+      std::vector<int> pos(t_r.size(), -1);
+      for (size_t i = 0; i < ph1.size(); ++i) pos[ph1[i]] = (int)i;
+      for (int r = 0; r < ranks; ++r)
+        for (int id : a1[r]) load[r] += meas1[pos[id]];
+      mm = *std::max_element(load.begin(), load.end());
+    }
+    // updates not yet due, earliest due first (then the target's order), into the slack below
+    // the phase's longest load
+    std::vector<std::pair<int, int>> opt;
+    for (auto& pd : pending)
+      if (!pd.second.empty()) opt.push_back(pd.first);
+    std::stable_sort(opt.begin(), opt.end(), [&](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+      return level[x.second] < level[y.second];
+    });
+    for (const auto& key : opt) {
+      std::vector<int>& ks = pending[key];
+      const int r = key.first, c = key.second;
+      const double g = r == nt ? kMeasGemvUs : kMeasGemmUs, fixed = r == nt ? 0.0 : kMeasTileUs;
+      int best = 0;
+      for (int q = 1; q < ranks; ++q)
+        if (load[q] < load[best]) best = q;
+      const int fit = (int)std::min<double>((double)ks.size(), std::floor((mm - load[best] - fixed) / g + 1e-9));
+      if (fit < 1) continue;
+      const int id = make_task(r, c, ks.data(), fit, false);
+      a1[best].push_back(id);
+      load[best] += fixed + g * fit;
+      ks.erase(ks.begin(), ks.begin() + fit);
+    }
+    for (auto it = pending.begin(); it != pending.end();) it = it->second.empty() ? pending.erase(it) : std::next(it);
     for (int j : lv_cols[lv]) {
       std::vector<int> rows = colrows[j];
       rows.push_back(nt);
@@ -262,8 +320,6 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks)
         cost2.push_back(r == nt ? kGemvUs : kGemmUs);
       }
     }
-    double m1 = 0.0, m2 = 0.0;
-    auto a1 = assign_lpt(ph1, cost1, ranks, &m1);
     auto a2 = assign_lpt(ph2, cost2, ranks, &m2);
     for (int r = 0; r < ranks; ++r) {
       p1.insert(p1.end(), a1[r].begin(), a1[r].end());
@@ -273,6 +329,8 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks)
     }
     est += m1 + m2 + 2.0 * kBarrierUs;
   }
+  for (const auto& pd : pending)
+    if (!pd.second.empty()) consistent = false;   // an update that was never due (cannot happen)
   std::vector<int> bptr(1, 0), brow;
   for (int k = 0; k < nt; ++k) {
     brow.insert(brow.end(), colrows[k].begin(), colrows[k].end());
