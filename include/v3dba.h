@@ -214,6 +214,37 @@ int v3dba_reduced_system(v3dba_handle h, int precision, double lambda, double* S
 /* Dimensions of a model / mode (dA camera block, dC global block). */
 int v3dba_dims(int model, int mode, int* dA, int* dC);
 
+/* ---- BundlePointStructure (V3D/include/Geometry/v3d_mviewutilities.h:132-205) -------------
+ * The flat bundle-adjustment inputs from a reconstruction, built on the GPU.  A reconstruction
+ * (vector<TriangulatedPoint>) is passed as tracks: track j (TriangulatedPoint j) has position
+ * track_pos[3 j .. 3 j + 2] and the measurements track_ptr[j] .. track_ptr[j + 1] - 1, each with
+ * meas_view, meas_id and the float image position meas_pos[2 m], [2 m + 1] (PointMeasurement).
+ *
+ * v3dba_bundle_point_structure replaces the constructor BundlePointStructure(reconstruction,
+ * nRequiredMeasurements) (h:136-158): the tracks with at least n_required measurements (a
+ * negative n_required keeps none, as the reference's size_t comparison does), in order, become
+ * points3d, their measurements (widened to double) measurements / measurement_ids /
+ * corresponding_view / corresponding_point, and xs_indices the kept tracks' indices.  The caller
+ * sizes the outputs for the maxima (n_tracks points, track_ptr[n_tracks] measurements; any may
+ * be NULL) and receives the counts in *n_points and *n_measurements. */
+int v3dba_bundle_point_structure(int n_tracks, const int* track_ptr, const double* track_pos, const int* meas_view,
+                                 const int* meas_id, const float* meas_pos, int n_required, int* n_points,
+                                 int* n_measurements, double* points3d, double* measurements, int* measurement_ids,
+                                 int* corresponding_view, int* corresponding_point, int* xs_indices);
+
+/* BundlePointStructure::createPointStructure(reconstruction, createFromScratch) (h:160-197).
+ * from_scratch != 0: the reconstruction becomes n_points tracks, track i at points3d[i] with the
+ * measurements whose corresponding_point is i, in their order (positions narrowed to float):
+ * track_ptr (n_points + 1), track_pos (3 n_points), meas_view / meas_id / meas_pos
+ * (n_measurements) are outputs and n_tracks is ignored.  from_scratch == 0: the n_tracks tracks
+ * keep their measurement lists (track_ptr is an input); track xs_indices[i] gets position
+ * points3d[i], and the measurements of the kept tracks, in order, get the positions
+ * measurements[...] one after another (meas_view, meas_id unused). */
+int v3dba_create_point_structure(int from_scratch, int n_points, int n_measurements, const double* points3d,
+                                 const double* measurements, const int* measurement_ids, const int* corresponding_view,
+                                 const int* corresponding_point, const int* xs_indices, int n_tracks, int* track_ptr,
+                                 double* track_pos, int* meas_view, int* meas_id, float* meas_pos);
+
 /* Standalone tile-sparse FP64 Cholesky solve on the GPU of a dense SPD system (row-major n x n,
  * host memory).  Returns V3DBA_OK and *fail = 1 when a pivot is not positive. */
 int v3dba_dense_cholesky_solve(int n, const double* S, const double* rhs, double* x, int* fail);

@@ -178,6 +178,15 @@ class Reference:
         return dict(verdict=v.value, n_points=ns.value, status=st.value, iterations=it.value, cost=cost.value,
                     R=Ro.reshape(3, 3, 3), T=To.reshape(3, 3), X=X[:3 * n].reshape(n, 3), kept=kept[:nm].copy())
 
+    def bundle_point_structure(self, tracks, n_required=2):
+        """The reference's BundlePointStructure(reconstruction, nRequiredMeasurements) on tracks
+        (dict: track_ptr, pos (n, 3), view, id, mpos (K, 2) float32); returns its flat arrays."""
+        return _bps_call(self.lib.v3dref_bundle_point_structure, tracks, n_required)
+
+    def create_point_structure(self, bps, from_scratch, tracks=None):
+        """The reference's BundlePointStructure::createPointStructure; returns the tracks."""
+        return _cps_call(self.lib.v3dref_create_point_structure, bps, from_scratch, tracks)
+
     def refine_rotations(self, graph, rotations=None, trace_cap=512):
         """V3D::refineConsistentRotations on a copy of the graph's initial rotations; returns
         (rotations (n, 3, 3), err per relinearization as printed by the reference)."""
@@ -186,6 +195,55 @@ class Reference:
         self.lib.v3dref_refine_rotations(graph.n_views, graph.n_pairs, _d(_f64(graph.rel)), _i(_i32(graph.pairs)),
                                          _d(R), _d(tr), trace_cap, C.byref(tlen))
         return R, tr[:min(tlen.value, trace_cap)].copy()
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+def _bps_call(fn, tracks, n_required):
+    """Calls a BundlePointStructure producer with the C signature of v3dba_bundle_point_structure
+    (the reference wrapper and the GPU entry point share it)."""
+    ptr = _i32(tracks["track_ptr"])
+    n = ptr.size - 1
+    K = int(ptr[-1])
+    pos, view, ids = _f64(tracks["pos"]), _i32(tracks["view"]), _i32(tracks["id"])
+    mpos = np.ascontiguousarray(tracks["mpos"], dtype=np.float32)
+    npts, nm = C.c_int(), C.c_int()
+    pts, meas = np.zeros((max(n, 1), 3)), np.zeros((max(K, 1), 2))
+    mid, cv, cp, xs = (np.zeros(max(K, 1), np.int32), np.zeros(max(K, 1), np.int32), np.zeros(max(K, 1), np.int32),
+                       np.zeros(max(n, 1), np.int32))
+    rc = fn(n, _i(ptr), _d(pos), _i(view), _i(ids), _fp(mpos), int(n_required), C.byref(npts), C.byref(nm), _d(pts),
+            _d(meas), _i(mid), _i(cv), _i(cp), _i(xs))
+    if rc != 0:
+        raise ValueError(f"BundlePointStructure failed: {rc}")
+    M, Kk = npts.value, nm.value
+    return dict(points3d=pts[:M].copy(), measurements=meas[:Kk].copy(), measurement_ids=mid[:Kk].copy(),
+                corresponding_view=cv[:Kk].copy(), corresponding_point=cp[:Kk].copy(), xs_indices=xs[:M].copy())
+
+
+def _cps_call(fn, bps, from_scratch, tracks):
+    """Calls a createPointStructure with the C signature of v3dba_create_point_structure."""
+    pts, meas = _f64(bps["points3d"]).reshape(-1, 3), _f64(bps["measurements"]).reshape(-1, 2)
+    M, K = pts.shape[0], meas.shape[0]
+    mid, cv, cp = _i32(bps["measurement_ids"]), _i32(bps["corresponding_view"]), _i32(bps["corresponding_point"])
+    xs = _i32(bps["xs_indices"])
+    if from_scratch:
+        ptr, pos = np.zeros(M + 1, np.int32), np.zeros((max(M, 1), 3))
+        view, ids, mpos = np.zeros(max(K, 1), np.int32), np.zeros(max(K, 1), np.int32), np.zeros((max(K, 1), 2), np.float32)
+        n = M
+    else:
+        ptr = _i32(tracks["track_ptr"]).copy()
+        n = ptr.size - 1
+        pos = _f64(tracks["pos"]).copy()
+        view, ids = _i32(tracks["view"]).copy(), _i32(tracks["id"]).copy()
+        mpos = np.ascontiguousarray(tracks["mpos"], dtype=np.float32).copy()
+    rc = fn(1 if from_scratch else 0, M, K, _d(pts), _d(meas), _i(mid), _i(cv), _i(cp), _i(xs), n, _i(ptr), _d(pos),
+            _i(view), _i(ids), _fp(mpos))
+    if rc != 0:
+        raise ValueError(f"createPointStructure failed: {rc}")
+    Kt = int(ptr[-1])
+    return dict(track_ptr=ptr, pos=pos[:n].copy(), view=view[:Kt].copy(), id=ids[:Kt].copy(), mpos=mpos[:Kt].copy())
 
 
 class _OrcProblem(C.Structure):

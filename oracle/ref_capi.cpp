@@ -543,5 +543,100 @@ int v3dref_triplet_stage(double const* R, double const* T, double const* focal, 
    return 0;
 }
 
+// ---- BundlePointStructure (V3D/include/Geometry/v3d_mviewutilities.h:132-205) ----------------
+// Tracks in the flat form of v3dba.h: track j = TriangulatedPoint j with pos trackPos[3j..] and
+// measurements trackPtr[j] .. trackPtr[j + 1] - 1 (view, id, float position).
+
+static std::vector<TriangulatedPoint>
+tracksToReconstruction(int nTracks, int const* trackPtr, double const* trackPos, int const* view, int const* id,
+                       float const* pos)
+{
+   std::vector<TriangulatedPoint> rec(nTracks);
+   for (int j = 0; j < nTracks; ++j)
+   {
+      rec[j].pos = makeVector3(trackPos[3*j], trackPos[3*j+1], trackPos[3*j+2]);
+      for (int m = trackPtr[j]; m < trackPtr[j+1]; ++m)
+      {
+         PointMeasurement pm;
+         pm.view = view ? view[m] : 0;
+         pm.id = id ? id[m] : -1;
+         pm.pos[0] = pos[2*m];
+         pm.pos[1] = pos[2*m+1];
+         rec[j].measurements.push_back(pm);
+      }
+   }
+   return rec;
+}
+
+static void
+reconstructionToTracks(std::vector<TriangulatedPoint> const& rec, int* trackPtr, double* trackPos, int* view, int* id,
+                       float* pos)
+{
+   int m = 0;
+   trackPtr[0] = 0;
+   for (size_t j = 0; j < rec.size(); ++j)
+   {
+      for (int c = 0; c < 3; ++c) trackPos[3*j+c] = rec[j].pos[c];
+      for (size_t k = 0; k < rec[j].measurements.size(); ++k, ++m)
+      {
+         if (view) view[m] = rec[j].measurements[k].view;
+         if (id) id[m] = rec[j].measurements[k].id;
+         pos[2*m] = rec[j].measurements[k].pos[0];
+         pos[2*m+1] = rec[j].measurements[k].pos[1];
+      }
+      trackPtr[j+1] = m;
+   }
+}
+
+int v3dref_bundle_point_structure(int nTracks, int const* trackPtr, double const* trackPos, int const* view,
+                                  int const* id, float const* pos, int nRequired, int* nPoints, int* nMeasurements,
+                                  double* points3d, double* measurements, int* measurementIds, int* correspondingView,
+                                  int* correspondingPoint, int* xsIndices)
+{
+   std::vector<TriangulatedPoint> const rec = tracksToReconstruction(nTracks, trackPtr, trackPos, view, id, pos);
+   BundlePointStructure bps(rec, nRequired);
+   *nPoints = (int)bps.points3d.size();
+   *nMeasurements = (int)bps.measurements.size();
+   for (size_t i = 0; i < bps.points3d.size(); ++i)
+   {
+      for (int c = 0; c < 3; ++c) points3d[3*i+c] = bps.points3d[i][c];
+      xsIndices[i] = bps.xsIndices[i];
+   }
+   for (size_t k = 0; k < bps.measurements.size(); ++k)
+   {
+      measurements[2*k] = bps.measurements[k][0];
+      measurements[2*k+1] = bps.measurements[k][1];
+      measurementIds[k] = bps.measurementIds[k];
+      correspondingView[k] = bps.correspondingView[k];
+      correspondingPoint[k] = bps.correspondingPoint[k];
+   }
+   return 0;
+}
+
+int v3dref_create_point_structure(int fromScratch, int nPoints, int nMeasurements, double const* points3d,
+                                  double const* measurements, int const* measurementIds, int const* correspondingView,
+                                  int const* correspondingPoint, int const* xsIndices, int nTracks, int* trackPtr,
+                                  double* trackPos, int* view, int* id, float* pos)
+{
+   BundlePointStructure bps;
+   for (int i = 0; i < nPoints; ++i)
+   {
+      bps.points3d.push_back(makeVector3(points3d[3*i], points3d[3*i+1], points3d[3*i+2]));
+      if (xsIndices) bps.xsIndices.push_back(xsIndices[i]);
+   }
+   for (int k = 0; k < nMeasurements; ++k)
+   {
+      bps.measurements.push_back(makeVector2(measurements[2*k], measurements[2*k+1]));
+      bps.measurementIds.push_back(measurementIds ? measurementIds[k] : -1);
+      bps.correspondingView.push_back(correspondingView ? correspondingView[k] : 0);
+      bps.correspondingPoint.push_back(correspondingPoint ? correspondingPoint[k] : 0);
+   }
+   std::vector<TriangulatedPoint> rec;
+   if (!fromScratch) rec = tracksToReconstruction(nTracks, trackPtr, trackPos, view, id, pos);
+   bps.createPointStructure(rec, fromScratch != 0);
+   reconstructionToTracks(rec, trackPtr, trackPos, view, id, pos);
+   return 0;
+}
+
 } // extern "C"
 

@@ -95,3 +95,23 @@ def test_oracle_pcg_converges(orc):
     x, it = orc.pcg(S, b, 6, rel_tol=1e-10, max_iter=500)
     assert it < 500
     assert rel(S @ x, b) < 1e-8
+
+
+def test_reference_bundle_point_structure_round_trip():
+    """The compiled reference's BundlePointStructure and createPointStructure (from scratch)
+    invert each other on tracks that all pass the measurement threshold."""
+    from oracle.bindings import Reference, reference_available
+    if not reference_available():
+        pytest.skip("compiled reference not present")
+    rng = np.random.default_rng(4)
+    lens = rng.integers(2, 6, size=100)
+    ptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    K = int(ptr[-1])
+    tracks = dict(track_ptr=ptr, pos=rng.normal(size=(100, 3)), view=rng.integers(0, 9, K).astype(np.int32),
+                  id=rng.integers(0, 999, K).astype(np.int32), mpos=rng.normal(size=(K, 2)).astype(np.float32))
+    ref = Reference()
+    bps = ref.bundle_point_structure(tracks, 2)
+    back = ref.create_point_structure(bps, True)
+    for k in tracks:
+        np.testing.assert_array_equal(back[k], tracks[k])
+    assert ref.bundle_point_structure(tracks, -1)["points3d"].shape[0] == 0   # size_t comparison

@@ -46,6 +46,7 @@ EXPORTS = (
     "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
     "v3dba_triplet_stage_flat", "v3dba_cholesky_schedule", "v3dba_tile_schedule", "v3dba_debug_fail_allocation",
     "v3dba_batch_create_flat", "v3dba_dense_cholesky_profile", "v3dba_check_pivot_reciprocals",
+    "v3dba_bundle_point_structure", "v3dba_create_point_structure",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -126,6 +127,11 @@ def _lib():
         L.v3dba_dims.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.v3dba_dense_cholesky_solve.argtypes = [C.c_int, _dp, _dp, _dp, C.POINTER(C.c_int)]
         L.v3dba_check_pivot_reciprocals.argtypes = [C.c_int, _dp, _dp]
+        _fq = C.POINTER(C.c_float)
+        L.v3dba_bundle_point_structure.argtypes = [C.c_int, _ip, _dp, _ip, _ip, _fq, C.c_int, C.POINTER(C.c_int),
+                                                   C.POINTER(C.c_int), _dp, _dp, _ip, _ip, _ip, _ip]
+        L.v3dba_create_point_structure.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _ip, _ip, _ip, _ip, C.c_int,
+                                                   _ip, _dp, _ip, _ip, _fq]
         L.v3dba_dense_cholesky_profile.argtypes = [C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.POINTER(C.c_int),
                                                    C.POINTER(C.c_uint64), C.c_int, C.POINTER(C.c_int),
                                                    C.POINTER(C.c_int)]
@@ -396,6 +402,53 @@ def tile_schedule(pattern, ranks=16):
     plan = {f: buf[bounds[i]:bounds[i + 1]].copy() for i, f in enumerate(LEVEL_PLAN_FIELDS)} if plen.value else {}
     return dict(order=order, n_levels=nl.value, ranks=ranks, uses_levels=bool(use.value), est_levels_us=float(est[0]),
                 est_steps_us=float(est[1]), plan=plan)
+
+
+def _tracks_args(tracks):
+    ptr = np.ascontiguousarray(tracks["track_ptr"], dtype=np.int32)
+    return (ptr, _f64(tracks["pos"]), np.ascontiguousarray(tracks["view"], dtype=np.int32),
+            np.ascontiguousarray(tracks["id"], dtype=np.int32), np.ascontiguousarray(tracks["mpos"], dtype=np.float32))
+
+
+def bundle_point_structure(tracks, n_required=2):
+    """BundlePointStructure(reconstruction, nRequiredMeasurements) on the GPU
+    (v3dba_bundle_point_structure).  tracks: dict of track_ptr (n+1), pos (n, 3), view (K), id (K),
+    mpos (K, 2) float32.  Returns dict of points3d, measurements, measurement_ids,
+    corresponding_view, corresponding_point, xs_indices."""
+    ptr, pos, view, ids, mpos = _tracks_args(tracks)
+    n, K = ptr.size - 1, int(ptr[-1])
+    npts, nm = C.c_int(), C.c_int()
+    pts, meas = np.zeros((max(n, 1), 3)), np.zeros((max(K, 1), 2))
+    mid, cv, cp = (np.zeros(max(K, 1), np.int32) for _ in range(3))
+    xs = np.zeros(max(n, 1), np.int32)
+    check(_lib().v3dba_bundle_point_structure(n, _i(ptr), _d(pos), _i(view), _i(ids), _f32p(mpos), int(n_required),
+                                              C.byref(npts), C.byref(nm), _d(pts), _d(meas), _i(mid), _i(cv), _i(cp),
+                                              _i(xs)), "v3dba_bundle_point_structure")
+    M, Kk = npts.value, nm.value
+    return dict(points3d=pts[:M].copy(), measurements=meas[:Kk].copy(), measurement_ids=mid[:Kk].copy(),
+                corresponding_view=cv[:Kk].copy(), corresponding_point=cp[:Kk].copy(), xs_indices=xs[:M].copy())
+
+
+def create_point_structure(bps, from_scratch=True, tracks=None):
+    """BundlePointStructure::createPointStructure on the GPU (v3dba_create_point_structure):
+    the reconstruction as tracks (a new one from scratch, else `tracks` updated)."""
+    pts, meas = _f64(bps["points3d"]).reshape(-1, 3), _f64(bps["measurements"]).reshape(-1, 2)
+    M, K = pts.shape[0], meas.shape[0]
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+    mid, cv, cp, xs = i32(bps["measurement_ids"]), i32(bps["corresponding_view"]), i32(bps["corresponding_point"]), \
+        i32(bps["xs_indices"])
+    if from_scratch:
+        ptr, pos = np.zeros(M + 1, np.int32), np.zeros((max(M, 1), 3))
+        view, ids, mpos = np.zeros(max(K, 1), np.int32), np.zeros(max(K, 1), np.int32), np.zeros((max(K, 1), 2), np.float32)
+        n = M
+    else:
+        ptr, pos, view, ids, mpos = (a.copy() for a in _tracks_args(tracks))
+        n = ptr.size - 1
+    check(_lib().v3dba_create_point_structure(1 if from_scratch else 0, M, K, _d(pts), _d(meas), _i(mid), _i(cv),
+                                              _i(cp), _i(xs), n, _i(ptr), _d(pos), _i(view), _i(ids), _f32p(mpos)),
+          "v3dba_create_point_structure")
+    Kt = int(ptr[-1])
+    return dict(track_ptr=ptr, pos=pos[:n].copy(), view=view[:Kt].copy(), id=ids[:Kt].copy(), mpos=mpos[:Kt].copy())
 
 
 def check_pivot_reciprocals(x):

@@ -643,17 +643,31 @@ int v3dba_batch_create(const v3dba_problem* problems, int count, v3dba_batch_t* 
     std::copy(q.T, q.T + 3 * q.n_cameras, T.begin() + 3 * (size_t)co);
     std::copy(q.K, q.K + 9 * q.n_cameras, K.begin() + 9 * (size_t)co);
     std::copy(q.X, q.X + 3 * q.n_points, X.begin() + 3 * (size_t)po);
-    // point-major observations (stable)
-    std::vector<int> c(q.n_points + 1, 0);
-    for (int k = 0; k < q.n_measurements; ++k) c[q.point[k] + 1]++;
-    for (int j = 0; j < q.n_points; ++j) c[j + 1] += c[j];
-    for (int j = 0; j <= q.n_points; ++j) ptr[po + j] = oo + c[j];
-    std::vector<int> fill(c.begin(), c.end() - 1);
-    for (int k = 0; k < q.n_measurements; ++k) {
-      const int dst = oo + fill[q.point[k]]++;
-      meas[2 * (size_t)dst] = q.measurements[2 * k];
-      meas[2 * (size_t)dst + 1] = q.measurements[2 * k + 1];
-      cam[dst] = (unsigned char)q.view[k];
+    // point-major observations (stable); inputs already in point order (a triplet stage's, or
+    // any BundlePointStructure's) are copied as they are
+    bool sorted = true;
+    for (int k = 1; k < q.n_measurements && sorted; ++k) sorted = q.point[k] >= q.point[k - 1];
+    if (sorted) {
+      int k = 0;
+      for (int j = 0; j < q.n_points; ++j) {
+        ptr[po + j] = oo + k;
+        while (k < q.n_measurements && q.point[k] == j) ++k;
+      }
+      ptr[po + q.n_points] = oo + q.n_measurements;
+      std::copy(q.measurements, q.measurements + 2 * (size_t)q.n_measurements, meas.begin() + 2 * (size_t)oo);
+      for (int k2 = 0; k2 < q.n_measurements; ++k2) cam[oo + k2] = (unsigned char)q.view[k2];
+    } else {
+      std::vector<int> c(q.n_points + 1, 0);
+      for (int k = 0; k < q.n_measurements; ++k) c[q.point[k] + 1]++;
+      for (int j = 0; j < q.n_points; ++j) c[j + 1] += c[j];
+      for (int j = 0; j <= q.n_points; ++j) ptr[po + j] = oo + c[j];
+      std::vector<int> fill(c.begin(), c.end() - 1);
+      for (int k = 0; k < q.n_measurements; ++k) {
+        const int dst = oo + fill[q.point[k]]++;
+        meas[2 * (size_t)dst] = q.measurements[2 * k];
+        meas[2 * (size_t)dst + 1] = q.measurements[2 * k + 1];
+        cam[dst] = (unsigned char)q.view[k];
+      }
     }
     co += q.n_cameras; po += q.n_points; oo += q.n_measurements;
   }
@@ -694,11 +708,17 @@ int v3dba_batch_create(const v3dba_problem* problems, int count, v3dba_batch_t* 
   BTRY(balloc(h, &h->d.init_cost, count));
   BTRY(balloc(h, &h->d.lambda_out, count));
   BTRY(balloc(h, &h->d.queue, 1));
-  std::vector<double> init;
-  init.insert(init.end(), R.begin(), R.end());
-  init.insert(init.end(), T.begin(), T.end());
-  init.insert(init.end(), X.begin(), X.end());
-  BTRY(bupload(h, &h->d_init, init));
+  // the initial parameters (for v3dba_batch_reset), copied on the device
+  BTRY(balloc(h, &h->d_init, 9 * (size_t)total_cams + 3 * (size_t)total_cams + 3 * (size_t)total_pts));
+  if (cudaMemcpy(h->d_init, h->d.R, sizeof(double) * 9 * total_cams, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+      cudaMemcpy(h->d_init + 9 * (size_t)total_cams, h->d.T, sizeof(double) * 3 * total_cams, cudaMemcpyDeviceToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(h->d_init + 12 * (size_t)total_cams, h->d.X, sizeof(double) * 3 * total_pts, cudaMemcpyDeviceToDevice) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    batch_free(h);
+    return V3DBA_ERR_CUDA;
+  }
 #undef BTRY
   *out = h;
   return V3DBA_OK;

@@ -284,6 +284,86 @@ int radix_sort(Scratch& sc, uint32_t** keys, int** vals, uint32_t* ktmp, int* vt
   return V3DBA_OK;
 }
 
+// ---- BundlePointStructure (V3D/include/Geometry/v3d_mviewutilities.h:132-205) ----------------
+
+// keep[j] = 1 when track j has at least n_required measurements (the reference compares the
+// size_t track length with the int threshold, so a negative threshold keeps nothing); cnt[j] =
+// its measurement count when kept.  Entry n of both is 0 (the scans then end in the totals).
+__global__ void k_bps_flags(const int* __restrict__ ptr, int n, int n_required, int* __restrict__ keep,
+                            int* __restrict__ cnt) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > n) return;
+  if (j == n) {
+    keep[n] = 0;
+    cnt[n] = 0;
+    return;
+  }
+  const int len = ptr[j + 1] - ptr[j];
+  const bool k = n_required >= 0 && len >= n_required;
+  keep[j] = k ? 1 : 0;
+  cnt[j] = k ? len : 0;
+}
+
+// One thread per kept track: its point, its index, and its measurements (float positions widened
+// to double, as makeVector2<double> does) at the scanned offsets.
+__global__ void k_bps_scatter(const int* __restrict__ ptr, const double* __restrict__ pos, const int* __restrict__ view,
+                              const int* __restrict__ id, const float* __restrict__ mpos, int n,
+                              const int* __restrict__ pidx, const int* __restrict__ midx, double* __restrict__ points3d,
+                              double* __restrict__ meas, int* __restrict__ ids, int* __restrict__ cview,
+                              int* __restrict__ cpoint, int* __restrict__ xs) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n || pidx[j + 1] == pidx[j]) return;
+  const int i = pidx[j], o = midx[j], b = ptr[j], len = ptr[j + 1] - b;
+  points3d[3 * (size_t)i] = pos[3 * (size_t)j];
+  points3d[3 * (size_t)i + 1] = pos[3 * (size_t)j + 1];
+  points3d[3 * (size_t)i + 2] = pos[3 * (size_t)j + 2];
+  xs[i] = j;
+  for (int k = 0; k < len; ++k) {
+    meas[2 * (size_t)(o + k)] = (double)mpos[2 * (size_t)(b + k)];
+    meas[2 * (size_t)(o + k) + 1] = (double)mpos[2 * (size_t)(b + k) + 1];
+    ids[o + k] = id[b + k];
+    cview[o + k] = view[b + k];
+    cpoint[o + k] = i;
+  }
+}
+
+// createPointStructure from scratch: measurement t of the new tracks is the caller's src = perm[t]
+// (grouped by point, the caller's order inside a point); positions narrowed to float.
+__global__ void k_cps_gather(const int* __restrict__ perm, const double* __restrict__ meas, const int* __restrict__ ids,
+                             const int* __restrict__ cview, int K, int* __restrict__ view, int* __restrict__ id,
+                             float* __restrict__ mpos) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= K) return;
+  const int src = perm[t];
+  view[t] = cview[src];
+  id[t] = ids[src];
+  mpos[2 * (size_t)t] = (float)meas[2 * (size_t)src];
+  mpos[2 * (size_t)t + 1] = (float)meas[2 * (size_t)src + 1];
+}
+
+__global__ void k_cps_lengths(const int* __restrict__ ptr, const int* __restrict__ xs, int M, int* __restrict__ len) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < M) len[i] = ptr[xs[i] + 1] - ptr[xs[i]];
+  else if (i == M) len[M] = 0;
+}
+
+// createPointStructure in place: kept track xs[i] gets point i and, in order, the next len_i
+// measurements (from offset off[i]) as its measurement positions.
+__global__ void k_cps_inplace(const int* __restrict__ ptr, const int* __restrict__ xs, const int* __restrict__ off,
+                              int M, const double* __restrict__ points3d, const double* __restrict__ meas,
+                              double* __restrict__ pos, float* __restrict__ mpos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const int j = xs[i], b = ptr[j], len = ptr[j + 1] - b, o = off[i];
+  pos[3 * (size_t)j] = points3d[3 * (size_t)i];
+  pos[3 * (size_t)j + 1] = points3d[3 * (size_t)i + 1];
+  pos[3 * (size_t)j + 2] = points3d[3 * (size_t)i + 2];
+  for (int k = 0; k < len; ++k) {
+    mpos[2 * (size_t)(b + k)] = (float)meas[2 * (size_t)(o + k)];
+    mpos[2 * (size_t)(b + k) + 1] = (float)meas[2 * (size_t)(o + k) + 1];
+  }
+}
+
 }  // namespace
 
 int build_structure_device(const v3dba_problem* p, const DevAlloc& alloc, cudaStream_t st, DeviceStructure& S) {
@@ -480,3 +560,172 @@ int group_by_key_device(const int* keys, int n, int nv, int* perm, int* ptr, cud
 }
 
 }  // namespace v3dba
+
+using namespace v3dba;
+
+namespace {
+
+// A stream and a scratch list for one standalone call; the stream is synchronised and destroyed
+// at the end.
+struct CallScope {
+  cudaStream_t st = nullptr;
+  Scratch* sc = nullptr;
+  ~CallScope() {
+    if (sc) delete sc;   // frees the buffers on the stream
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  }
+};
+
+template <typename T>
+int up_copy(Scratch& sc, T** d, const T* h, size_t n, cudaStream_t st) {
+  int rc = sc.get(d, n);
+  if (rc) return rc;
+  if (n && h) V3DBA_CUDA_TRY(cudaMemcpyAsync(*d, h, sizeof(T) * n, cudaMemcpyHostToDevice, st));
+  return V3DBA_OK;
+}
+
+template <typename T>
+int down_copy(T* h, const T* d, size_t n, cudaStream_t st) {
+  if (n && h) V3DBA_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, st));
+  return V3DBA_OK;
+}
+
+bool valid_track_ptr(const int* ptr, int n) {
+  if (ptr[0] != 0) return false;
+  for (int j = 0; j < n; ++j)
+    if (ptr[j + 1] < ptr[j]) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" int v3dba_bundle_point_structure(int n_tracks, const int* track_ptr, const double* track_pos,
+                                            const int* meas_view, const int* meas_id, const float* meas_pos,
+                                            int n_required, int* n_points, int* n_measurements, double* points3d,
+                                            double* measurements, int* measurement_ids, int* corresponding_view,
+                                            int* corresponding_point, int* xs_indices) {
+  if (n_tracks < 0 || !track_ptr || !n_points || !n_measurements) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (!valid_track_ptr(track_ptr, n_tracks)) return V3DBA_ERR_INVALID_INPUT;
+  const int K = track_ptr[n_tracks];
+  if ((n_tracks && !track_pos) || (K && (!meas_view || !meas_id || !meas_pos))) return V3DBA_ERR_INVALID_ARGUMENT;
+  NvtxRange nvtx("v3dba_bundle_point_structure");
+  CallScope cs;
+  V3DBA_CUDA_TRY(cudaStreamCreateWithFlags(&cs.st, cudaStreamNonBlocking));
+  cs.sc = new Scratch();
+  cs.sc->st = cs.st;
+  Scratch& sc = *cs.sc;
+  const cudaStream_t st = cs.st;
+  int *d_ptr, *d_view, *d_id, *d_keep, *d_cnt, *o_ids, *o_view, *o_point, *o_xs;
+  double *d_pos, *o_pts, *o_meas;
+  float* d_mpos;
+  int rc;
+  if ((rc = up_copy(sc, &d_ptr, track_ptr, (size_t)n_tracks + 1, st)) ||
+      (rc = up_copy(sc, &d_pos, track_pos, 3 * (size_t)n_tracks, st)) ||
+      (rc = up_copy(sc, &d_view, meas_view, (size_t)K, st)) || (rc = up_copy(sc, &d_id, meas_id, (size_t)K, st)) ||
+      (rc = up_copy(sc, &d_mpos, meas_pos, 2 * (size_t)K, st)) || (rc = sc.get(&d_keep, (size_t)n_tracks + 1)) ||
+      (rc = sc.get(&d_cnt, (size_t)n_tracks + 1)) || (rc = sc.get(&o_pts, 3 * (size_t)n_tracks)) ||
+      (rc = sc.get(&o_meas, 2 * (size_t)K)) || (rc = sc.get(&o_ids, (size_t)K)) || (rc = sc.get(&o_view, (size_t)K)) ||
+      (rc = sc.get(&o_point, (size_t)K)) || (rc = sc.get(&o_xs, (size_t)n_tracks)))
+    return rc;
+  k_bps_flags<<<cdiv(n_tracks + 1, 256), 256, 0, st>>>(d_ptr, n_tracks, n_required, d_keep, d_cnt);
+  V3DBA_LAUNCH_CHECK();
+  if ((rc = scan_exclusive(sc, d_keep, n_tracks + 1, st)) || (rc = scan_exclusive(sc, d_cnt, n_tracks + 1, st))) return rc;
+  if (n_tracks > 0) {
+    k_bps_scatter<<<cdiv(n_tracks, 128), 128, 0, st>>>(d_ptr, d_pos, d_view, d_id, d_mpos, n_tracks, d_keep, d_cnt,
+                                                       o_pts, o_meas, o_ids, o_view, o_point, o_xs);
+    V3DBA_LAUNCH_CHECK();
+  }
+  int tot[2] = {0, 0};
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(&tot[0], d_keep + n_tracks, sizeof(int), cudaMemcpyDeviceToHost, st));
+  V3DBA_CUDA_TRY(cudaMemcpyAsync(&tot[1], d_cnt + n_tracks, sizeof(int), cudaMemcpyDeviceToHost, st));
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+  const int M = tot[0], Kk = tot[1];
+  if ((rc = down_copy(points3d, o_pts, 3 * (size_t)M, st)) || (rc = down_copy(measurements, o_meas, 2 * (size_t)Kk, st)) ||
+      (rc = down_copy(measurement_ids, o_ids, (size_t)Kk, st)) || (rc = down_copy(corresponding_view, o_view, (size_t)Kk, st)) ||
+      (rc = down_copy(corresponding_point, o_point, (size_t)Kk, st)) || (rc = down_copy(xs_indices, o_xs, (size_t)M, st)))
+    return rc;
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+  *n_points = M;
+  *n_measurements = Kk;
+  return V3DBA_OK;
+}
+
+extern "C" int v3dba_create_point_structure(int from_scratch, int n_points, int n_measurements, const double* points3d,
+                                            const double* measurements, const int* measurement_ids,
+                                            const int* corresponding_view, const int* corresponding_point,
+                                            const int* xs_indices, int n_tracks, int* track_ptr, double* track_pos,
+                                            int* meas_view, int* meas_id, float* meas_pos) {
+  if (n_points < 0 || n_measurements < 0 || !track_ptr || !track_pos) return V3DBA_ERR_INVALID_ARGUMENT;
+  if ((n_points && !points3d) || (n_measurements && !measurements)) return V3DBA_ERR_INVALID_ARGUMENT;
+  NvtxRange nvtx("v3dba_create_point_structure");
+  CallScope cs;
+  V3DBA_CUDA_TRY(cudaStreamCreateWithFlags(&cs.st, cudaStreamNonBlocking));
+  cs.sc = new Scratch();
+  cs.sc->st = cs.st;
+  Scratch& sc = *cs.sc;
+  const cudaStream_t st = cs.st;
+  int rc;
+  if (from_scratch) {
+    const int K = n_measurements, M = n_points;
+    if (K && (!measurement_ids || !corresponding_view || !corresponding_point || !meas_view || !meas_id || !meas_pos))
+      return V3DBA_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < K; ++k)
+      if (corresponding_point[k] < 0 || corresponding_point[k] >= M) return V3DBA_ERR_INVALID_INPUT;
+    int *d_cp, *d_ids, *d_cv, *d_perm, *d_ptr, *o_view, *o_id;
+    double* d_meas;
+    float* o_mpos;
+    if ((rc = up_copy(sc, &d_cp, corresponding_point, (size_t)K, st)) ||
+        (rc = up_copy(sc, &d_ids, measurement_ids, (size_t)K, st)) ||
+        (rc = up_copy(sc, &d_cv, corresponding_view, (size_t)K, st)) ||
+        (rc = up_copy(sc, &d_meas, measurements, 2 * (size_t)K, st)) || (rc = sc.get(&d_perm, (size_t)K)) ||
+        (rc = sc.get(&d_ptr, (size_t)M + 1)) || (rc = sc.get(&o_view, (size_t)K)) || (rc = sc.get(&o_id, (size_t)K)) ||
+        (rc = sc.get(&o_mpos, 2 * (size_t)K)))
+      return rc;
+    if ((rc = group_by_key_device(d_cp, K, M, d_perm, d_ptr, st))) return rc;
+    if (K > 0) {
+      k_cps_gather<<<cdiv(K, 256), 256, 0, st>>>(d_perm, d_meas, d_ids, d_cv, K, o_view, o_id, o_mpos);
+      V3DBA_LAUNCH_CHECK();
+    }
+    if ((rc = down_copy(track_ptr, d_ptr, (size_t)M + 1, st)) || (rc = down_copy(meas_view, o_view, (size_t)K, st)) ||
+        (rc = down_copy(meas_id, o_id, (size_t)K, st)) || (rc = down_copy(meas_pos, o_mpos, 2 * (size_t)K, st)))
+      return rc;
+    V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (M) std::memcpy(track_pos, points3d, sizeof(double) * 3 * (size_t)M);
+    return V3DBA_OK;
+  }
+  // in place: the tracks keep their measurement lists; kept track xs[i] is updated
+  const int M = n_points;
+  if (n_tracks < 0 || (M && !xs_indices) || !valid_track_ptr(track_ptr, n_tracks)) return V3DBA_ERR_INVALID_INPUT;
+  const int KT = track_ptr[n_tracks];
+  if (KT && !meas_pos) return V3DBA_ERR_INVALID_ARGUMENT;
+  long need = 0;
+  for (int i = 0; i < M; ++i) {
+    if (xs_indices[i] < 0 || xs_indices[i] >= n_tracks) return V3DBA_ERR_INVALID_INPUT;
+    need += track_ptr[xs_indices[i] + 1] - track_ptr[xs_indices[i]];
+  }
+  if (need > n_measurements) return V3DBA_ERR_INVALID_INPUT;
+  int *d_ptr, *d_xs, *d_off;
+  double *d_pts, *d_meas, *d_pos;
+  float* d_mpos;
+  if ((rc = up_copy(sc, &d_ptr, (const int*)track_ptr, (size_t)n_tracks + 1, st)) ||
+      (rc = up_copy(sc, &d_xs, xs_indices, (size_t)M, st)) || (rc = sc.get(&d_off, (size_t)M + 1)) ||
+      (rc = up_copy(sc, &d_pts, points3d, 3 * (size_t)M, st)) ||
+      (rc = up_copy(sc, &d_meas, measurements, 2 * (size_t)n_measurements, st)) ||
+      (rc = up_copy(sc, &d_pos, (const double*)track_pos, 3 * (size_t)n_tracks, st)) ||
+      (rc = up_copy(sc, &d_mpos, (const float*)meas_pos, 2 * (size_t)KT, st)))
+    return rc;
+  k_cps_lengths<<<cdiv(M + 1, 256), 256, 0, st>>>(d_ptr, d_xs, M, d_off);
+  V3DBA_LAUNCH_CHECK();
+  if ((rc = scan_exclusive(sc, d_off, M + 1, st))) return rc;
+  if (M > 0) {
+    k_cps_inplace<<<cdiv(M, 128), 128, 0, st>>>(d_ptr, d_xs, d_off, M, d_pts, d_meas, d_pos, d_mpos);
+    V3DBA_LAUNCH_CHECK();
+  }
+  if ((rc = down_copy(track_pos, d_pos, 3 * (size_t)n_tracks, st)) || (rc = down_copy(meas_pos, d_mpos, 2 * (size_t)KT, st)))
+    return rc;
+  V3DBA_CUDA_TRY(cudaStreamSynchronize(st));
+  return V3DBA_OK;
+}
