@@ -488,6 +488,9 @@ int v3dba_structure(v3dba_handle h, int64_t* n_pairs, int* n_blocks, int32_t* o_
 /* FP64 tensor-core (DMMA) throughput of the current GPU in TFLOP/s, measured by a short kernel
  * of independent mma.sync f64 chains on every SM (benchmark support). */
 int v3dba_measure_fp64_mma_peak(double* tflops);
+/* Benchmark support (no counterpart in the reference): the FP64 FMA-pipe (non-tensor) throughput of
+ * the current GPU in TFLOP/s, measured by a short kernel of independent FMA chains. */
+int v3dba_measure_fp64_fma_peak(double* tflops);
 
 /* FLOPs the tile Cholesky executes per factor + solve of this problem's dense reduced system
  * (64^3 GEMM tiles of its panel and trailing tasks plus the diagonal factors; benchmark

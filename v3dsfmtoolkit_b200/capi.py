@@ -46,7 +46,7 @@ EXPORTS = (
     "v3dba_rotations_autotune", "v3dba_default_triplet_stage_options", "v3dba_triplet_stage",
     "v3dba_triplet_stage_flat", "v3dba_cholesky_schedule", "v3dba_tile_schedule", "v3dba_debug_fail_allocation",
     "v3dba_batch_create_flat", "v3dba_dense_cholesky_profile", "v3dba_check_pivot_reciprocals",
-    "v3dba_bundle_point_structure", "v3dba_create_point_structure",
+    "v3dba_bundle_point_structure", "v3dba_create_point_structure", "v3dba_measure_fp64_fma_peak",
 )
 STAGES = ("linearize", "camera_chunks", "camera_finish", "relin_finalize", "point_eliminate", "schur_chunks",
           "schur_finish", "rhs_chunks", "rhs_finish", "global_block", "point_backsub", "camera_update",
@@ -149,6 +149,7 @@ def _lib():
         L.v3dba_batch_get_params.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
         L.v3dba_batch_get_all_params.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.v3dba_measure_fp64_mma_peak.argtypes = [_dp]
+        L.v3dba_measure_fp64_fma_peak.argtypes = [_dp]
         L.v3dba_cholesky_flops.argtypes = [C.c_void_p, _dp]
         L.v3dba_cholesky_schedule.argtypes = [C.c_void_p, _ip, _ip, _ip]
         L.v3dba_tile_schedule.argtypes = [C.c_int, C.POINTER(C.c_uint8), C.c_int, _ip, _ip, _ip, _dp, _ip, C.c_int,
@@ -239,6 +240,12 @@ def dims(model, mode):
 def fp64_mma_peak_tflops() -> float:
     t = C.c_double()
     check(_lib().v3dba_measure_fp64_mma_peak(C.byref(t)), "v3dba_measure_fp64_mma_peak")
+    return t.value
+
+
+def fp64_fma_peak_tflops() -> float:
+    t = C.c_double()
+    check(_lib().v3dba_measure_fp64_fma_peak(C.byref(t)), "v3dba_measure_fp64_fma_peak")
     return t.value
 
 

@@ -534,9 +534,13 @@ namespace {
 
 template <typename T>
 int balloc(v3dba_batch_t h, T** p, size_t n) {
+  // stream-ordered, from the device's pool (which keeps what a destroyed batch freed): a batch
+  // created per call does not pay cudaMalloc / cudaFree each time
   void* q = nullptr;
+  int rc0 = ensure_pool();
+  if (rc0) return rc0;
   if (injected_alloc_failure()) return V3DBA_ERR_OUT_OF_MEMORY;
-  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(n, 1) * sizeof(T), h->stream);
   if (e != cudaSuccess) { cudaGetLastError(); return V3DBA_ERR_OUT_OF_MEMORY; }
   h->allocs.push_back(q);
   *p = static_cast<T*>(q);
@@ -547,14 +551,17 @@ template <typename T>
 int bupload(v3dba_batch_t h, T** p, const std::vector<T>& v) {
   int rc = balloc(h, p, v.size());
   if (rc) return rc;
-  if (!v.empty()) V3DBA_CUDA_TRY(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  // the host vector outlives the copy: v3dba_batch_create synchronises the stream before returning
+  if (!v.empty()) V3DBA_CUDA_TRY(cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
   return V3DBA_OK;
 }
 
 void batch_free(v3dba_batch_t h) {
   if (!h) return;
-  if (h->stream) cudaStreamSynchronize(h->stream);
-  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) {
+    for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
+    cudaStreamSynchronize(h->stream);
+  }
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -710,11 +717,13 @@ int v3dba_batch_create(const v3dba_problem* problems, int count, v3dba_batch_t* 
   BTRY(balloc(h, &h->d.queue, 1));
   // the initial parameters (for v3dba_batch_reset), copied on the device
   BTRY(balloc(h, &h->d_init, 9 * (size_t)total_cams + 3 * (size_t)total_cams + 3 * (size_t)total_pts));
-  if (cudaMemcpy(h->d_init, h->d.R, sizeof(double) * 9 * total_cams, cudaMemcpyDeviceToDevice) != cudaSuccess ||
-      cudaMemcpy(h->d_init + 9 * (size_t)total_cams, h->d.T, sizeof(double) * 3 * total_cams, cudaMemcpyDeviceToDevice) !=
+  if (cudaMemcpyAsync(h->d_init, h->d.R, sizeof(double) * 9 * total_cams, cudaMemcpyDeviceToDevice, h->stream) !=
           cudaSuccess ||
-      cudaMemcpy(h->d_init + 12 * (size_t)total_cams, h->d.X, sizeof(double) * 3 * total_pts, cudaMemcpyDeviceToDevice) !=
-          cudaSuccess) {
+      cudaMemcpyAsync(h->d_init + 9 * (size_t)total_cams, h->d.T, sizeof(double) * 3 * total_cams,
+                      cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess ||
+      cudaMemcpyAsync(h->d_init + 12 * (size_t)total_cams, h->d.X, sizeof(double) * 3 * total_pts,
+                      cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess) {
     cudaGetLastError();
     batch_free(h);
     return V3DBA_ERR_CUDA;
