@@ -44,3 +44,14 @@ def reduce_scalar(dist, value: float, op: str, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def gather_shards(dist, local: list) -> list:
+    """The per-rank result lists of a sharded job, concatenated in rank order (every rank gets the
+    whole list; with contiguous shards from shard_range this is the job's order).  Host objects
+    over the process group (gloo or NCCL); the identity without a process group."""
+    if dist is None:
+        return list(local)
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, list(local))
+    return [x for part in parts for x in part]
