@@ -150,6 +150,26 @@ __device__ __forceinline__ void unpack_sym(int u, int& r, int& c) {
 
 constexpr int kPtThreads = 128;
 constexpr int kCamWarps = 4;
+// Lanes per point of the track kernels that store or load one block per observation: the lanes of
+// a group take the observations of one track in turn, so a warp's 16-byte stores / loads of one
+// trip hit runs of consecutive blocks instead of 32 scattered ones (the observations of a track
+// are contiguous in the point-major order), at the price of idle lanes on short tracks and of
+// the group sums.  Measured on the 200-camera scene (375k observations, tracks of 3-12), in µs
+// per launch for 1 / 2 / 4 / 8 lanes: k_linearize FP32 53.8 / 51.3 / 61.1 / 86.8, FP64 105.6 /
+// 87.9 / 92.1 / 113.3; k_point_backsub FP32 13.5 / 16.6 / 14.8 / 14.6, FP64 30.2 / 17.7 / 20.8 /
+// 21.0; k_point_eliminate was fastest with one lane (23.1 / 49.7) and keeps one.
+constexpr int kLinLanes = 2;
+template <typename Real>
+__host__ __device__ constexpr int backsub_lanes() { return sizeof(Real) == 8 ? 2 : 1; }
+constexpr int kMaxPtLanes = 2;
+
+// Sum over the G consecutive lanes of a group (all lanes of the warp take part).
+template <int G, typename T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 
 template <int DC>
 struct RelinNV {
@@ -158,8 +178,9 @@ struct RelinNV {
   static constexpr int NV = NS + 2;        // + max |gb|, max diag V
 };
 
-// One thread per point: linearise every observation of its track (FP64), store the weighted
-// blocks, and accumulate V_j, gb_j, Y_j; Z, gc and the cost go to per-block partials.
+// kLinLanes lanes per point: each linearises every kLinLanes-th observation of the track (FP64),
+// stores the weighted blocks, and accumulates its share of V_j, gb_j, Y_j, summed over the group
+// at the end in a fixed order; Z, gc and the cost go to per-block partials.
 template <int MODEL, int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
@@ -169,25 +190,28 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
   constexpr int NS = RelinNV<DC>::NS, NV = RelinNV<DC>::NV, NZ = L::NZ;
   __shared__ double red[(kPtThreads / 32) * NV];
   const Dims& D = s.d;
-  const int tp = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tp = gt / kLinLanes, lig = gt % kLinLanes;
   const int j = tp < D.M ? (s.p_order ? s.p_order[tp] : tp) : D.M;   // longest tracks first (p_order)
   double v[NV];
 #pragma unroll
   for (int t = 0; t < NV; ++t) v[t] = (t < NS) ? 0.0 : -1e30;
+  double V[6] = {0, 0, 0, 0, 0, 0}, gb[3] = {0, 0, 0}, Y[3][DCc];
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+#pragma unroll
+    for (int c = 0; c < DCc; ++c) Y[b][c] = 0.0;
+  const bool fixB = j < D.nnB;
+  int k0 = 0, k1 = 0;
 
   if (j < D.M) {
-    const bool fixB = j < D.nnB;
     const double X[3] = {s.cur.X[3 * j], s.cur.X[3 * j + 1], s.cur.X[3 * j + 2]};
-    double V[6] = {0, 0, 0, 0, 0, 0}, gb[3] = {0, 0, 0}, Y[3][DCc];
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-#pragma unroll
-      for (int c = 0; c < DCc; ++c) Y[b][c] = 0.0;
     Real* oA = reinterpret_cast<Real*>(s.o_A);
     Real* oW = reinterpret_cast<Real*>(s.o_W);
     Real* oC = reinterpret_cast<Real*>(s.o_C);
-    const int k0 = s.p_ptr[j], k1 = s.p_ptr[j + 1];
-    for (int k = k0; k < k1; ++k) {
+    k0 = s.p_ptr[j];
+    k1 = s.p_ptr[j + 1];
+    for (int k = k0 + lig; k < k1; k += kLinLanes) {
       const int i = s.o_cam[k];
       const bool fixA = i < D.nnA;
       Cam cam;
@@ -265,12 +289,21 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
         for (int c = 0; c < DCc; ++c) v[1 + NZ + c] += C[0][c] * r0 + C[1][c] * r1;
       }
     }
-    Real* pV = reinterpret_cast<Real*>(s.p_V) + (size_t)j * L::SV;
+  }
+  // the group's sums (every lane takes part in the shuffles)
+#pragma unroll
+  for (int t = 0; t < 6; ++t) V[t] = group_sum<kLinLanes>(V[t]);
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    gb[b] = group_sum<kLinLanes>(gb[b]);
+#pragma unroll
+    for (int c = 0; c < DCc; ++c) Y[b][c] = DC > 0 ? group_sum<kLinLanes>(Y[b][c]) : 0.0;
+  }
+  if (j < D.M && lig == 0) {
     Real vv[L::SV];
 #pragma unroll
     for (int t = 0; t < L::SV; ++t) vv[t] = t < 6 ? Real(V[t]) : Real(0);
     vstore(reinterpret_cast<Real*>(s.p_V) + (size_t)j * L::SV, vv);
-    (void)pV;
     double g4[4] = {gb[0], gb[1], gb[2], 0.0};
     vstore(s.p_gb + (size_t)j * 4, g4);
     if (DC > 0) {
@@ -767,27 +800,35 @@ __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double
   constexpr int DCc = L::DCc;
   __shared__ double red[(kPtThreads / 32) * 2];
   const Dims& D = s.d;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int G = backsub_lanes<Real>();
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = gt / G, lig = gt % G;
+  const bool active = j < D.M && j >= D.nnB;
   double v[2] = {0.0, 0.0};
-  if (j < D.M) {
-    const double* x = s.x;
+  double acc[3] = {0, 0, 0};
+  const double* x = s.x;
+  if (active) {
+    // this lane's share of sum_k T_k^T dc_i over the track
+    const Real* oT = reinterpret_cast<const Real*>(s.o_T);
+    for (int k = s.p_ptr[j] + lig; k < s.p_ptr[j + 1]; k += G) {
+      const int i = s.o_cam[k];
+      Real t[L::SW];
+      vload(oT + (size_t)k * L::SW, t);
+#pragma unroll
+      for (int a = 0; a < DA; ++a) {
+        const double da = x[i * DA + a];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] += double(t[a * 3 + c]) * da;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) acc[c] = group_sum<G>(acc[c]);
+  if (j < D.M && lig == 0) {
     double db[3] = {0, 0, 0};
-    if (j >= D.nnB) {
+    if (active) {
       double q[4];
       vload(s.p_q + (size_t)j * 4, q);
-      double acc[3] = {0, 0, 0};
-      const Real* oT = reinterpret_cast<const Real*>(s.o_T);
-      for (int k = s.p_ptr[j]; k < s.p_ptr[j + 1]; ++k) {
-        const int i = s.o_cam[k];
-        Real t[L::SW];
-        vload(oT + (size_t)k * L::SW, t);
-#pragma unroll
-        for (int a = 0; a < DA; ++a) {
-          const double da = x[i * DA + a];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) acc[c] += double(t[a * 3 + c]) * da;
-        }
-      }
       if (DC > 0) {
         Real yv[L::SY];
         vload(reinterpret_cast<const Real*>(s.p_YV) + (size_t)j * L::SY, yv);
@@ -955,17 +996,20 @@ struct PartLayout {
   size_t relin_pt, relin_cam, elim, backsub, camupd, obs;
 };
 
+// blocks of a track kernel with `lanes` lanes per point (the partial regions are sized for the most)
+inline int lane_blocks(int M, int lanes = kMaxPtLanes) { return cdiv((int64_t)std::max(M, 1) * lanes, kPtThreads); }
+
 template <int DA, int DC>
 inline PartLayout part_layout(const DevState& s) {
   PartLayout p;
-  const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);
+  const int bl = lane_blocks(s.d.M);
   const int bc = cdiv(std::max(s.d.N, 1), kCamWarps);
   const int bu = cdiv(std::max(s.d.N, 1), 128);
   p.relin_pt = 0;
-  p.relin_cam = p.relin_pt + (size_t)bp * RelinNV<DC>::NV;
+  p.relin_cam = p.relin_pt + (size_t)bl * RelinNV<DC>::NV;
   p.elim = p.relin_cam + (size_t)bc * 2;
-  p.backsub = p.elim + (size_t)bp * ElimNV<DC>::NV;
-  p.camupd = p.backsub + (size_t)bp * 2;
+  p.backsub = p.elim + (size_t)bl * ElimNV<DC>::NV;
+  p.camupd = p.backsub + (size_t)bl * 2;
   p.obs = p.camupd + (size_t)bu * 2;
   return p;
 }
@@ -975,14 +1019,16 @@ struct Ops {
   // Launches one stage of the LM iteration (see LmStage in lm.cuh).
   static int stage(DevState& s, int id, int init_lambda, double tau, cudaStream_t st) {
     const PartLayout pl = part_layout<DA, DC>(s);
-    const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);
+    const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);                  // one lane per point
+    const int bl = lane_blocks(s.d.M, kLinLanes);                          // the linearisation
+    const int bb = lane_blocks(s.d.M, backsub_lanes<Real>());              // the back-substitution
     const int bc = cdiv(std::max(s.d.N, 1), kCamWarps);
     const int bu = cdiv(std::max(s.d.N, 1), 128);
     const int bo = cdiv(std::max(s.d.K, 1), 256);
     cudaError_t e = cudaSuccess;
     switch (id) {
       case kStageLinearize:
-        e = launch_pdl(k_linearize<MODEL, DA, DC, Real>, dim3(bp), dim3(kPtThreads), 0, st, s, s.part + pl.relin_pt);
+        e = launch_pdl(k_linearize<MODEL, DA, DC, Real>, dim3(bl), dim3(kPtThreads), 0, st, s, s.part + pl.relin_pt);
         break;
       case kStageCameraChunks:
         if (s.nch_cam == 0) return V3DBA_OK;
@@ -994,7 +1040,7 @@ struct Ops {
                        s.part + pl.relin_cam);
         break;
       case kStageRelinFinalize:
-        e = launch_pdl(k_relin_finalize<DC>, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.relin_pt), bp,
+        e = launch_pdl(k_relin_finalize<DC>, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.relin_pt), bl,
                        (const double*)(s.part + pl.relin_cam), bc, init_lambda, tau);
         break;
       case kStagePointEliminate:
@@ -1021,7 +1067,7 @@ struct Ops {
         e = launch_pdl(k_global_block<DA, DC>, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.elim), bp);
         break;
       case kStagePointBacksub:
-        e = launch_pdl(k_point_backsub<DA, DC, Real>, dim3(bp), dim3(kPtThreads), 0, st, s, s.part + pl.backsub);
+        e = launch_pdl(k_point_backsub<DA, DC, Real>, dim3(bb), dim3(kPtThreads), 0, st, s, s.part + pl.backsub);
         break;
       case kStageCameraUpdate:
         e = launch_pdl(k_camera_update<MODEL, DA, DC>, dim3(bu), dim3(128), 0, st, s, s.part + pl.camupd);
@@ -1030,7 +1076,7 @@ struct Ops {
         e = launch_pdl(k_obs_cost<MODEL>, dim3(bo), dim3(256), 0, st, s, (ParamSet)s.trial, 0, s.part + pl.obs);
         break;
       case kStageTrialFinalize:
-        e = launch_pdl(k_trial_finalize, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.backsub), bp,
+        e = launch_pdl(k_trial_finalize, dim3(1), dim3(256), 0, st, s, (const double*)(s.part + pl.backsub), bb,
                        (const double*)(s.part + pl.camupd), bu, (const double*)(s.part + pl.obs), bo);
         break;
       default:
@@ -1084,12 +1130,12 @@ size_t block_chunk_values(int DA) { return (size_t)round32(DA * DA); }
 
 // size (in doubles) of the partial buffer for the given dims
 size_t partial_doubles(const DevState& s) {
-  const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);
   const int bc = cdiv(std::max(s.d.N, 1), kCamWarps);
   const int bu = cdiv(std::max(s.d.N, 1), 128);
   const int bo = cdiv(std::max(s.d.K, 1), 256);
   const size_t maxNV = RelinNV<7>::NV;
-  return (size_t)bp * maxNV + (size_t)bc * 2 + (size_t)bp * ElimNV<7>::NV + (size_t)bp * 2 + (size_t)bu * 2 + bo + 64;
+  const int bl = lane_blocks(s.d.M);
+  return (size_t)bl * maxNV + (size_t)bc * 2 + (size_t)bl * ElimNV<7>::NV + (size_t)bl * 2 + (size_t)bu * 2 + bo + 64;
 }
 
 template <typename Real>
