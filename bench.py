@@ -167,10 +167,30 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # the sampler is running (its first line is written) before the timed region starts
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
+        with open(self.path) as f:
+            self.skip = sum(1 for _ in f)   # samples taken before the timed region
+
+    def sample_now(self):
+        """One more sample at once (short timed regions end between two periodic samples)."""
+        if self.proc is None:
+            return
+        try:
+            out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=10).stdout
+            with open(self.path, "a") as f:
+                f.write(out)
+        except (OSError, subprocess.SubprocessError):
+            pass
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.sample_now()
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -178,7 +198,7 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in list(open(self.path))[getattr(self, "skip", 0):]:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
