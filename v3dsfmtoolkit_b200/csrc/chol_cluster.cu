@@ -275,6 +275,19 @@ __device__ __forceinline__ void load_tile(double* dst, const double* __restrict_
   asm volatile("cp.async.commit_group;\n" ::);
 }
 __device__ __forceinline__ void tile_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// The copies of load_tile without the commit (several tiles in one group).
+__device__ __forceinline__ void copy_tile(double* dst, const double* __restrict__ S, size_t ld, size_t r0, size_t c0) {
+  for (int e = threadIdx.x; e < TB * TB / 2; e += blockDim.x) {
+    const int c = e >> 5, m2 = (e & 31) * 2;
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst + c * LDT + m2);
+    const double* g = S + (c0 + c) * ld + r0 + m2;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g));
+  }
+}
+__device__ __forceinline__ void tile_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+// Shared memory of k_chol_levels: six 64 x LDT tiles (two sets of input + two operands, so that
+// the next phase-1 task's tiles load while the current one computes) and the rhs reduction.
+constexpr size_t kLevelsSmem = (6 * TB * LDT + 4 * TB) * sizeof(double);
 
 }  // namespace
 
@@ -532,6 +545,10 @@ __global__ void __launch_bounds__(256)
   double* T0 = sm;
   double* T1 = sm + TB * LDT;
   double* T2 = sm + 2 * TB * LDT;
+  // phase 1: tile set 0 = (T2 input, T0 and T1 operands), set 1 = the next three tiles
+  auto In = [&](int set) { return set ? sm + 5 * TB * LDT : T2; };
+  auto Oa = [&](int set) { return set ? sm + 3 * TB * LDT : T0; };
+  auto Ob = [&](int set) { return set ? sm + 4 * TB * LDT : T1; };
   const size_t lds = (size_t)ld;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
   auto stamp = [&](int slot) {
@@ -544,7 +561,7 @@ __global__ void __launch_bounds__(256)
   // rhs row of tile column j (at physical column pc0): b_j -= sum_k L_jk y_k (phase 1) and
   // y_j = Z_j b_j (phase 2); thread (group, col) sums every fourth t, groups combined in a fixed
   // order through shared memory
-  double* red = T0;
+  double* red = sm + 6 * TB * LDT;
   auto rhs_update = [&](size_t pc0, int t) {
     const int col = tid & 63, grp = tid >> 6;
     double acc = 0.0;
@@ -574,7 +591,28 @@ __global__ void __launch_bounds__(256)
 
   for (int lv = 0; lv < P.n_levels; ++lv) {
     stamp(2 * lv);
-    for (int e = P.p1ptr[lv * ranks + rank]; e < P.p1ptr[lv * ranks + rank + 1]; ++e) {
+    // The input tile and the first update's operands of the CTA's next task are fetched into the
+    // other tile set while the current task computes its last product (tasks of one phase are
+    // independent: their targets differ and their operands are panels of earlier levels).
+    const int e_end = P.p1ptr[lv * ranks + rank + 1];
+    auto issue = [&](int e, int set) -> bool {
+      const int t = P.p1[e];
+      const int r = P.tr[t], j = P.tc[t], mode = P.tmode[t] & 3;
+      if (r == nt) return false;
+      const size_t pr0 = (size_t)P.perm[r] * TB, pc0 = (size_t)P.perm[j] * TB;
+      if (mode == 1) copy_tile(In(set), S, lds, pr0, pc0);
+      else if (mode == 2) copy_tile(In(set), S, lds, pc0, pr0);
+      if (P.tcptr[t] < P.tcptr[t + 1]) {
+        const size_t pk0 = (size_t)P.perm[P.ck[P.tcptr[t]]] * TB;
+        copy_tile(Oa(set), S, lds, pr0, pk0);                 // L_rk
+        if (r != j) copy_tile(Ob(set), S, lds, pc0, pk0);     // L_jk
+      }
+      tile_commit();
+      return true;
+    };
+    bool fetched = false;   // the current task's tiles were issued by the previous one
+    int set = 0;
+    for (int e = P.p1ptr[lv * ranks + rank]; e < e_end; ++e, set ^= 1) {
       const int t = P.p1[e];
       const int r = P.tr[t], j = P.tc[t], mode = P.tmode[t] & 3;
       const size_t pr0 = (size_t)P.perm[r] * TB, pc0 = (size_t)P.perm[j] * TB;
@@ -582,24 +620,36 @@ __global__ void __launch_bounds__(256)
       __syncthreads();
       if (r == nt) {   // the rhs row: only row 0 of its tiles is nonzero, so each update is a GEMV
         rhs_update(pc0, t);
+        fetched = false;
         continue;
       }
-      if (mode == 1) load_tile(T2, S, lds, pr0, pc0);
-      else if (mode == 2) load_tile(T2, S, lds, pc0, pr0);
+      if (!fetched) issue(e, set);
+      fetched = false;
+      double* Ti = In(set);
+      double* Ta = Oa(set);
+      double* Tb = Ob(set);
       double acc[2][2][2][2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) acc_zero(acc[h]);
-      for (int u = P.tcptr[t]; u < P.tcptr[t + 1]; ++u) {
-        const size_t pk0 = (size_t)P.perm[P.ck[u]] * TB;
-        load_tile(T0, S, lds, pr0, pk0);                 // L_rk
-        if (!diag) load_tile(T1, S, lds, pc0, pk0);      // L_jk
+      const int u0 = P.tcptr[t], u1 = P.tcptr[t + 1];
+      if (u0 == u1) {   // no updates: wait for the input, then fetch the next task's tiles
         tile_wait();
         __syncthreads();
-        cta_gemm_abt_acc(acc, T0, false, diag ? T0 : T1);
+        if (e + 1 < e_end) fetched = issue(e + 1, set ^ 1);
+      }
+      for (int u = u0; u < u1; ++u) {
+        if (u > u0) {
+          const size_t pk0 = (size_t)P.perm[P.ck[u]] * TB;
+          copy_tile(Ta, S, lds, pr0, pk0);                 // L_rk
+          if (!diag) copy_tile(Tb, S, lds, pc0, pk0);      // L_jk
+          tile_commit();
+        }
+        tile_wait();       // only this task's copies are in flight here
+        __syncthreads();
+        if (u + 1 == u1 && e + 1 < e_end) fetched = issue(e + 1, set ^ 1);
+        cta_gemm_abt_acc(acc, Ta, false, diag ? Ta : Tb);
         __syncthreads();
       }
-      tile_wait();
-      __syncthreads();
       if (factor) {
 #pragma unroll
         for (int h = 0; h < 2; ++h)
@@ -608,12 +658,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int b = 0; b < 2; ++b)
 #pragma unroll
-              for (int i = 0; i < 2; ++i) T2[frag_col(h, b, i) * LDT + frag_row(a)] -= acc[h][a][b][i];
+              for (int i = 0; i < 2; ++i) Ti[frag_col(h, b, i) * LDT + frag_row(a)] -= acc[h][a][b][i];
         __syncthreads();
-        const bool ok = cta_factor_tile8(T2, T1);
+        const bool ok = cta_factor_tile8(Ti, Ta);   // Z into this set's first operand tile
         if (!ok && tid == 0) atomicExch(fail, 1);
         double* Z = ldiag + (size_t)j * TB * TB;
-        for (int f = tid; f < TB * TB; f += blockDim.x) Z[f] = T1[(f >> 6) * LDT + (f & 63)];
+        for (int f = tid; f < TB * TB; f += blockDim.x) Z[f] = Ta[(f >> 6) * LDT + (f & 63)];
       } else {
 #pragma unroll
         for (int h = 0; h < 2; ++h)
@@ -624,11 +674,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
                 const int row = frag_row(a), col = frag_col(h, b, i);
-                const double in = mode == 1 ? T2[col * LDT + row] : mode == 2 ? T2[row * LDT + col] : 0.0;
+                const double in = mode == 1 ? Ti[col * LDT + row] : mode == 2 ? Ti[row * LDT + col] : 0.0;
                 S[(pc0 + col) * lds + pr0 + row] = in - acc[h][a][b][i];
               }
       }
     }
+    tile_wait();   // nothing is in flight past the phase (no task is left to prefetch)
     cl.sync();   // arrive.release / wait.acquire at cluster scope: the CTAs' writes are visible
     stamp(2 * lv + 1);
     for (int e = P.p2ptr[lv * ranks + rank]; e < P.p2ptr[lv * ranks + rank + 1]; ++e) {
@@ -743,7 +794,7 @@ int chol_cluster_setup() {
   V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(3 * TB * LDT * sizeof(double))));
   V3DBA_CUDA_TRY(cudaFuncSetAttribute(k_chol_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(3 * TB * LDT * sizeof(double))));
+                                      (int)kLevelsSmem));
   done_mask.fetch_or(bit);
   return V3DBA_OK;
 }
@@ -784,7 +835,7 @@ int chol_levels_solve(const TileChol& tc, double* S, double* x, int* d_fail, cud
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(tc.lv_ranks, 1, 1);
   cfg.blockDim = dim3(256, 1, 1);
-  cfg.dynamicSmemBytes = 3 * TB * LDT * sizeof(double);
+  cfg.dynamicSmemBytes = kLevelsSmem;
   cfg.stream = st;
   cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -814,7 +865,7 @@ int chol_levels_ranks() {
     cudaGetLastError();
     return ranks;
   }
-  const size_t smem = 3 * TB * LDT * sizeof(double);
+  const size_t smem = kLevelsSmem;
   if (cudaFuncSetAttribute(k_chol_levels, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(16, 1, 1);
