@@ -117,3 +117,17 @@ def test_stereo_header_matches_reference(name):
     assert status == int(g["status"]) and iters == int(g["iterations"])
     assert param_rel((R, T, X), (g["R"], g["T"], g["X"])) < 1e-5
 
+
+
+POINTS_DEMO = os.path.join(ROOT, "tests", "shim", "_build", "points_demo")
+
+
+@pytest.mark.skipif(not os.path.exists(POINTS_DEMO), reason="points demo not built (needs the reference headers)")
+@pytest.mark.parametrize("seed", [1, 2])
+def test_dropin_bundle_point_structure_matches_reference_struct(seed):
+    """include/v3d_b200/v3d_bundlepoints.h against the reference's inline BundlePointStructure in
+    one C++ caller: identical members after the constructor (thresholds -1 .. 5, empty and long
+    tracks) and identical reconstructions after createPointStructure in both branches."""
+    r = subprocess.run([POINTS_DEMO, str(seed)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "0 failures" in r.stdout
