@@ -239,7 +239,8 @@ int v3dba_bundle_point_structure(int n_tracks, const int* track_ptr, const doubl
  * (n_measurements) are outputs and n_tracks is ignored.  from_scratch == 0: the n_tracks tracks
  * keep their measurement lists (track_ptr is an input); track xs_indices[i] gets position
  * points3d[i], and the measurements of the kept tracks, in order, get the positions
- * measurements[...] one after another (meas_view, meas_id unused). */
+ * measurements[...] one after another (meas_view, meas_id unused).  Arrays with nothing to
+ * read or write (no points, no measurements, no tracks) may be NULL. */
 int v3dba_create_point_structure(int from_scratch, int n_points, int n_measurements, const double* points3d,
                                  const double* measurements, const int* measurement_ids, const int* corresponding_view,
                                  const int* corresponding_point, const int* xs_indices, int n_tracks, int* track_ptr,

@@ -102,3 +102,20 @@ def test_invalid_inputs_are_rejected():
     with pytest.raises(capi.V3dbaError) as e:
         capi.create_point_structure(bps, from_scratch=True)
     assert e.value.code == capi.ERR_INVALID_INPUT
+
+
+def test_empty_write_back_accepts_null_arrays():
+    """A structure that kept no track (n_required above every track length, or negative) writes
+    back an empty reconstruction from scratch; the arrays with nothing to hold may be NULL, as
+    data() of an empty std::vector is."""
+    import ctypes as C
+    lib = capi.library()
+    ptr = np.full(1, -7, np.int32)
+    rc = lib.v3dba_create_point_structure(1, 0, 0, None, None, None, None, None, None, 0,
+                                          ptr.ctypes.data_as(C.POINTER(C.c_int)), None, None, None, None)
+    assert rc == capi.OK
+    assert ptr[0] == 0
+    # in place over zero tracks: nothing is read or written but track_ptr[0]
+    rc = lib.v3dba_create_point_structure(0, 0, 0, None, None, None, None, None, None, 0,
+                                          ptr.ctypes.data_as(C.POINTER(C.c_int)), None, None, None, None)
+    assert rc == capi.OK

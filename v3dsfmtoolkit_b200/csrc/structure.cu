@@ -658,8 +658,11 @@ extern "C" int v3dba_create_point_structure(int from_scratch, int n_points, int 
                                             const int* corresponding_view, const int* corresponding_point,
                                             const int* xs_indices, int n_tracks, int* track_ptr, double* track_pos,
                                             int* meas_view, int* meas_id, float* meas_pos) {
-  if (n_points < 0 || n_measurements < 0 || !track_ptr || !track_pos) return V3DBA_ERR_INVALID_ARGUMENT;
+  if (n_points < 0 || n_measurements < 0 || !track_ptr) return V3DBA_ERR_INVALID_ARGUMENT;
   if ((n_points && !points3d) || (n_measurements && !measurements)) return V3DBA_ERR_INVALID_ARGUMENT;
+  // track_pos is written for the n_points new tracks (from scratch) or the n_tracks existing ones
+  // (in place); with none it may be NULL, as data() of an empty vector is
+  if (!track_pos && (from_scratch ? n_points > 0 : n_tracks > 0)) return V3DBA_ERR_INVALID_ARGUMENT;
   NvtxRange nvtx("v3dba_create_point_structure");
   CallScope cs;
   V3DBA_CUDA_TRY(cudaStreamCreateWithFlags(&cs.st, cudaStreamNonBlocking));
