@@ -68,9 +68,10 @@ struct DevState {
   ParamSet cur, trial, init;
   // per-observation (8-byte slots; FP32 mode uses the first half of each array)
   void* o_A = nullptr;      // 2*DA
-  void* o_W = nullptr;      // DA*3   W_k = A_k^T B_k
   void* o_C = nullptr;      // 2*DC
-  void* o_T = nullptr;      // DA*3   T_k = W_k Vinv_j
+  float* o_W = nullptr;     // DA*3   W_k = A_k^T B_k (FP32 blocks only)
+  float* o_T = nullptr;     // DA*3   T_k = W_k Vinv_j (FP32 blocks only)
+  double* o_B = nullptr;    // 2*3    B_k (FP64 blocks only; W and T are applied factor by factor)
   double* o_ga = nullptr;   // DA     A_k^T r_k (FP64)
   double* o_w = nullptr;    // Huber weights of the last linearisation
   // per point

@@ -7,6 +7,13 @@
 // `Real` (float in mixed mode, double in FP64 mode); their sums are taken in FP64, except the
 // camera-pair Schur sums of the mixed mode, which accumulate in FP32.  All reductions run in a
 // fixed order (no floating-point atomics), so results are bit-reproducible run to run.
+//
+// Per-observation storage differs by precision.  FP32 blocks store the products W_k = A_k^T B_k
+// and T_k = W_k Vinv_j (two 4-byte 6x3 blocks), which the Schur, rhs and back-substitution
+// kernels gather.  FP64 blocks store B_k instead (2x3) and apply W_k and T_k factor by factor
+// (W_k x = A_k^T (B_k x), T_k^T y = Vinv_j B_k^T (A_k y)): the linearisation writes 96 bytes less
+// per observation and the point elimination writes no per-observation block at all, against
+// 126 instead of 108 FMAs and one more point-block gather per Schur pair.
 #include <algorithm>
 #include <cstdio>
 
@@ -171,6 +178,11 @@ __device__ __forceinline__ T group_sum(T v) {
   return v;
 }
 
+// FP32 blocks store W_k and T_k per observation; FP64 blocks store B_k (see the file header).
+template <typename Real>
+__host__ __device__ constexpr bool stores_products() { return sizeof(Real) == 4; }
+constexpr int kSB = 8;   // stride of B_k (2 x 3 row-major) in doubles
+
 template <int DC>
 struct RelinNV {
   static constexpr int NZ = nsym(DC);
@@ -207,7 +219,6 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
   if (j < D.M) {
     const double X[3] = {s.cur.X[3 * j], s.cur.X[3 * j + 1], s.cur.X[3 * j + 2]};
     Real* oA = reinterpret_cast<Real*>(s.o_A);
-    Real* oW = reinterpret_cast<Real*>(s.o_W);
     Real* oC = reinterpret_cast<Real*>(s.o_C);
     k0 = s.p_ptr[j];
     k1 = s.p_ptr[j + 1];
@@ -243,14 +254,25 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
 #pragma unroll
           for (int q = 0; q < DA; ++q) a[r * DA + q] = Real(A[r][q]);
         vstore(oA + (size_t)k * L::SA, a);
-        Real wv[L::SW];
+        if constexpr (stores_products<Real>()) {
+          float wv[L::SW];
 #pragma unroll
-        for (int t = 0; t < L::SW; ++t) wv[t] = Real(0);
+          for (int t = 0; t < L::SW; ++t) wv[t] = 0.f;
 #pragma unroll
-        for (int q = 0; q < DA; ++q)
+          for (int q = 0; q < DA; ++q)
 #pragma unroll
-          for (int b = 0; b < 3; ++b) wv[q * 3 + b] = Real(A[0][q] * B[0][b] + A[1][q] * B[1][b]);
-        vstore(oW + (size_t)k * L::SW, wv);
+            for (int b = 0; b < 3; ++b) wv[q * 3 + b] = float(A[0][q] * B[0][b] + A[1][q] * B[1][b]);
+          vstore(s.o_W + (size_t)k * L::SW, wv);
+        } else {
+          double bv[kSB];
+#pragma unroll
+          for (int t = 0; t < kSB; ++t) bv[t] = 0.0;
+#pragma unroll
+          for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) bv[r * 3 + b] = B[r][b];
+          vstore(s.o_B + (size_t)k * kSB, bv);
+        }
         if (DC > 0) {
           Real cv[L::SC];
 #pragma unroll
@@ -497,8 +519,8 @@ __device__ __forceinline__ bool inv3(const double a[6], double o[6]) {
   return true;
 }
 
-// One thread per point: Vinv_j = (V_j + lambda I)^-1, q_j = Vinv gb, Vinv Y_j and
-// T_k = W_k Vinv_j for its observations; Y^T Vinv Y and Y^T q go to per-block partials.
+// One thread per point: Vinv_j = (V_j + lambda I)^-1, q_j = Vinv gb, Vinv Y_j and, with FP32
+// blocks, T_k = W_k Vinv_j for its observations; Y^T Vinv Y and Y^T q go to per-block partials.
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
@@ -561,21 +583,21 @@ __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, doub
       for (int c = 0; c < DCc; ++c)
         v[nsym(DC) + c] = double(yv[c]) * q[0] + double(yv[DCc + c]) * q[1] + double(yv[2 * DCc + c]) * q[2];
     }
-    const Real* oW = reinterpret_cast<const Real*>(s.o_W);
-    Real* oT = reinterpret_cast<Real*>(s.o_T);
-    for (int k = s.p_ptr[j]; k < s.p_ptr[j + 1]; ++k) {
-      Real w[L::SW];
-      vload(oW + (size_t)k * L::SW, w);
-      Real t[L::SW];
+    if constexpr (stores_products<Real>()) {
+      for (int k = s.p_ptr[j]; k < s.p_ptr[j + 1]; ++k) {
+        float w[L::SW];
+        vload(s.o_W + (size_t)k * L::SW, w);
+        float t[L::SW];
 #pragma unroll
-      for (int x = 0; x < L::SW; ++x) t[x] = Real(0);
+        for (int x = 0; x < L::SW; ++x) t[x] = 0.f;
 #pragma unroll
-      for (int r = 0; r < DA; ++r)
+        for (int r = 0; r < DA; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-          t[r * 3 + c] = Real(double(w[r * 3]) * vi[s3(0, c)] + double(w[r * 3 + 1]) * vi[s3(1, c)] +
-                              double(w[r * 3 + 2]) * vi[s3(2, c)]);
-      vstore(oT + (size_t)k * L::SW, t);
+          for (int c = 0; c < 3; ++c)
+            t[r * 3 + c] = float(double(w[r * 3]) * vi[s3(0, c)] + double(w[r * 3 + 1]) * vi[s3(1, c)] +
+                                 double(w[r * 3 + 2]) * vi[s3(2, c)]);
+        vstore(s.o_T + (size_t)k * L::SW, t);
+      }
     }
   }
   block_reduce<NV, NV>(v, red);
@@ -585,7 +607,8 @@ __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, doub
   }
 }
 
-// One warp per chunk of a camera-pair block's observation pairs: partial sum T_k W_m^T.
+// One warp per chunk of a camera-pair block's observation pairs: partial sum T_k W_m^T (FP32
+// blocks: the stored T_k and W_m; FP64 blocks: A_k^T (B_k Vinv_j B_m^T) A_m).
 template <int DA, typename Real>
 __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
@@ -598,13 +621,45 @@ __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __rest
   Real acc[SV::VP];
 #pragma unroll
   for (int t = 0; t < SV::VP; ++t) acc[t] = Real(0);
-  const Real* oT = reinterpret_cast<const Real*>(s.o_T);
-  const Real* oW = reinterpret_cast<const Real*>(s.o_W);
-  // FP32 blocks: a lane takes its pairs p and p + 32 in one trip, so both pairs' gathers are in
-  // flight together (same summation order as one pair per trip); FP64 blocks keep one pair per
-  // trip, which already fills the register file (as do the 13-unknown FP32 blocks).
-  constexpr int U = sizeof(Real) == 4 && DA <= 11 ? 2 : 1;
   const int end = s.bc_end[ch];
+  if constexpr (!stores_products<Real>()) {
+    // FP64 blocks: T_k W_m^T = A_k^T (B_k Vinv_j B_m^T) A_m, 126 FMAs per pair
+    const double* oA = reinterpret_cast<const double*>(s.o_A);
+    for (int p = s.bc_beg[ch] + lane; p < end; p += 32) {
+      const int k = s.pr_k[p], m = s.pr_m[p];
+      const int j = s.o_pt[k];
+      double Ak[L::SA], Am[L::SA], Bk[kSB], Bm[kSB], vi[8];
+      vload(oA + (size_t)k * L::SA, Ak);
+      vload(s.o_B + (size_t)k * kSB, Bk);
+      vload(oA + (size_t)m * L::SA, Am);
+      vload(s.o_B + (size_t)m * kSB, Bm);
+      vload(reinterpret_cast<const double*>(s.p_Vinv) + (size_t)j * L::SV, vi);
+      double Q[2][3];   // B_k Vinv_j
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          Q[r][c] = Bk[3 * r] * vi[s3(0, c)] + Bk[3 * r + 1] * vi[s3(1, c)] + Bk[3 * r + 2] * vi[s3(2, c)];
+      double Mx[2][2];  // B_k Vinv_j B_m^T
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int t = 0; t < 2; ++t) Mx[r][t] = Q[r][0] * Bm[3 * t] + Q[r][1] * Bm[3 * t + 1] + Q[r][2] * Bm[3 * t + 2];
+#pragma unroll
+      for (int c = 0; c < DA; ++c) {
+        const double n0 = Mx[0][0] * Am[c] + Mx[0][1] * Am[DA + c];
+        const double n1 = Mx[1][0] * Am[c] + Mx[1][1] * Am[DA + c];
+#pragma unroll
+        for (int a = 0; a < DA; ++a) acc[a * DA + c] += Ak[a] * n0 + Ak[DA + a] * n1;
+      }
+    }
+  } else {
+  const float* oT = s.o_T;
+  const float* oW = s.o_W;
+  // FP32 blocks: a lane takes its pairs p and p + 32 in one trip, so both pairs' gathers are in
+  // flight together (same summation order as one pair per trip), except with 13 unknowns per
+  // camera, whose blocks already fill the register file.
+  constexpr int U = DA <= 11 ? 2 : 1;
   for (int p = s.bc_beg[ch] + lane; p < end; p += 32 * U) {
     int k[U], m[U];
 #pragma unroll
@@ -613,7 +668,7 @@ __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __rest
       k[u] = s.pr_k[q];
       m[u] = s.pr_m[q];
     }
-    Real t[U][L::SW], w[U][L::SW];
+    float t[U][L::SW], w[U][L::SW];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       vload(oT + (size_t)k[u] * L::SW, t[u]);
@@ -629,6 +684,7 @@ __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __rest
           acc[a * DA + c] += t[u][a * 3] * w[u][c * 3] + t[u][a * 3 + 1] * w[u][c * 3 + 1] +
                              t[u][a * 3 + 2] * w[u][c * 3 + 2];
     }
+  }
   }
   warp_reduce_transpose(acc);
 #pragma unroll
@@ -674,7 +730,7 @@ __global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* 
 }
 
 // One warp per chunk of a camera's observations: partial sum_k W_k q_j(k) and sum_k T_k Y_j(k),
-// the latter as sum_k W_k (Vinv Y)_j(k).
+// the latter as sum_k W_k (Vinv Y)_j(k) (FP64 blocks: W_k x as A_k^T (B_k x)).
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
@@ -688,14 +744,35 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, doubl
   double acc[RV::VP];
 #pragma unroll
   for (int t = 0; t < RV::VP; ++t) acc[t] = 0.0;
-  const Real* oW = reinterpret_cast<const Real*>(s.o_W);
   for (int idx = s.cc_beg[ch] + lane; idx < s.cc_end[ch]; idx += 32) {
     const int k = s.c_obs[idx];
     const int j = s.o_pt[k];
-    Real w[L::SW];
-    vload(oW + (size_t)k * L::SW, w);
     double q[4];
     vload(s.p_q + (size_t)j * 4, q);
+    if constexpr (!stores_products<Real>()) {
+      // W_k x = A_k^T (B_k x)
+      double A[L::SA], B[kSB];
+      vload(reinterpret_cast<const double*>(s.o_A) + (size_t)k * L::SA, A);
+      vload(s.o_B + (size_t)k * kSB, B);
+      const double bq0 = B[0] * q[0] + B[1] * q[1] + B[2] * q[2];
+      const double bq1 = B[3] * q[0] + B[4] * q[1] + B[5] * q[2];
+#pragma unroll
+      for (int a = 0; a < DA; ++a) acc[a] += A[a] * bq0 + A[DA + a] * bq1;
+      if (DC > 0) {
+        double yv[L::SY];
+        vload(reinterpret_cast<const double*>(s.p_YV) + (size_t)j * L::SY, yv);
+#pragma unroll
+        for (int c = 0; c < DCc; ++c) {
+          const double by0 = B[0] * yv[c] + B[1] * yv[DCc + c] + B[2] * yv[2 * DCc + c];
+          const double by1 = B[3] * yv[c] + B[4] * yv[DCc + c] + B[5] * yv[2 * DCc + c];
+#pragma unroll
+          for (int a = 0; a < DA; ++a) acc[DA + a * DCc + c] += A[a] * by0 + A[DA + a] * by1;
+        }
+      }
+      continue;
+    }
+    float w[L::SW];
+    vload(s.o_W + (size_t)k * L::SW, w);
 #pragma unroll
     for (int a = 0; a < DA; ++a) acc[a] += double(w[a * 3]) * q[0] + double(w[a * 3 + 1]) * q[1] + double(w[a * 3 + 2]) * q[2];
     if (DC > 0) {
@@ -791,7 +868,8 @@ __global__ void __launch_bounds__(256) k_global_block(DevState s, const double* 
 
 // ---- trial step ----------------------------------------------------------------------------
 
-// One thread per point: db_j = q_j - sum_k T_k^T da_i(k) - (Vinv Y_j) dc; X' = X + db.
+// G lanes per point: db_j = q_j - sum_k T_k^T da_i(k) - (Vinv Y_j) dc; X' = X + db.  With FP64
+// blocks the sum is Vinv_j sum_k B_k^T (A_k da_i(k)).
 template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
@@ -808,17 +886,32 @@ __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double
   double acc[3] = {0, 0, 0};
   const double* x = s.x;
   if (active) {
-    // this lane's share of sum_k T_k^T dc_i over the track
-    const Real* oT = reinterpret_cast<const Real*>(s.o_T);
+    // this lane's share of sum_k T_k^T dc_i over the track (FP64 blocks: of sum_k B_k^T A_k dc_i,
+    // multiplied by Vinv_j below)
     for (int k = s.p_ptr[j] + lig; k < s.p_ptr[j + 1]; k += G) {
       const int i = s.o_cam[k];
-      Real t[L::SW];
-      vload(oT + (size_t)k * L::SW, t);
+      if constexpr (stores_products<Real>()) {
+        float t[L::SW];
+        vload(s.o_T + (size_t)k * L::SW, t);
 #pragma unroll
-      for (int a = 0; a < DA; ++a) {
-        const double da = x[i * DA + a];
+        for (int a = 0; a < DA; ++a) {
+          const double da = x[i * DA + a];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[c] += double(t[a * 3 + c]) * da;
+          for (int c = 0; c < 3; ++c) acc[c] += double(t[a * 3 + c]) * da;
+        }
+      } else {
+        double A[L::SA], B[kSB];
+        vload(reinterpret_cast<const double*>(s.o_A) + (size_t)k * L::SA, A);
+        vload(s.o_B + (size_t)k * kSB, B);
+        double ad0 = 0.0, ad1 = 0.0;
+#pragma unroll
+        for (int a = 0; a < DA; ++a) {
+          const double da = x[i * DA + a];
+          ad0 += A[a] * da;
+          ad1 += A[DA + a] * da;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] += B[c] * ad0 + B[3 + c] * ad1;
       }
     }
   }
@@ -829,6 +922,13 @@ __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double
     if (active) {
       double q[4];
       vload(s.p_q + (size_t)j * 4, q);
+      if constexpr (!stores_products<Real>()) {
+        double vi[8];
+        vload(reinterpret_cast<const double*>(s.p_Vinv) + (size_t)j * L::SV, vi);
+        const double a0 = acc[0], a1 = acc[1], a2 = acc[2];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) acc[r] = vi[s3(r, 0)] * a0 + vi[s3(r, 1)] * a1 + vi[s3(r, 2)] * a2;
+      }
       if (DC > 0) {
         Real yv[L::SY];
         vload(reinterpret_cast<const Real*>(s.p_YV) + (size_t)j * L::SY, yv);

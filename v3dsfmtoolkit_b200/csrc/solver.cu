@@ -469,9 +469,10 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   const int SX = (dA * std::max(dC, 1) + 3) & ~3;
   double* tmp;
   TRY(dalloc(h, &tmp, Kz * SA)); s.o_A = tmp;
-  TRY(dalloc(h, &tmp, Kz * SW)); s.o_W = tmp;
   TRY(dalloc(h, &tmp, dC ? Kz * SC : 4)); s.o_C = tmp;
-  TRY(dalloc(h, &tmp, Kz * SW)); s.o_T = tmp;
+  TRY(dalloc(h, &s.o_W, Kz * SW));   // FP32 blocks
+  TRY(dalloc(h, &s.o_T, Kz * SW));
+  TRY(dalloc(h, &s.o_B, Kz * 8));    // FP64 blocks
   TRY(dalloc(h, &s.o_ga, Kz * SG));
   TRY(dalloc(h, &s.o_w, Kz));
   TRY(dalloc(h, &tmp, Mz * 8)); s.p_V = tmp;
