@@ -9,12 +9,14 @@ baselines barely fix).  Its final parameters there are not a property of the pro
 path: the reference started with tau * (1 + 1e-12) instead of tau ends with the same cost to
 2e-8 but points 2e-3 apart (relative to the scene's extent), and with tau * (1 + 2e-12) on
 another path (31 rejected steps instead of 23), 2.3e-5 above in cost and 0.7 apart in points.
-So the comparisons here are:
+The reference's spread is estimated from its own runs with tau * (1 + k * 1e-12), k = 1 .. 7 (a
+handful of samples of a chaotic path: fewer would understate it).  So the comparisons here are:
   * the first iterations, where the two implementations take the same accept / reject
     decisions: cost and parameters to tight tolerances;
   * the 100-iteration run and the runs that stop on the reference's final cost: same status,
     cost within the spread of the reference's own tau-perturbed runs, and gauge-aligned
-    parameters no further from the reference's than the reference's own perturbed runs are.
+    parameters no further from the nearest of the reference's end states than the reference's
+    own perturbed runs are from its unperturbed one.
 """
 import json
 import multiprocessing as mp
@@ -44,15 +46,18 @@ def _reference_run(args):
                                            "n_rejected": info["n_rejected"]}
 
 
+N_PERTURBED = 8   # the reference's own runs with tau * (1 + k * 1e-12), k = 0 .. N_PERTURBED - 1
+
+
 @pytest.fixture(scope="module")
 def reference_runs():
     from oracle.bindings import reference_available
     if not reference_available():
         pytest.skip("compiled reference not present")
-    jobs = [(k, 100) for k in range(4)] + [(0, PREFIX_ITERATIONS)]
-    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+    jobs = [(k, 100) for k in range(N_PERTURBED)] + [(0, PREFIX_ITERATIONS)]
+    with mp.get_context("spawn").Pool(min(len(jobs), max(os.cpu_count() or 1, 1))) as pool:
         out = pool.map(_reference_run, jobs)
-    return {"perturbed": out[:4], "prefix": out[4]}
+    return {"perturbed": out[:N_PERTURBED], "prefix": out[N_PERTURBED]}
 
 
 @pytest.fixture(scope="module")
@@ -60,6 +65,12 @@ def scene():
     sc = scenes.sequence_scene()
     ref = json.load(open(os.path.join(GOLDEN, "bench_reference.json")))["sequence200"]
     return sc, ref
+
+
+def _nearest_reference(p, runs):
+    """Gauge-aligned distance from p to the nearest of the reference's own end states (its runs
+    under a 1e-12 change of tau end in several places of the nearly flat valley)."""
+    return min(_aligned_error(p, q) for q, _, _ in runs)
 
 
 def _aligned_error(p, q):
@@ -98,7 +109,8 @@ def test_100_iterations_within_the_reference_spread(reference_runs, scene):
     """FP64 and mixed precision, 100 iterations: the reference's status (TIMEOUT), the cost no
     higher than the highest of the reference's tau-perturbed runs (1e-6) and not far below the
     lowest (a lower cost is a better minimum, so 1e-5 there), the gauge-aligned parameters no
-    further from the reference's run than its own perturbed runs."""
+    further from the nearest of the reference's runs than its perturbed runs are from its
+    unperturbed one."""
     sc, _ = scene
     runs = reference_runs["perturbed"]
     p0, c0, i0 = runs[0]
@@ -110,7 +122,7 @@ def test_100_iterations_within_the_reference_spread(reference_runs, scene):
         h.reset_params()
         r = h.minimize(max_iterations=100, precision=precision)
         c = h.cost()
-        err = _aligned_error(h.get_params(), p0)
+        err = _nearest_reference(h.get_params(), runs)
         print(f"precision {precision}: cost {(c - c0) / c0:+.3e} rel, rejections {r.n_rejected} "
               f"(reference {i0['n_rejected']}), aligned parameters {err:.3e} (reference spread {spread:.3e})")
         assert r.status == i0["status"] == capi.STATUS_TIMEOUT
@@ -122,7 +134,8 @@ def test_100_iterations_within_the_reference_spread(reference_runs, scene):
 def test_runs_to_the_reference_cost(reference_runs, scene):
     """The bench's step: minimize() until the reference's final cost (1e-6 relative), tau scaled by
     1 + k * 1e-12.  At least 6 of 8 runs in each precision reach it; their parameters are no
-    further (gauge-aligned) from the reference's than its own perturbed runs.  A run that stops
+    further (gauge-aligned) from the nearest of the reference's runs than its perturbed runs are
+    from its unperturbed one.  A run that stops
     with SMALL_UPDATE instead has entered a region where the reference's LM stalls as well: the
     reference started from that run's parameters also ends with SMALL_UPDATE without reaching
     the cost."""
@@ -141,8 +154,12 @@ def test_runs_to_the_reference_cost(reference_runs, scene):
             params = h.get_params()
             if r.reached_stop_cost:
                 reached += 1
+                err = _nearest_reference(params, runs)
+                print(f"precision {precision} k {k}: reached in {r.iterations} iterations, aligned parameters "
+                      f"{err:.3e} from the nearest reference run, {_aligned_error(params, p0):.3e} from the "
+                      f"unperturbed one (reference spread {spread:.3e})")
                 assert h.cost() <= target
-                assert _aligned_error(params, p0) <= spread
+                assert err <= spread
             else:
                 assert r.status == capi.STATUS_SMALL_UPDATE
                 assert h.cost() <= c0 * (1 + 1e-3)
