@@ -94,8 +94,10 @@ def parse_args():
                                            "cluster2000", "rotations10000"],
                     default="sequence200")
     ap.add_argument("--profile-stages", type=int, default=0, metavar="R",
-                    help="run every stage of one LM iteration R times (mixed precision) and exit; "
+                    help="run every stage of one LM iteration R times and exit; "
                          "the small, fixed launch sequence that ncu captures are taken on")
+    ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed",
+                    help="block precision of --profile-stages")
     return ap.parse_args()
 
 
@@ -104,7 +106,8 @@ def run_profile_stages(args):
     from v3dsfmtoolkit_b200 import capi
     torch.cuda.set_device(0)
     h = capi.Handle.from_scene(make_scene())
-    print(json.dumps(h.profile_stages(capi.PRECISION_MIXED, reps=args.profile_stages)), flush=True)
+    prec = capi.PRECISION_FP64 if args.profile_precision == "fp64" else capi.PRECISION_MIXED
+    print(json.dumps(h.profile_stages(prec, reps=args.profile_stages)), flush=True)
     h.close()
 
 
