@@ -40,7 +40,6 @@ namespace {
 constexpr int TB = 64;
 constexpr int LDT = 68;          // shared leading dimension (bank-conflict free DMMA fragments)
 constexpr int kCluster = 8;
-constexpr unsigned FULL = 0xffffffffu;
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -166,7 +165,7 @@ __device__ __noinline__ bool warp_chol_inv8(const double* D, double* Zd) {
 // the 64x64 tile A (shared, col-major LDT, lower triangle valid; A is overwritten).  Blocked by
 // 8 columns with lookahead: warp 0 carries the chain of diagonal blocks (the update of the next
 // diagonal block by the panel just formed, then its inverse factor, warp_chol_inv8) while warps
-// 1..7 apply the other trailing updates (A_ij -= L_ip L_jp^T) and form block row p of Z
+// 1..3 and 5..7 apply the other trailing updates (A_ij -= L_ip L_jp^T) and form block row p of Z
 // (Z_pj = -Z_pp sum_{t=j}^{p-1} L_pt Z_tj); the panel blocks L_ip = A_ip Z_pp^T are formed by the
 // first warps between.  All products are 8x8 DMMA blocks.  Returns false on a non-positive pivot.
 __device__ bool cta_factor_tile8(double* A, double* Zs) {
@@ -203,14 +202,17 @@ __device__ bool cta_factor_tile8(double* A, double* Zs) {
         __syncwarp();
         if (!warp_chol_inv8(A + 8 * q1 * LDT + 8 * q1, Zs + 8 * q1 * LDT + 8 * q1) && (tid & 31) == 0) s_ok8 = 0;
       }
-    } else {
-      // Tasks of this iteration, dealt to warps 1..7 in turn: first the trailing blocks (i, j),
-      // p+1 <= j <= i < 8, other than (p+1, p+1) (the lower triangle of the trailing block matrix
-      // numbered row by row: u -> (ii, jj), ii(ii+1)/2 <= u < (ii+1)(ii+2)/2), then block row p of
-      // Z.  Each warp steps straight to its own tasks.
+    } else if (w != 4) {
+      // Tasks of this iteration, dealt in turn to warps 1..7 except 4 (which shares warp 0's
+      // scheduler partition: kept free of DMMA work, the pivot chain runs ~15 % faster): first
+      // the trailing blocks (i, j), p+1 <= j <= i < 8, other than (p+1, p+1) (the lower triangle
+      // of the trailing block matrix numbered row by row: u -> (ii, jj), ii(ii+1)/2 <= u <
+      // (ii+1)(ii+2)/2), then block row p of Z.  Each warp steps straight to its own tasks.
+      constexpr int NW = 6;
+      const int slot = w < 4 ? w - 1 : w - 2;
       const int m = 7 - p;
       const int n_upd = m * (m + 1) / 2 - 1;
-      for (int k = w - 1; k < n_upd; k += 7) {
+      for (int k = slot; k < n_upd; k += NW) {
         const int u = k + 1;
         int ii = 0;
         while ((ii + 1) * (ii + 2) / 2 <= u) ++ii;
@@ -219,7 +221,7 @@ __device__ bool cta_factor_tile8(double* A, double* Zs) {
         warp_mma8(acc, A + 8 * p * LDT + 8 * i, 1, LDT, A + 8 * p * LDT + 8 * j, LDT, 1, 8);
         acc_store8(acc, A + 8 * j * LDT + 8 * i, LDT, -1.0, 1.0);
       }
-      for (int j = ((w - 1 - n_upd) % 7 + 7) % 7; j < p; j += 7) {
+      for (int j = ((slot - n_upd) % NW + NW) % NW; j < p; j += NW) {
         double acc[2] = {0.0, 0.0};
         for (int t = j; t < p; ++t)
           warp_mma8(acc, A + 8 * t * LDT + 8 * p, 1, LDT, Zs + 8 * j * LDT + 8 * t, 1, LDT, 8);
@@ -262,6 +264,22 @@ __device__ __forceinline__ void cta_gemm_abt_acc(double (&acc)[2][2][2][2], cons
     const int bj = 2 * (w & 1) + h;
     if (a_t) warp_mma16(acc[h], A + 16 * bi * LDT, LDT, 1, B + 16 * bj, LDT, 1, TB);
     else warp_mma16(acc[h], A + 16 * bi, 1, LDT, B + 16 * bj, LDT, 1, TB);
+  }
+}
+
+// The lower triangle of a symmetric update: the 10 16x16 blocks (bi >= bj) of acc += A A^T, two
+// per warp at most and 3 / 3 / 2 / 2 per scheduler partition (warp w runs on partition w % 4)
+// instead of 4 each for the full tile.  kLowerBlk[w][h] = 4 bi + bj, or -1.  Each element is
+// summed in the same order as by cta_gemm_abt_acc, so its lower triangle is the same bits.
+__constant__ signed char kLowerBlk[8][2] = {{0, 4}, {8, 9}, {12, 13}, {14, 15}, {5, -1}, {10, -1}, {-1, -1}, {-1, -1}};
+__device__ __forceinline__ void cta_gemm_aat_lower_acc(double (&acc)[2][2][2][2], const double* A) {
+  const int w = threadIdx.x >> 5;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int b = kLowerBlk[w][h];
+    if (b < 0) continue;
+    const int bi = b >> 2, bj = b & 3;
+    warp_mma16(acc[h], A + 16 * bi, 1, LDT, A + 16 * bj, LDT, 1, TB);
   }
 }
 
@@ -649,18 +667,35 @@ __global__ void __launch_bounds__(256)
         tile_wait();       // only this task's copies are in flight here
         __syncthreads();
         if (u + 1 == u1 && e + 1 < e_end) fetched = issue(e + 1, set ^ 1);
-        cta_gemm_abt_acc(acc, Ta, false, diag ? Ta : Tb);
+        if (diag) cta_gemm_aat_lower_acc(acc, Ta);   // only the lower triangle of a diagonal tile is read
+        else cta_gemm_abt_acc(acc, Ta, false, Tb);
         __syncthreads();
       }
+      // the 16x16 block (bi, bj) of fragment set h: the full ownership of cta_gemm_abt_acc, or
+      // the lower-triangle table of cta_gemm_aat_lower_acc on a diagonal tile
+      auto blk = [&](int h, int& bi, int& bj) -> bool {
+        if (!diag) {
+          bi = w >> 1;
+          bj = 2 * (w & 1) + h;
+          return true;
+        }
+        const int b = kLowerBlk[w][h];
+        bi = b >> 2;
+        bj = b & 3;
+        return b >= 0;
+      };
       if (factor) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < 2; ++h) {
+          int bi, bj;
+          if (!blk(h, bi, bj)) continue;
 #pragma unroll
           for (int a = 0; a < 2; ++a)
 #pragma unroll
             for (int b = 0; b < 2; ++b)
 #pragma unroll
-              for (int i = 0; i < 2; ++i) Ti[frag_col(h, b, i) * LDT + frag_row(a)] -= acc[h][a][b][i];
+              for (int i = 0; i < 2; ++i) Ti[(16 * bj + 8 * b + 2 * q + i) * LDT + 16 * bi + 8 * a + g] -= acc[h][a][b][i];
+        }
         __syncthreads();
         const bool ok = cta_factor_tile8(Ti, Ta);   // Z into this set's first operand tile
         if (!ok && tid == 0) atomicExch(fail, 1);
@@ -668,17 +703,20 @@ __global__ void __launch_bounds__(256)
         for (int f = tid; f < TB * TB; f += blockDim.x) Z[f] = Ta[(f >> 6) * LDT + (f & 63)];
       } else {
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < 2; ++h) {
+          int bi, bj;
+          if (!blk(h, bi, bj)) continue;
 #pragma unroll
           for (int a = 0; a < 2; ++a)
 #pragma unroll
             for (int b = 0; b < 2; ++b)
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
-                const int row = frag_row(a), col = frag_col(h, b, i);
+                const int row = 16 * bi + 8 * a + g, col = 16 * bj + 8 * b + 2 * q + i;
                 const double in = mode == 1 ? Ti[col * LDT + row] : mode == 2 ? Ti[row * LDT + col] : 0.0;
                 S[(pc0 + col) * lds + pr0 + row] = in - acc[h][a][b][i];
               }
+        }
       }
     }
     tile_wait();   // nothing is in flight past the phase (no task is left to prefetch)
