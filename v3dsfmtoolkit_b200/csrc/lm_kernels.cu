@@ -28,17 +28,24 @@ namespace v3dba {
 __host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
 __host__ __device__ constexpr int nsym(int n) { return n * (n + 1) / 2; }
 
-template <int DA, int DC>
+// x elements of T rounded up to whole 16-byte vectors (4 floats, 2 doubles).
+template <typename T>
+__host__ __device__ constexpr int vround(int x) {
+  return sizeof(T) == 4 ? (x + 3) & ~3 : (x + 1) & ~1;
+}
+
+// Strides of the blocks stored in `Real`, in whole 16-byte vectors.
+template <int DA, int DC, typename Real = float>
 struct Lay {
   static constexpr int DCc = DC > 0 ? DC : 1;
-  static constexpr int SA = round4(2 * DA);      // A_k, Real
-  static constexpr int SW = round4(3 * DA);      // W_k / T_k, Real
-  static constexpr int SC = round4(2 * DCc);     // C_k, Real
-  static constexpr int SG = (DA + 1) & ~1;       // A_k^T r_k, double
-  static constexpr int SV = 8;                   // V_j / Vinv_j upper triangle, Real
-  static constexpr int SY = round4(3 * DCc);     // Y_j / Vinv_j Y_j, Real
-  static constexpr int SU = round4(DA * DA);     // U_i, Real
-  static constexpr int SX = round4(DA * DCc);    // X_i, Real
+  static constexpr int SA = vround<Real>(2 * DA);    // A_k, Real
+  static constexpr int SW = round4(3 * DA);          // W_k / T_k, float (FP32 blocks only)
+  static constexpr int SC = vround<Real>(2 * DCc);   // C_k, Real
+  static constexpr int SG = (DA + 1) & ~1;           // A_k^T r_k, double
+  static constexpr int SV = vround<Real>(6);         // V_j / Vinv_j upper triangle, Real
+  static constexpr int SY = vround<Real>(3 * DCc);   // Y_j / Vinv_j Y_j, Real
+  static constexpr int SU = vround<Real>(DA * DA);   // U_i, Real
+  static constexpr int SX = vround<Real>(DA * DCc);  // X_i, Real
   static constexpr int NZ = nsym(DC);
 };
 
@@ -81,20 +88,36 @@ __device__ __forceinline__ void vstore(double* p, const double (&v)[N]) {
   for (int t = 0; t < N / 2; ++t) q[t] = make_double2(v[2 * t], v[2 * t + 1]);
 }
 
-// Deterministically folds `nblk` rows of NV partials (first NS summed, the rest maxed) with
-// one block; result in out[0..NV) of thread 0.
+// Deterministically folds the NV per-block partials of `nblk` blocks (first NS summed, the rest
+// maxed), stored value-major: part[t * nblk + b] (see store_partials).  Warp w folds values w,
+// w + nwarps, ...: lane l reads blocks l, l + 32, ... in order (coalesced), then a fixed shuffle
+// tree.  Every thread receives the results in out[0..NV); smem needs NV doubles.
 template <int NV, int NS>
 __device__ void fold_partials(const double* __restrict__ part, int nblk, double (&out)[NV], double* smem) {
-#pragma unroll
-  for (int t = 0; t < NV; ++t) out[t] = (t < NS) ? 0.0 : -1e30;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-#pragma unroll
-    for (int t = 0; t < NV; ++t) {
-      const double u = part[(size_t)b * NV + t];
-      out[t] = (t < NS) ? out[t] + u : fmax(out[t], u);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int t = wid; t < NV; t += nw) {
+    const bool sum = t < NS;
+    double acc = sum ? 0.0 : -1e30;
+    for (int b = lane; b < nblk; b += 32) {
+      const double u = part[(size_t)t * nblk + b];
+      acc = sum ? acc + u : fmax(acc, u);
     }
+    acc = sum ? warp_sum(acc) : warp_max(acc);
+    if (lane == 0) smem[t] = acc;
   }
-  block_reduce<NV, NS>(out, smem);
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < NV; ++t) out[t] = smem[t];
+  __syncthreads();   // smem may be reused right away
+}
+
+// The block's NV partials (valid in thread 0) to part[t * gridDim.x + blockIdx.x].
+template <int NV>
+__device__ __forceinline__ void store_partials(double* __restrict__ part, const double (&v)[NV]) {
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int t = 0; t < NV; ++t) part[(size_t)t * gridDim.x + blockIdx.x] = v[t];
+  }
 }
 
 // Warp-wide sum of V values (V a multiple of 32) by recursive halving: each of the five
@@ -181,7 +204,7 @@ __device__ __forceinline__ T group_sum(T v) {
 // FP32 blocks store W_k and T_k per observation; FP64 blocks store B_k (see the file header).
 template <typename Real>
 __host__ __device__ constexpr bool stores_products() { return sizeof(Real) == 4; }
-constexpr int kSB = 8;   // stride of B_k (2 x 3 row-major) in doubles
+constexpr int kSB = 6;   // stride of B_k (2 x 3 row-major) in doubles
 
 template <int DC>
 struct RelinNV {
@@ -197,7 +220,7 @@ template <int MODEL, int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, DC>;
+  using L = Lay<DA, DC, Real>;
   constexpr int DCc = L::DCc;
   constexpr int NS = RelinNV<DC>::NS, NV = RelinNV<DC>::NV, NZ = L::NZ;
   __shared__ double red[(kPtThreads / 32) * NV];
@@ -347,10 +370,7 @@ __global__ void __launch_bounds__(kPtThreads) k_linearize(DevState s, double* __
     }
   }
   block_reduce<NV, NS>(v, red);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int t = 0; t < NV; ++t) part[(size_t)blockIdx.x * NV + t] = v[t];
-  }
+  store_partials(part, v);
 }
 
 // One warp per chunk of a camera's observation list: partial U = sum A^T A, ga = sum A^T r,
@@ -359,7 +379,7 @@ template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_camera_chunks(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, DC>;
+  using L = Lay<DA, DC, Real>;
   using CV = CamV<DA, DC>;
   constexpr int DCc = L::DCc;
   const int lane = threadIdx.x & 31;
@@ -406,7 +426,7 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_camera_finish(DevState s, co
                                                                    double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, DC>;
+  using L = Lay<DA, DC, Real>;
   using CV = CamV<DA, DC>;
   constexpr int DCc = L::DCc;
   constexpr int PER = CV::VP / 32;
@@ -450,10 +470,7 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_camera_finish(DevState s, co
     }
   }
   block_reduce<2, 0>(v, red);
-  if (threadIdx.x == 0) {
-    part[(size_t)blockIdx.x * 2] = v[0];
-    part[(size_t)blockIdx.x * 2 + 1] = v[1];
-  }
+  store_partials(part, v);
 }
 
 // Sums the relinearisation partials: cost, Z, gc, gradient max, max diagonal, initial lambda.
@@ -525,7 +542,7 @@ template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, DC>;
+  using L = Lay<DA, DC, Real>;
   constexpr int DCc = L::DCc;
   constexpr int NV = ElimNV<DC>::NV;
   __shared__ double red[(kPtThreads / 32) * NV];
@@ -601,10 +618,7 @@ __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, doub
     }
   }
   block_reduce<NV, NV>(v, red);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int t = 0; t < NV; ++t) part[(size_t)blockIdx.x * NV + t] = v[t];
-  }
+  store_partials(part, v);
 }
 
 // One warp per chunk of a camera-pair block's observation pairs: partial sum T_k W_m^T (FP32
@@ -613,7 +627,7 @@ template <int DA, typename Real>
 __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, 0>;
+  using L = Lay<DA, 0, Real>;
   using SV = SchurV<DA>;
   const int lane = threadIdx.x & 31;
   const int ch = blockIdx.x * 4 + (threadIdx.x >> 5);
@@ -628,7 +642,7 @@ __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __rest
     for (int p = s.bc_beg[ch] + lane; p < end; p += 32) {
       const int k = s.pr_k[p], m = s.pr_m[p];
       const int j = s.o_pt[k];
-      double Ak[L::SA], Am[L::SA], Bk[kSB], Bm[kSB], vi[8];
+      double Ak[L::SA], Am[L::SA], Bk[kSB], Bm[kSB], vi[L::SV];
       vload(oA + (size_t)k * L::SA, Ak);
       vload(s.o_B + (size_t)k * kSB, Bk);
       vload(oA + (size_t)m * L::SA, Am);
@@ -697,7 +711,7 @@ template <int DA, typename Real>
 __global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, 0>;
+  using L = Lay<DA, 0, Real>;
   using SV = SchurV<DA>;
   constexpr int PER = SV::VP / 32;
   const int lane = threadIdx.x & 31;
@@ -735,7 +749,7 @@ template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, DC>;
+  using L = Lay<DA, DC, Real>;
   using RV = RhsV<DA, DC>;
   constexpr int DCc = L::DCc;
   const int lane = threadIdx.x & 31;
@@ -798,7 +812,7 @@ template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const double* __restrict__ cpart) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, DC>;
+  using L = Lay<DA, DC, Real>;
   using RV = RhsV<DA, DC>;
   constexpr int DCc = L::DCc;
   constexpr int PER = RV::VP / 32;
@@ -874,7 +888,7 @@ template <int DA, int DC, typename Real>
 __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double* __restrict__ part) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
-  using L = Lay<DA, DC>;
+  using L = Lay<DA, DC, Real>;
   constexpr int DCc = L::DCc;
   __shared__ double red[(kPtThreads / 32) * 2];
   const Dims& D = s.d;
@@ -923,7 +937,7 @@ __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double
       double q[4];
       vload(s.p_q + (size_t)j * 4, q);
       if constexpr (!stores_products<Real>()) {
-        double vi[8];
+        double vi[L::SV];
         vload(reinterpret_cast<const double*>(s.p_Vinv) + (size_t)j * L::SV, vi);
         const double a0 = acc[0], a1 = acc[1], a2 = acc[2];
 #pragma unroll
@@ -951,10 +965,7 @@ __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double
     for (int r = 0; r < 3; ++r) s.trial.X[3 * j + r] = s.cur.X[3 * j + r] + db[r];
   }
   block_reduce<2, 2>(v, red);
-  if (threadIdx.x == 0) {
-    part[(size_t)blockIdx.x * 2] = v[0];
-    part[(size_t)blockIdx.x * 2 + 1] = v[1];
-  }
+  store_partials(part, v);
 }
 
 // One thread per camera (plus the globals on thread 0 of block 0): trial parameters.
@@ -1031,10 +1042,7 @@ __global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __res
     for (int t = 0; t < 4; ++t) s.trial.dist[t] = dist[t];
   }
   block_reduce<2, 2>(v, red);
-  if (threadIdx.x == 0) {
-    part[(size_t)blockIdx.x * 2] = v[0];
-    part[(size_t)blockIdx.x * 2 + 1] = v[1];
-  }
+  store_partials(part, v);
 }
 
 // One thread per observation: sum |w e|^2 at parameters P, with the stored (frozen) weights or

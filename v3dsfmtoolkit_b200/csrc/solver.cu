@@ -464,6 +464,8 @@ int v3dba_create(const v3dba_problem* p, v3dba_handle* out) {
   TRY(alloc_params(h, s.trial, N, M));
   TRY(alloc_params(h, s.init, N, M));
   const size_t Kz = std::max(K, 1), Mz = std::max(M, 1), Nz = std::max(N, 1);
+  // 8-byte slots per block, sized for the larger (FP32, 4-float vectors) of the two strides that
+  // lm_kernels.cu uses for each block
   const int SA = (2 * dA + 3) & ~3, SW = (3 * dA + 3) & ~3, SC = (2 * std::max(dC, 1) + 3) & ~3;
   const int SG = (dA + 1) & ~1, SY = (3 * std::max(dC, 1) + 3) & ~3, SU = (dA * dA + 3) & ~3;
   const int SX = (dA * std::max(dC, 1) + 3) & ~3;
