@@ -283,6 +283,25 @@ __device__ __forceinline__ void cta_gemm_aat_lower_acc(double (&acc)[2][2][2][2]
   }
 }
 
+// Panel product acc += A Z^T with Z = L_jj^-1 lower triangular (col-major LDT): Z^T is upper
+// triangular, so output block column bj takes only the first 16 (bj + 1) terms of the inner
+// dimension (the skipped k-steps are exact zeros: the same bits as the full product).  Warp w
+// owns row block bi = w >> 1 and the block columns {3, 0} (even w) or {2, 1} (odd w), 5 units of
+// k-steps each, so every scheduler partition carries 10 units instead of 16.
+__device__ __forceinline__ int panel_bj(int w, int h) { return (w & 1) ? 2 - h : 3 * (1 - h); }
+__device__ __forceinline__ void cta_gemm_azt_acc(double (&acc)[2][2][2][2], const double* A, bool a_t,
+                                                 const double* Z) {
+  const int w = threadIdx.x >> 5;
+  const int bi = w >> 1;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int bj = panel_bj(w, h);
+    const int K = 16 * (bj + 1);
+    if (a_t) warp_mma16(acc[h], A + 16 * bi * LDT, LDT, 1, Z + 16 * bj, LDT, 1, K);
+    else warp_mma16(acc[h], A + 16 * bi, 1, LDT, Z + 16 * bj, LDT, 1, K);
+  }
+}
+
 // Tile copy global -> shared with cp.async (16-byte pieces, all in flight at once); the caller
 // waits with tile_wait() and a barrier.
 __device__ __forceinline__ void load_tile(double* dst, const double* __restrict__ S, size_t ld, size_t r0, size_t c0) {
@@ -605,9 +624,8 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     if (tid < TB) S[(pc0 + tid) * lds + n_pad] = ((red[tid] + red[TB + tid]) + red[2 * TB + tid]) + red[3 * TB + tid];
   };
-  // fragment element (h, a, b, i) of this thread: tile row and column
+  // tile row of fragment row a of this thread (the full-tile ownership of cta_gemm_abt_acc)
   auto frag_row = [&](int a) { return 16 * (w >> 1) + 8 * a + g; };
-  auto frag_col = [&](int h, int b, int i) { return 16 * (2 * (w & 1) + h) + 8 * b + 2 * q + i; };
 
   for (int lv = 0; lv < P.n_levels; ++lv) {
     stamp(2 * lv);
@@ -747,16 +765,18 @@ __global__ void __launch_bounds__(256)
       double acc[2][2][2][2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) acc_zero(acc[h]);
-      cta_gemm_abt_acc(acc, T0, tr_in, T1);
+      cta_gemm_azt_acc(acc, T0, tr_in, T1);   // T1 = Z_j, lower triangular
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
+      for (int h = 0; h < 2; ++h) {
+        const int bj = panel_bj(w, h);
 #pragma unroll
         for (int a = 0; a < 2; ++a)
 #pragma unroll
           for (int b = 0; b < 2; ++b)
 #pragma unroll
             for (int i = 0; i < 2; ++i)
-              S[(pc0 + frag_col(h, b, i)) * lds + pr0 + frag_row(a)] = acc[h][a][b][i];
+              S[(pc0 + 16 * bj + 8 * b + 2 * q + i) * lds + pr0 + frag_row(a)] = acc[h][a][b][i];
+      }
     }
     cl.sync();   // arrive.release / wait.acquire at cluster scope: the CTAs' writes are visible
   }
