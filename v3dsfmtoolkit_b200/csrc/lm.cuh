@@ -220,6 +220,8 @@ struct PcgState {
   int* rb = nullptr;            // block id of each row entry
   int* rc = nullptr;            // column camera of each row entry
   unsigned char* rt = nullptr;  // 1: use the transpose of the stored block
+  int* rd = nullptr;            // [N] entry of (i, i) in row i: the row's transposed entries
+                                // (columns < i) come before it, its direct ones after it
   int* diag_blk = nullptr;      // [N] block id of (i, i)
   void* Sb = nullptr;           // blocks (8-byte slots)
   double* Pinv = nullptr;       // inverse diagonal blocks

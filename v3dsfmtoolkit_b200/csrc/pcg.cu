@@ -50,6 +50,7 @@ struct PcgArgs {
   const int* rb;                   // block id of each row entry
   const int* rc;                   // column camera of each row entry
   const unsigned char* rt;         // 1 when the stored block is (col, row): use its transpose
+  const int* rd;                   // [N] entry of the diagonal block in row i (see PcgState)
   const void* Sb;                  // blocks, dA x dA row-major, Real
   const double* Pinv;              // [N] dA x dA inverse diagonal blocks (block-Jacobi)
   const float* cinv;               // learned: [N] 6 x 6 lower-triangular C_i^-1
@@ -197,8 +198,7 @@ __device__ __forceinline__ void grid_sums(double (&v)[NV], double* part, int& pa
 // E_(i,k) C_k^-1 r_k over its lower neighbours k (the transposed entries of its row).
 __device__ __forceinline__ void learned_lower_row(const PcgArgs& a, int i, int lane, const double* r, double* t) {
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int e = a.rp[i] + lane; e < a.rp[i + 1]; e += 32) {
-    if (!a.rt[e]) continue;
+  for (int e = a.rp[i] + lane; e < a.rd[i]; e += 32) {   // the transposed entries: a prefix of the row
     double v[6];
     const double* rv = r + (size_t)a.rc[e] * 6;
 #pragma unroll
@@ -221,8 +221,7 @@ __device__ __forceinline__ void learned_lower_row(const PcgArgs& a, int i, int l
 __device__ __forceinline__ void learned_lower_row_step(const PcgArgs& a, int i, int lane, const double* r,
                                                        const double* Ap, double alpha, double* t) {
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int e = a.rp[i] + lane; e < a.rp[i + 1]; e += 32) {
-    if (!a.rt[e]) continue;
+  for (int e = a.rp[i] + lane; e < a.rd[i]; e += 32) {   // the transposed entries: a prefix of the row
     double v[6];
     const size_t o = (size_t)a.rc[e] * 6;
 #pragma unroll
@@ -243,8 +242,12 @@ __device__ __forceinline__ void learned_lower_row_step(const PcgArgs& a, int i, 
 // neighbours l (the direct entries of its row).  Returns z_i[lane] on lanes < 6.
 __device__ __forceinline__ double learned_upper_row(const PcgArgs& a, int i, int lane, const double* t) {
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int e = a.rp[i] + lane; e < a.rp[i + 1]; e += 32) {
-    if (a.rt[e] || a.rc[e] == i) continue;
+  // the direct entries after the diagonal one: a suffix of the row, taken by each lane at the
+  // same positions rp[i] + lane + 32 m as in a walk over the whole row (the same sums)
+  int e = a.rp[i] + lane;
+  const int lo = a.rd[i] + 1;
+  if (e < lo) e += (lo - e + 31) / 32 * 32;
+  for (; e < a.rp[i + 1]; e += 32) {
     double v[6];
     const double* tv = t + (size_t)a.rc[e] * 6;
 #pragma unroll
@@ -572,17 +575,20 @@ int pcg_plan(PcgState& ps, const std::vector<int>& b_i, const std::vector<int>& 
     if (l != i) rows[l].push_back({i, (int)(2 * b + 1)});
     else diag[i] = (int)b;
   }
-  std::vector<int> rp(1, 0), rb, rc;
+  std::vector<int> rp(1, 0), rb, rc, rd(N, -1);
   std::vector<unsigned char> rt;
   for (int i = 0; i < N; ++i) {
     std::sort(rows[i].begin(), rows[i].end());
     for (auto& e : rows[i]) {
+      // sorted by column: transposed entries (columns < i), the diagonal, direct entries
+      if (e.first == i) rd[i] = (int)rc.size();
+      if ((e.second & 1) != (e.first < i ? 1 : 0)) return V3DBA_ERR_INVALID_INPUT;
       rc.push_back(e.first);
       rb.push_back(e.second / 2);
       rt.push_back((unsigned char)(e.second & 1));
     }
     rp.push_back((int)rc.size());
-    if (diag[i] < 0) return V3DBA_ERR_INVALID_INPUT;
+    if (diag[i] < 0 || rd[i] < 0) return V3DBA_ERR_INVALID_INPUT;
   }
   auto up = [](auto** d, const auto& h) -> int {
     using T = typename std::remove_reference<decltype(h)>::type::value_type;
@@ -593,7 +599,7 @@ int pcg_plan(PcgState& ps, const std::vector<int>& b_i, const std::vector<int>& 
   };
   int rc2;
   if ((rc2 = up(&ps.rp, rp)) || (rc2 = up(&ps.rb, rb)) || (rc2 = up(&ps.rc, rc)) || (rc2 = up(&ps.rt, rt)) ||
-      (rc2 = up(&ps.diag_blk, diag)))
+      (rc2 = up(&ps.rd, rd)) || (rc2 = up(&ps.diag_blk, diag)))
     return rc2;
   return V3DBA_OK;
 }
@@ -619,7 +625,7 @@ int pcg_alloc(PcgState& ps, int nb, int N, int DA) {
 }
 
 void pcg_free(PcgState& ps) {
-  cudaFree(ps.rp); cudaFree(ps.rb); cudaFree(ps.rc); cudaFree(ps.rt); cudaFree(ps.diag_blk);
+  cudaFree(ps.rp); cudaFree(ps.rb); cudaFree(ps.rc); cudaFree(ps.rt); cudaFree(ps.rd); cudaFree(ps.diag_blk);
   cudaFree(ps.Sb); cudaFree(ps.Pinv); cudaFree(ps.vec); cudaFree(ps.part); cudaFree(ps.iters);
   cudaFree(ps.gauge_rows); cudaFree(ps.gauge_L);
   ps = PcgState();
@@ -648,7 +654,7 @@ PcgArgs make_args(PcgState& ps, int N, int DA, double tol, int max_iter, double*
   const size_t n = (size_t)N * DA;
   PcgArgs a;
   a.N = N; a.DA = DA; a.n = (int)n;
-  a.rp = ps.rp; a.rb = ps.rb; a.rc = ps.rc; a.rt = ps.rt; a.Sb = ps.Sb;
+  a.rp = ps.rp; a.rb = ps.rb; a.rc = ps.rc; a.rt = ps.rt; a.rd = ps.rd; a.Sb = ps.Sb;
   a.Pinv = ps.Pinv; a.b = ps.b; a.x = x;
   a.r = ps.vec + n; a.z = ps.vec + 2 * n; a.p = ps.vec + 3 * n; a.Ap = ps.vec + 4 * n;
   a.t = ps.vec + 5 * n; a.p2 = ps.vec + 6 * n; a.r2 = ps.vec + 7 * n;
