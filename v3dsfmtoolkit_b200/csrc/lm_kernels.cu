@@ -111,13 +111,18 @@ __device__ void fold_partials(const double* __restrict__ part, int nblk, double 
   __syncthreads();   // smem may be reused right away
 }
 
-// The block's NV partials (valid in thread 0) to part[t * gridDim.x + blockIdx.x].
+// The block's NV partials (valid in thread 0) to part[t * nblk + bid] (by default the launch's
+// block index and count; a stage run as a block range of a merged launch passes its own).
 template <int NV>
-__device__ __forceinline__ void store_partials(double* __restrict__ part, const double (&v)[NV]) {
+__device__ __forceinline__ void store_partials(double* __restrict__ part, const double (&v)[NV], int bid, int nblk) {
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int t = 0; t < NV; ++t) part[(size_t)t * gridDim.x + blockIdx.x] = v[t];
+    for (int t = 0; t < NV; ++t) part[(size_t)t * nblk + bid] = v[t];
   }
+}
+template <int NV>
+__device__ __forceinline__ void store_partials(double* __restrict__ part, const double (&v)[NV]) {
+  store_partials(part, v, (int)blockIdx.x, (int)gridDim.x);
 }
 
 // Warp-wide sum of V values (V a multiple of 32) by recursive halving: each of the five
@@ -624,13 +629,11 @@ __global__ void __launch_bounds__(kPtThreads) k_point_eliminate(DevState s, doub
 // One warp per chunk of a camera-pair block's observation pairs: partial sum T_k W_m^T (FP32
 // blocks: the stored T_k and W_m; FP64 blocks: A_k^T (B_k Vinv_j B_m^T) A_m).
 template <int DA, typename Real>
-__global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __restrict__ part) {
-  pdl_wait();      // the previous stage's writes are visible
-  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+__device__ __forceinline__ void schur_chunks_body(DevState s, double* __restrict__ part, int bid, int nblk) {
   using L = Lay<DA, 0, Real>;
   using SV = SchurV<DA>;
   const int lane = threadIdx.x & 31;
-  const int ch = blockIdx.x * 4 + (threadIdx.x >> 5);
+  const int ch = bid * 4 + (threadIdx.x >> 5);
   if (ch >= s.nch_blk) return;
   Real acc[SV::VP];
 #pragma unroll
@@ -705,19 +708,27 @@ __global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __rest
   for (int t = 0; t < SV::VP / 32; ++t) part[(size_t)ch * SV::VP + lane * (SV::VP / 32) + t] = double(acc[t]);
 }
 
+template <int DA, typename Real>
+__global__ void __launch_bounds__(128) k_schur_chunks(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+  schur_chunks_body<DA, Real>(s, part, blockIdx.x, gridDim.x);
+}
+
 // One warp per camera-pair block (i <= l): S_il = delta_il (U_i + lambda I) - sum of its chunk
 // partials, written into the lower triangle of the dense column-major S.
 template <int DA, typename Real>
-__global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* __restrict__ part) {
-  pdl_wait();      // the previous stage's writes are visible
-  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+__device__ __forceinline__ void schur_finish_body(DevState s, const double* __restrict__ part, int bid, int nblk,
+                                                  bool skip_fixed_diag = false) {
   using L = Lay<DA, 0, Real>;
   using SV = SchurV<DA>;
   constexpr int PER = SV::VP / 32;
   const int lane = threadIdx.x & 31;
-  const int b = blockIdx.x * 4 + (threadIdx.x >> 5);
+  const int b = bid * 4 + (threadIdx.x >> 5);
   if (b >= s.nb) return;
   const int i = s.b_i[b], l = s.b_l[b];
+  // beside rhs_finish in one launch, the identity block of a fixed camera is rhs_finish's alone
+  if (skip_fixed_diag && i == l && i < s.d.nnA) return;
   double sum[PER];
 #pragma unroll
   for (int t = 0; t < PER; ++t) sum[t] = 0.0;
@@ -743,17 +754,22 @@ __global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* 
   }
 }
 
+template <int DA, typename Real>
+__global__ void __launch_bounds__(128) k_schur_finish(DevState s, const double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+  schur_finish_body<DA, Real>(s, part, blockIdx.x, gridDim.x);
+}
+
 // One warp per chunk of a camera's observations: partial sum_k W_k q_j(k) and sum_k T_k Y_j(k),
 // the latter as sum_k W_k (Vinv Y)_j(k) (FP64 blocks: W_k x as A_k^T (B_k x)).
 template <int DA, int DC, typename Real>
-__global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, double* __restrict__ part) {
-  pdl_wait();      // the previous stage's writes are visible
-  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+__device__ __forceinline__ void rhs_chunks_body(DevState s, double* __restrict__ part, int bid, int nblk) {
   using L = Lay<DA, DC, Real>;
   using RV = RhsV<DA, DC>;
   constexpr int DCc = L::DCc;
   const int lane = threadIdx.x & 31;
-  const int ch = blockIdx.x * kCamWarps + (threadIdx.x >> 5);
+  const int ch = bid * kCamWarps + (threadIdx.x >> 5);
   if (ch >= s.nch_cam) return;
   double acc[RV::VP];
 #pragma unroll
@@ -806,19 +822,24 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, doubl
   for (int t = 0; t < RV::VP / 32; ++t) part[(size_t)ch * RV::VP + lane * (RV::VP / 32) + t] = acc[t];
 }
 
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kCamWarps * 32) k_rhs_chunks(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+  rhs_chunks_body<DA, DC, Real>(s, part, blockIdx.x, gridDim.x);
+}
+
 // One warp per camera: rhs_i = ga_i - sum W q and the camera/global border X_i - sum T Y into S;
 // identity block, zero rhs and zero border for fixed cameras.
 template <int DA, int DC, typename Real>
-__global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const double* __restrict__ cpart) {
-  pdl_wait();      // the previous stage's writes are visible
-  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+__device__ __forceinline__ void rhs_finish_body(DevState s, const double* __restrict__ cpart, int bid, int nblk) {
   using L = Lay<DA, DC, Real>;
   using RV = RhsV<DA, DC>;
   constexpr int DCc = L::DCc;
   constexpr int PER = RV::VP / 32;
   const Dims& D = s.d;
   const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * kCamWarps + (threadIdx.x >> 5);
+  const int i = bid * kCamWarps + (threadIdx.x >> 5);
   if (i >= D.N) return;
   const size_t ld = s.ld, rs = s.rhs_stride;
   const int c0 = D.N * DA;
@@ -853,11 +874,16 @@ __global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const
   }
 }
 
-// Global block: S_cc = Z + lambda I - sum_j Y_j^T Vinv_j Y_j, rhs_c = gc - sum_j Y_j^T q_j.
-template <int DA, int DC>
-__global__ void __launch_bounds__(256) k_global_block(DevState s, const double* __restrict__ part, int nbp) {
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kCamWarps * 32) k_rhs_finish(DevState s, const double* __restrict__ cpart) {
   pdl_wait();      // the previous stage's writes are visible
   pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+  rhs_finish_body<DA, DC, Real>(s, cpart, blockIdx.x, gridDim.x);
+}
+
+// Global block: S_cc = Z + lambda I - sum_j Y_j^T Vinv_j Y_j, rhs_c = gc - sum_j Y_j^T q_j.
+template <int DA, int DC>
+__device__ __forceinline__ void global_block_body(DevState s, const double* __restrict__ part, int nbp, int bid, int nblk) {
   constexpr int NV = ElimNV<DC>::NV;
   constexpr int DCc = DC > 0 ? DC : 1;
   __shared__ double red[8 * NV];
@@ -880,20 +906,25 @@ __global__ void __launch_bounds__(256) k_global_block(DevState s, const double* 
   }
 }
 
+template <int DA, int DC>
+__global__ void __launch_bounds__(256) k_global_block(DevState s, const double* __restrict__ part, int nbp) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+  global_block_body<DA, DC>(s, part, nbp, blockIdx.x, gridDim.x);
+}
+
 // ---- trial step ----------------------------------------------------------------------------
 
 // G lanes per point: db_j = q_j - sum_k T_k^T da_i(k) - (Vinv Y_j) dc; X' = X + db.  With FP64
 // blocks the sum is Vinv_j sum_k B_k^T (A_k da_i(k)).
 template <int DA, int DC, typename Real>
-__global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double* __restrict__ part) {
-  pdl_wait();      // the previous stage's writes are visible
-  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+__device__ __forceinline__ void point_backsub_body(DevState s, double* __restrict__ part, int bid, int nblk) {
   using L = Lay<DA, DC, Real>;
   constexpr int DCc = L::DCc;
   __shared__ double red[(kPtThreads / 32) * 2];
   const Dims& D = s.d;
   constexpr int G = backsub_lanes<Real>();
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = bid * blockDim.x + threadIdx.x;
   const int j = gt / G, lig = gt % G;
   const bool active = j < D.M && j >= D.nnB;
   double v[2] = {0.0, 0.0};
@@ -965,17 +996,22 @@ __global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double
     for (int r = 0; r < 3; ++r) s.trial.X[3 * j + r] = s.cur.X[3 * j + r] + db[r];
   }
   block_reduce<2, 2>(v, red);
-  store_partials(part, v);
+  store_partials(part, v, bid, nblk);
+}
+
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(kPtThreads) k_point_backsub(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+  point_backsub_body<DA, DC, Real>(s, part, blockIdx.x, gridDim.x);
 }
 
 // One thread per camera (plus the globals on thread 0 of block 0): trial parameters.
 template <int MODEL, int DA, int DC>
-__global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __restrict__ part) {
-  pdl_wait();      // the previous stage's writes are visible
-  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+__device__ __forceinline__ void camera_update_body(DevState s, double* __restrict__ part, int bid, int nblk) {
   __shared__ double red[4 * 2];
   const Dims& D = s.d;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = bid * blockDim.x + threadIdx.x;
   const double* x = s.x;
   double v[2] = {0.0, 0.0};
   if (i < D.N) {
@@ -1024,7 +1060,7 @@ __global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __res
       for (int t = 0; t < 4; ++t) s.trial.dist[4 * i + t] = dist[t];
     }
   }
-  if (MODEL == kModelCommon && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (MODEL == kModelCommon && bid == 0 && threadIdx.x == 0) {
     double K[9], dist[4];
     for (int t = 0; t < 9; ++t) K[t] = s.cur.K[t];
     for (int t = 0; t < 4; ++t) dist[t] = s.cur.dist[t];
@@ -1042,7 +1078,52 @@ __global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __res
     for (int t = 0; t < 4; ++t) s.trial.dist[t] = dist[t];
   }
   block_reduce<2, 2>(v, red);
-  store_partials(part, v);
+  store_partials(part, v, bid, nblk);
+}
+
+template <int MODEL, int DA, int DC>
+__global__ void __launch_bounds__(128) k_camera_update(DevState s, double* __restrict__ part) {
+  pdl_wait();      // the previous stage's writes are visible
+  pdl_trigger();   // the next stage may be scheduled once all blocks of this one are resident
+  camera_update_body<MODEL, DA, DC>(s, part, blockIdx.x, gridDim.x);
+}
+
+// ---- merged launches of independent stages (the LM path) -------------------------------------
+// Stages that do not read each other's output run as block ranges of one launch: one kernel
+// boundary (drain and fill) less each.  Every block runs the same code on the same data as in the
+// stage's own kernel (block index and count of its range), so the results are the same bits.
+
+// Schur chunks (blocks [0, g1)) and reduced-rhs chunks: both read only the elimination's output.
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(128) k_chunks_merged(DevState s, int g1, int g2) {
+  pdl_wait();
+  pdl_trigger();
+  if ((int)blockIdx.x < g1) schur_chunks_body<DA, Real>(s, s.part_bc, blockIdx.x, g1);
+  else rhs_chunks_body<DA, DC, Real>(s, s.part_cc, blockIdx.x - g1, g2);
+}
+
+// Schur finish (blocks [0, g1)), rhs / border finish ([g1, g1 + g2)) and, with global
+// parameters, the global block (the last block): they write disjoint parts of S and rhs.
+template <int DA, int DC, typename Real>
+__global__ void __launch_bounds__(128) k_finish_merged(DevState s, int g1, int g2, const double* __restrict__ pelim,
+                                                       int nbp) {
+  pdl_wait();
+  pdl_trigger();
+  const int b = blockIdx.x;
+  if (b < g1) schur_finish_body<DA, Real>(s, s.part_bc, b, g1, true);
+  else if (b < g1 + g2) rhs_finish_body<DA, DC, Real>(s, s.part_cc, b - g1, g2);
+  else global_block_body<DA, DC>(s, pelim, nbp, 0, 1);
+}
+
+// Camera (and global) update (blocks [0, g1)) and point back-substitution: both read the
+// reduced solution and the current parameters and write different parts of the trial ones.
+template <int MODEL, int DA, int DC, typename Real>
+__global__ void __launch_bounds__(128) k_update_merged(DevState s, int g1, int g2, double* __restrict__ pcam,
+                                                       double* __restrict__ ppt) {
+  pdl_wait();
+  pdl_trigger();
+  if ((int)blockIdx.x < g1) camera_update_body<MODEL, DA, DC>(s, pcam, blockIdx.x, g1);
+  else point_backsub_body<DA, DC, Real>(s, ppt, blockIdx.x - g1, g2);
 }
 
 // One thread per observation: sum |w e|^2 at parameters P, with the stored (frozen) weights or
@@ -1208,11 +1289,39 @@ struct Ops {
   static int relinearize(DevState& s, bool init_lambda, double tau, cudaStream_t st) {
     return run(s, kStageLinearize, kStageRelinFinalize, init_lambda ? 1 : 0, tau, st);
   }
-  static int build_reduced(DevState& s, cudaStream_t st) {
-    return run(s, kStagePointEliminate, kStageGlobalBlock, 0, 0.0, st);
+  static int launched(cudaError_t e) {
+    if (e != cudaSuccess) {
+      fprintf(stderr, "v3dba: merged launch failed: %s\n", cudaGetErrorString(e));
+      cudaGetLastError();
+      return V3DBA_ERR_CUDA;
+    }
+    V3DBA_LAUNCH_CHECK();
+    return V3DBA_OK;
   }
+  // elimination, then the Schur and rhs chunks in one launch, then the three finishing stages in
+  // one launch (the same work as the stages kStagePointEliminate .. kStageGlobalBlock)
+  static int build_reduced(DevState& s, cudaStream_t st) {
+    int rc = stage(s, kStagePointEliminate, 0, 0.0, st);
+    if (rc) return rc;
+    const PartLayout pl = part_layout<DA, DC>(s);
+    const int g1 = s.nch_blk > 0 ? cdiv(s.nch_blk, 4) : 0, g2 = s.nch_cam > 0 ? cdiv(s.nch_cam, kCamWarps) : 0;
+    if (g1 + g2 > 0 && (rc = launched(launch_pdl(k_chunks_merged<DA, DC, Real>, dim3(g1 + g2), dim3(128), 0, st, s,
+                                                 g1, g2))))
+      return rc;
+    const int f1 = s.nb > 0 ? cdiv(s.nb, 4) : 0, f2 = cdiv(std::max(s.d.N, 1), kCamWarps);
+    const int bp = cdiv(std::max(s.d.M, 1), kPtThreads);
+    return launched(launch_pdl(k_finish_merged<DA, DC, Real>, dim3(f1 + f2 + (DC > 0 ? 1 : 0)), dim3(128), 0, st, s,
+                               f1, f2, (const double*)(s.part + pl.elim), bp));
+  }
+  // camera update and point back-substitution in one launch, then the trial cost and the step
+  // statistics (the stages kStagePointBacksub .. kStageTrialFinalize)
   static int finish_trial(DevState& s, cudaStream_t st) {
-    return run(s, kStagePointBacksub, kStageTrialFinalize, 0, 0.0, st);
+    const PartLayout pl = part_layout<DA, DC>(s);
+    const int bu = cdiv(std::max(s.d.N, 1), 128), bb = lane_blocks(s.d.M, backsub_lanes<Real>());
+    int rc = launched(launch_pdl(k_update_merged<MODEL, DA, DC, Real>, dim3(bu + bb), dim3(128), 0, st, s, bu, bb,
+                                 s.part + pl.camupd, s.part + pl.backsub));
+    if (rc) return rc;
+    return run(s, kStageTrialCost, kStageTrialFinalize, 0, 0.0, st);
   }
   static int cost(DevState& s, const ParamSet& P, double* d_out, cudaStream_t st) {
     const PartLayout pl = part_layout<DA, DC>(s);
