@@ -245,6 +245,9 @@ int tile_chol_plan(TileChol& tc, int n, std::vector<uint8_t>& tile_nz);
 void tile_chol_free(TileChol& tc);
 // Zeroes the pattern tiles of S (column-major, ld) and sets the padding diagonal to 1.
 int tile_chol_zero(const TileChol& tc, double* S, double* rhs, cudaStream_t st);
+// The same, and in the same launch the start of a trial: *d_lambda = lambda, *d_fail = 0.
+int tile_chol_zero_setup(const TileChol& tc, double* S, double lambda, double* d_lambda, int* d_fail,
+                         cudaStream_t st);
 // Factors S in place and writes the solution to x; *d_fail = 1 on a non-positive pivot.
 int tile_chol_solve(const TileChol& tc, double* S, double* x, int* d_fail, cudaStream_t st);
 // Same factorisation and solve in one launch of an 8-CTA thread-block cluster.

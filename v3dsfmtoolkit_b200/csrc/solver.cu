@@ -608,9 +608,13 @@ int run_trial(v3dba_handle h, const LmOps* ops, double lambda, bool pcg, int pre
   int rc;
   {
     NvtxRange nvtx("v3dba.reduced_system");
-    V3DBA_CUDA_TRY(launch_pdl(k_trial_setup, dim3(1), dim3(1), 0, st, lambda, s.d_lambda, s.d_fail));
-    V3DBA_LAUNCH_CHECK();
-    if (!pcg && (rc = tile_chol_zero(h->chol, s.S, s.rhs, st))) return rc;
+    if (!pcg && !h->chol.h_tiles.empty()) {
+      // clearing the reduced system's tiles also sets the damping and the failure flag
+      if ((rc = tile_chol_zero_setup(h->chol, s.S, lambda, s.d_lambda, s.d_fail, st))) return rc;
+    } else {
+      V3DBA_CUDA_TRY(launch_pdl(k_trial_setup, dim3(1), dim3(1), 0, st, lambda, s.d_lambda, s.d_fail));
+      V3DBA_LAUNCH_CHECK();
+    }
     if ((rc = ops->build_reduced(s, st))) return rc;
   }
   int fallback = 0;

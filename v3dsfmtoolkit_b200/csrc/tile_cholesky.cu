@@ -220,10 +220,18 @@ __global__ void __launch_bounds__(256) k_chol_backsolve(const double* __restrict
   }
 }
 
+// Clears the pattern tiles of S (padding diagonal 1).  With d_lambda set, block 0 also starts the
+// trial: the damping and a cleared failure flag (the work of the trial-setup kernel, one launch
+// less per trial).
 __global__ void __launch_bounds__(256) k_chol_zero(double* __restrict__ S, int ld, int nt, int n, int n_pad,
-                                                   const int* __restrict__ tiles) {
+                                                   const int* __restrict__ tiles, double lambda,
+                                                   double* __restrict__ d_lambda, int* __restrict__ d_fail) {
   pdl_wait();
   pdl_trigger();
+  if (d_lambda && blockIdx.x == 0 && threadIdx.x == 0) {
+    *d_lambda = lambda;
+    *d_fail = 0;
+  }
   const int t = tiles[blockIdx.x];
   const int tr = t / (nt + 1) , tc = t % (nt + 1);
   const size_t r0 = (size_t)tr * TB, c0 = (size_t)tc * TB;
@@ -322,7 +330,16 @@ void tile_chol_free(TileChol& tc) {
 int tile_chol_zero(const TileChol& tc, double* S, double* /*rhs*/, cudaStream_t st) {
   if (tc.h_tiles.empty()) return V3DBA_OK;
   V3DBA_CUDA_TRY(launch_pdl(k_chol_zero, dim3((unsigned)tc.h_tiles.size()), dim3(256), 0, st, S, tc.ld, tc.nt, tc.n,
-                            tc.n_pad, (const int*)tc.d_tiles));
+                            tc.n_pad, (const int*)tc.d_tiles, 0.0, (double*)nullptr, (int*)nullptr));
+  V3DBA_LAUNCH_CHECK();
+  return V3DBA_OK;
+}
+
+int tile_chol_zero_setup(const TileChol& tc, double* S, double lambda, double* d_lambda, int* d_fail,
+                         cudaStream_t st) {
+  if (tc.h_tiles.empty()) return V3DBA_ERR_INVALID_ARGUMENT;
+  V3DBA_CUDA_TRY(launch_pdl(k_chol_zero, dim3((unsigned)tc.h_tiles.size()), dim3(256), 0, st, S, tc.ld, tc.nt, tc.n,
+                            tc.n_pad, (const int*)tc.d_tiles, lambda, d_lambda, d_fail));
   V3DBA_LAUNCH_CHECK();
   return V3DBA_OK;
 }
