@@ -15,9 +15,9 @@
  *   v3dba_set_params /
  *   v3dba_get_params       <- the optimizer's in-place mutation of the caller's cameras, points,
  *                             K and distortion references (v3d_metricbundle.h:94-95, 232-233, 316)
- *                             StereoMetricBundleOptimizer (V3D/include/Geometry/v3d_stereobundle.h:
- *                              22-163, V3D/src/Geometry/v3d_stereobundle.cpp:45-67) as
- *                              V3DBA_MODEL_STEREO
+ *   v3dba_create with
+ *   V3DBA_MODEL_STEREO     <- StereoMetricBundleOptimizer (V3D/include/Geometry/v3d_stereobundle.h:
+ *                              22-163, V3D/src/Geometry/v3d_stereobundle.cpp:45-67)
  *   v3dba_refine_consistent_rotations / v3dba_rotations_*
  *                          <- V3D::refineConsistentRotations and its SparseRotationOptimizer
  *                             (V3D/include/Geometry/v3d_mviewutilities.h:359-362,
