@@ -17,7 +17,7 @@ reduced-system Cholesky (dtype "f32+f64").
 --impl reference times the reference's own CPU optimizer (compiled from its sources) on the same
 scene: complete minimize() runs to its own stop, setup included, single-threaded as the reference
 is (one run on the 200-camera scene, ~75 s).  --workload circle20 is the 20-camera plain metric
-BA (FP64).
+BA (2k points, 8k observations, FP64 throughout).
 With N > 1 every rank solves its own replica (a single BA does not shard; "replicas only").
 
 --workload cluster2000 measures the large-scene path: 2,000 cameras in 20 clusters, 1M points,

@@ -2,7 +2,7 @@
 
 The reference has no iterative solver and no learned component (it factors the damped normal
 equations with LDL^T, V3D/src/Math/v3d_optimization.cpp:1096-1145), so this module restates the
-method of ``v3dsfmtoolkit_b200/csrc/precond_gnn.cu`` from its mathematics and is the judge of
+method of ``v3dsfmtoolkit_b200/csrc/precond_gnn.cu`` from its mathematics and is the check of
 the CUDA kernels' features, network outputs, loss and weight gradients:
 
   * normalisation: C_i C_i^T = S_ii, F_e = C_b^-1 S_(b,a) C_a^-T for every edge a < b;
@@ -14,7 +14,7 @@ the CUDA kernels' features, network outputs, loss and weight gradients:
     of MurmurHash3 over the entry index and the seed) and dL/dcoef;
   * the gauge basis Z of a camera set (the 7 similarity motions).
 
-Parity of the preconditioned solve itself is judged against block-Jacobi PCG (oracle
+Parity of the preconditioned solve itself is checked against block-Jacobi PCG (oracle
 ``orc_pcg``) and the direct solve.  Nothing in the product path imports this file.
 """
 from __future__ import annotations

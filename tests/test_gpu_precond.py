@@ -1,7 +1,7 @@
 """Learned PCG preconditioner and gauge coarse space on the GPU: features, network outputs, loss
 and weight gradients against the CPU oracle; BF16 inference against the FP32 path; training;
 PCG iteration cuts; and the LM loop with the learned preconditioner against block-Jacobi as
-fallback and judge."""
+fallback and check."""
 import os
 
 import numpy as np
@@ -157,7 +157,7 @@ def test_trained_model_cuts_pcg_iterations_on_held_out_systems():
 def test_lm_with_learned_preconditioner_matches_block_jacobi():
     """FP64 blocks: the LM loop with the learned preconditioner reaches the cost of the
     block-Jacobi run within 1e-6 relative with at most half its PCG iterations; block-Jacobi
-    judges it."""
+    is the check."""
     m = shipped_model()
     sc = scenes.cluster_scene(n_groups=4, cams_per_group=50, n_points=30000, seed=990011)
     hj = capi.Handle.from_scene(sc)
