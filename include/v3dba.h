@@ -59,7 +59,7 @@ enum {
   V3DBA_ERR_CUDA = 3,               /* a CUDA call failed                                   */
   V3DBA_ERR_OUT_OF_MEMORY = 4,      /* device allocation failed                            */
   V3DBA_ERR_NO_DEVICE = 5,          /* no CUDA device                                       */
-  V3DBA_ERR_UNSUPPORTED = 6,        /* a configuration this build does not handle           */
+  V3DBA_ERR_UNSUPPORTED = 6,        /* a configuration this library does not handle         */
   V3DBA_ERR_TIMEOUT = 7,            /* a bounded device-side wait gave up                   */
   V3DBA_ERR_NUMERICAL = 8           /* training of the learned preconditioner diverged       */
 };
