@@ -40,12 +40,14 @@ namespace {
 constexpr double kGemmUs = 2.0, kFactorUs = 20.0, kBarrierUs = 1.0, kStoreUs = 0.5;
 // the same for one update or solve of the rhs row (a GEMV over one tile)
 constexpr double kGemvUs = 0.6;
-// Measured on B200 (sequence200 pattern, per CTA): one tile update with its operand loads, the
-// factor of a diagonal tile, the load + store of an updated tile.  They size the phase budget
-// into which updates that are not yet due are moved.  (A sweep of the update / factor costs over
-// 3.5-6 / 9-14 us moved the sequence200 factor + solve between 0.234 and 0.252 ms; applying every
-// update only when due took 0.334 ms.)
-constexpr double kMeasGemmUs = 3.5, kMeasFactorUs = 9.0, kMeasTileUs = 1.5, kMeasGemvUs = 1.0;
+// Measured on B200 (sequence200 pattern, per CTA): one tile update with its operand loads, one
+// update of a diagonal tile (its lower triangle only, one operand tile), the factor of a diagonal
+// tile, the load + store of an updated tile, one update of the rhs row.  They size the phase
+// budget into which updates that are not yet due are moved.  (A sweep of the update / factor
+// costs over 3.5-6 / 9-14 us moved the sequence200 factor + solve between 0.234 and 0.252 ms;
+// applying every update only when due took 0.334 ms.  The diagonal-update and rhs costs are
+// fitted to the phase times of the kernel's own timestamps.)
+constexpr double kMeasGemmUs = 3.5, kMeasDiagUs = 2.8, kMeasFactorUs = 9.0, kMeasTileUs = 1.5, kMeasGemvUs = 2.0;
 
 struct TileGraph {
   int nt = 0;
@@ -268,7 +270,7 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks)
       }
       ph1.push_back(make_task(r, c, it->second.data(), nc, factor));
       cost1.push_back(factor ? kFactorUs + kGemmUs * nc : (r == nt ? kGemvUs : kGemmUs) * nc + kStoreUs);
-      meas1.push_back(factor ? kMeasFactorUs + kMeasTileUs + kMeasGemmUs * nc
+      meas1.push_back(factor ? kMeasFactorUs + kMeasTileUs + kMeasDiagUs * nc
                              : r == nt ? kMeasGemvUs * nc : kMeasGemmUs * nc + kMeasTileUs);
       it = pending.erase(it);
     }
@@ -293,7 +295,7 @@ int tile_levels_build(TileChol& tc, const std::vector<uint8_t>& orig, int ranks)
     for (const auto& key : opt) {
       std::vector<int>& ks = pending[key];
       const int r = key.first, c = key.second;
-      const double g = r == nt ? kMeasGemvUs : kMeasGemmUs, fixed = r == nt ? 0.0 : kMeasTileUs;
+      const double g = r == nt ? kMeasGemvUs : (r == c ? kMeasDiagUs : kMeasGemmUs), fixed = r == nt ? 0.0 : kMeasTileUs;
       int best = 0;
       for (int q = 1; q < ranks; ++q)
         if (load[q] < load[best]) best = q;
