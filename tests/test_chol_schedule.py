@@ -199,6 +199,48 @@ def test_sequence_pattern_is_cut_into_few_levels():
     assert s["est_levels_us"] < 0.85 * s["est_steps_us"]
 
 
+# Per-CTA costs (µs) of k_chol_levels on B200, from its per-level phase timestamps on the
+# 200-camera sequence pattern: a tile update with its operand loads, an update of a diagonal tile
+# (lower triangle, one operand tile), an update of the rhs row, the factor of a diagonal tile, the
+# load + store of an updated tile, a cluster barrier, a panel product, an rhs-row solve.
+MEASURED_US = dict(gemm=3.5, gdiag=2.8, gemv=2.0, factor=9.0, tile=1.5, barrier=0.8, panel=3.8, solve=1.8)
+
+
+def replay_phases(s, nt, c=MEASURED_US):
+    """Phase-1 and phase-2 durations of every level of a plan: the longest CTA's task costs plus
+    the barrier that ends the phase."""
+    P, R = s["plan"], s["ranks"]
+    p1, p2 = [], []
+    for lv in range(s["n_levels"]):
+        loads1, loads2 = np.zeros(R), np.zeros(R)
+        for r in range(R):
+            for t in P["p1"][P["p1ptr"][lv * R + r]:P["p1ptr"][lv * R + r + 1]]:
+                nk = P["task_cptr"][t + 1] - P["task_cptr"][t]
+                row, col = P["task_r"][t], P["task_c"][t]
+                if row == nt:
+                    loads1[r] += c["gemv"] * nk
+                elif row == col:
+                    loads1[r] += c["tile"] + c["gdiag"] * nk + (c["factor"] if P["task_mode"][t] & FACTOR else 0.0)
+                else:
+                    loads1[r] += c["tile"] + c["gemm"] * nk
+            for t in P["p2"][P["p2ptr"][lv * R + r]:P["p2ptr"][lv * R + r + 1]]:
+                loads2[r] += c["solve"] if P["task_r"][t] == nt else c["panel"]
+        p1.append(loads1.max() + c["barrier"])
+        p2.append(loads2.max() + c["barrier"])
+    return np.array(p1), np.array(p2)
+
+
+def test_sequence_plan_replayed_at_measured_costs():
+    """The sequence plan replayed at the measured per-task costs: its phases sum to 169.2 µs, and
+    the kernel's own timestamps for the same plan sum to 170.4 µs.  A planner that charged 3.5 µs
+    per diagonal update and 1 µs per rhs update made a plan that replays at 183.7 µs; on the GPU
+    the two plans took 0.2226 (that one) and 0.2135 ms (this one) per factor + solve."""
+    s = capi.tile_schedule(band_arrow(19))
+    p1, p2 = replay_phases(s, 19)
+    assert p1.sum() + p2.sum() < 172.0
+    assert p1.max() < 23.0                 # no phase longer than the top level's factor + 4 updates
+
+
 def test_dense_pattern_keeps_the_column_kernel():
     s = capi.tile_schedule(np.tril(np.ones((12, 12), bool)))
     assert not s["uses_levels"]
